@@ -1,0 +1,189 @@
+/* tcs.h — C ABI of the B200 thread-coarsened stencil engine (libtcs.so).
+ *
+ * This is the drop-in boundary for the reference's host interface `launchUpdateGrid.h`
+ * (cuda/launchUpdateGrid.h:13-18) and the generated implementation of it
+ * (cuda/generateLaunchUpdateGrid.py:71-158).  The reference bakes one stencil parameter set
+ * into one generated `kernels.cu`; here a `tcs_stencil` handle plays that role: it is created
+ * from a `tcs_spec` (the generators' argv, cuda/generate2DStencil_cuda.py:31-44,
+ * cuda/generate3DStencil_cuda.py:32-46) and owns the kernels instantiated for it.
+ *
+ * Conventions: plain C types only; device buffers are raw device pointers owned by the caller;
+ * `stream` is a cudaStream_t (NULL = legacy default stream, as in the reference).  Every call
+ * returns a status (TCS_OK or a TCS_ERR_* code) and never throws or exits; the message of the
+ * last failure on the calling thread is available from tcs_last_error().
+ */
+#ifndef TCS_H
+#define TCS_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TCS_ABI_VERSION 1
+
+/* Status codes. */
+#define TCS_OK 0
+#define TCS_ERR_INVALID_VALUE 1   /* bad/mismatched argument: the reference throws cudaErrorInvalidValue */
+#define TCS_ERR_CUDA 2            /* a CUDA runtime/driver call failed */
+#define TCS_ERR_COMPILE 3         /* NVRTC instantiation of the kernel templates failed */
+#define TCS_ERR_UNSUPPORTED 4     /* launch shape not supported by the requested kernel variant */
+#define TCS_ERR_DEVICE_TIMEOUT 5  /* a bounded device-side wait expired (recorded by the kernel) */
+#define TCS_ERR_NO_DEVICE 6       /* no CUDA device is visible */
+
+/* Parameter enumerations (string forms in the reference: 'Box'/'Star', 'Row'/'Column',
+ * 'Jacobi'/'Variable', 'None'/'Read'/'Write'). */
+#define TCS_BOX 0
+#define TCS_STAR 1
+#define TCS_ROW 0
+#define TCS_COLUMN 1
+#define TCS_JACOBI 0
+#define TCS_VARIABLE 1
+#define TCS_ALIGN_NONE 0
+#define TCS_ALIGN_READ 1
+#define TCS_ALIGN_WRITE 2
+#define TCS_F64 0 /* the reference's arithmetic (double) */
+#define TCS_F32 1 /* single-precision grids */
+
+/* Kernel variants. */
+#define TCS_VARIANT_AUTO 0   /* march when the tile fits its TMA/shared-memory limits, else direct */
+#define TCS_VARIANT_DIRECT 1 /* reference launch geometry, operands through L1 */
+#define TCS_VARIANT_MARCH 2  /* TMA-fed shared-memory ring, CTAs march along the slowest axis */
+
+typedef struct tcs_stencil tcs_stencil; /* opaque handle: one instantiated parameter set */
+
+/* Stencil parameter set (cuda/generate2DStencil_cuda.py:31-44, cuda/generate3DStencil_cuda.py:32-46,
+ * cuda/benchmark.h:40-47). */
+typedef struct tcs_spec {
+  int dimension;     /* 2 or 3 */
+  int neighbourhood; /* TCS_BOX | TCS_STAR */
+  int orientation;   /* TCS_ROW | TCS_COLUMN */
+  int coefficients;  /* TCS_JACOBI | TCS_VARIABLE */
+  int range;         /* >= 1 */
+  int cx, cy, cz;    /* coarsening factors >= 1 (cz ignored in 2D) */
+  int alignment;     /* TCS_ALIGN_NONE | TCS_ALIGN_READ | TCS_ALIGN_WRITE */
+  int cl_size;       /* alignment size in grid points (> 0 unless alignment is None) */
+  int precision;     /* TCS_F64 | TCS_F32 */
+} tcs_spec;
+
+/* Grid geometry after coarsening truncation and alignment padding
+ * (cuda/benchmark.cpp:262-308, cuda/benchmark.h:100-123). */
+typedef struct tcs_geometry {
+  unsigned grid[3];         /* gridSize: x = padded row pitch (xmem), y, z (1 in 2D) */
+  unsigned elements[3];     /* gridElements: updated (interior) points per axis (1 for z in 2D) */
+  unsigned threads[3];      /* gridThreads = elements / coarsening */
+  unsigned left_offset;     /* Write alignment: padding left of every row (baked into kernels) */
+  unsigned right_offset;    /* Read/Write alignment: padding right of every row */
+  unsigned long long n_points; /* N = grid[0]*grid[1]*grid[2]: elements per buffer */
+} tcs_geometry;
+
+/* Launch parameters of one sweep. */
+typedef struct tcs_launch {
+  unsigned block[3];        /* thread-block shape (z = 1 in 2D) */
+  unsigned grid_blocks[3];  /* direct variant: CTA grid; zeros = ceil(gridThreads / block) */
+  int variant;              /* TCS_VARIANT_* */
+  unsigned segments;        /* march: CTAs along the march axis per tile column (0 = auto) */
+  unsigned depth;           /* march: chunks in flight ahead of the current step (0 = auto) */
+} tcs_launch;
+
+/* Resolved launch of one sweep (what tcs_update_grid will run). */
+typedef struct tcs_plan {
+  int variant;              /* TCS_VARIANT_DIRECT or TCS_VARIANT_MARCH */
+  unsigned grid_blocks[3];
+  unsigned block[3];
+  unsigned dyn_smem;        /* dynamic shared memory per CTA in bytes */
+  unsigned seg_len;         /* march: outputs along the march axis per CTA */
+  unsigned nslot;           /* march: ring slots */
+  unsigned width;           /* march: shared-memory row width in elements */
+  unsigned depth;           /* march: chunks in flight */
+  int ctas_per_sm;          /* occupancy of the resolved kernel at this shape */
+  int num_sms;
+} tcs_plan;
+
+/* Library / error state. */
+int tcs_abi_version(void);
+const char* tcs_last_error(void);
+
+/* Host-only parameter logic (no GPU needed). */
+/* Validate a parameter set: stencilBenchmark::checkParameters (cuda/benchmark.cpp:430-491)
+ * and the generators' argv checks (cuda/generate2DStencil_cuda.py:49-60). */
+int tcs_spec_validate(const tcs_spec* spec);
+/* stencilSize and flopsPerUpdate (cuda/benchmark.cpp:62-81). */
+int tcs_stencil_size(const tcs_spec* spec, unsigned* stencil_size, unsigned* flops_per_update);
+/* Truncation to a coarsening multiple and Read/Write row padding (cuda/benchmark.cpp:142-179). */
+int tcs_compute_geometry(const tcs_spec* spec, unsigned nx, unsigned ny, unsigned nz,
+                         tcs_geometry* out);
+/* Left offset baked into Write-aligned kernels (cuda/generate2DStencil_cuda.py:83-85). */
+int tcs_left_offset(const tcs_spec* spec, unsigned* left_offset);
+
+/* Handle lifetime.  tcs_create instantiates (or loads from the cubin cache) the kernels of the
+ * parameter set on the current device; it is the equivalent of generating and building
+ * kernels.cu + launchUpdateGrid.cu (cuda/RunBenchmark.sh:118-129). */
+int tcs_create(const tcs_spec* spec, tcs_stencil** out);
+int tcs_destroy(tcs_stencil* h);
+int tcs_get_spec(const tcs_stencil* h, tcs_spec* out);
+
+/* copyMask (cuda/generateLaunchUpdateGrid.py:77-82): upload `n` <= stencilSize coefficients
+ * into the module's constant bank (converted to float for TCS_F32).  Jacobi stencils ignore it,
+ * like the reference's empty copyMask. */
+int tcs_copy_mask(tcs_stencil* h, const double* mask, unsigned n);
+
+/* maxPotentialBlockSize (cuda/generateLaunchUpdateGrid.py:84-89) of the direct kernel. */
+int tcs_max_potential_block_size(tcs_stencil* h, int* out);
+
+/* Resolve a launch without running it. */
+int tcs_plan_launch(tcs_stencil* h, const unsigned grid[3], unsigned right_offset,
+                    const tcs_launch* launch, tcs_plan* out);
+
+/* One sweep out = stencil(in) over the interior: the `updateGrid<<<gridBlocks, blockSize>>>`
+ * launch of cuda/generateLaunchUpdateGrid.py:92-100.  `grid` is the padded gridSize and
+ * `right_offset` the row padding, exactly as the reference kernel receives them.  Asynchronous
+ * on `stream`. */
+int tcs_update_grid(tcs_stencil* h, const unsigned grid[3], unsigned right_offset,
+                    const tcs_launch* launch, const void* in, void* out, void* stream);
+
+/* `n` ping-pong sweeps a -> b -> a ...; *result_in_b = 1 when the last sweep wrote b. */
+int tcs_sweeps(tcs_stencil* h, const unsigned grid[3], unsigned right_offset,
+               const tcs_launch* launch, void* a, void* b, unsigned n, void* stream,
+               int* result_in_b);
+
+/* `n` ping-pong sweeps timed with CUDA events on `stream` (synchronises); *ms = elapsed. */
+int tcs_time_sweeps(tcs_stencil* h, const unsigned grid[3], unsigned right_offset,
+                    const tcs_launch* launch, void* a, void* b, unsigned n, void* stream,
+                    float* ms);
+
+/* benchmarkUpdateGrid (cuda/launchUpdateGrid.h:13, cuda/generateLaunchUpdateGrid.py:103-147):
+ * runtime sanity check of the baked-in parameters, then the doubling loop of synchronous
+ * launches with host timestamps.  Writes up to `cap` per-launch durations [s]; *n_out is the
+ * number measured.  The ping-pong swap is local, as in the reference. */
+int tcs_benchmark_update_grid(tcs_stencil* h, const char* coeff_type, const char* neighbourhood,
+                              unsigned stencil_range, unsigned dimension, const char* alignment,
+                              double max_time, const unsigned grid[3], const unsigned block[3],
+                              const unsigned grid_blocks[3], void* d_array0, void* d_array1,
+                              unsigned right_offset, double* durations, unsigned cap,
+                              unsigned* n_out);
+
+/* launchInit (cuda/launchUpdateGrid.h:14, cuda/generateLaunchUpdateGrid.py:150-158): the
+ * reference's `init` pattern (cuda/generate2DStencil_cuda.py:321-350,
+ * cuda/generate3DStencil_cuda.py:386-430), synchronous. */
+int tcs_launch_init(tcs_stencil* h, const unsigned grid[3], const unsigned block[3],
+                    const unsigned grid_blocks[3], void* d_array, unsigned right_offset);
+
+/* Read (and optionally clear) the device status word of the handle's kernels. */
+int tcs_device_status(tcs_stencil* h, unsigned* status, int clear);
+
+/* Launch used by tcs_benchmark_update_grid (default TCS_VARIANT_AUTO with auto segments/depth;
+ * TCS_VARIANT_DIRECT reproduces the reference's own grid geometry exactly). */
+int tcs_set_dropin_launch(tcs_stencil* h, int variant, unsigned segments, unsigned depth);
+
+/* Instantiate the kernels of a parameter set into the cubin cache without a GPU (NVRTC only);
+ * writes the cache path.  Used by the build step so GPU runs start warm. */
+int tcs_precompile(const tcs_spec* spec, char* cubin_path, unsigned path_cap);
+
+/* Number of SMs of the current device. */
+int tcs_device_sm_count(int* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TCS_H */

@@ -1,0 +1,85 @@
+"""The engine's kernel arithmetic and addressing, checked on the CPU.
+
+* tcs_tile.cuh (the per-thread arithmetic every sweep kernel runs) is compiled for the host and
+  compared bit for bit with the reference fixtures and with the oracle on random parameter sets.
+* The march kernel's TMA/ring addressing is replayed by tests/march_model.py for many shapes.
+"""
+
+import numpy as np
+import pytest
+
+import host_tile
+import march_model
+import oracle as O
+from oracle import ref_configs
+from make_golden import fixture_input, HERE as GOLDEN
+
+
+@pytest.mark.parametrize("cfg", ref_configs.PARITY, ids=ref_configs.key)
+def test_kernel_arithmetic_matches_reference_fixture(cfg):
+    f = np.load(GOLDEN / ("%s.npz" % ref_configs.key(cfg)))
+    spec, raw, g, a, mask = fixture_input(cfg, int(f["seed"]))
+    out = host_tile.sweeps(cfg, a, g.grid, g.left_offset, g.right_offset, int(f["nsweeps"]), mask)
+    assert np.array_equal(out, f["out"])
+
+
+def _random_cfgs(n, seed):
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        d = int(rng.integers(2, 4))
+        r = int(rng.integers(1, 4 if d == 3 else 6))
+        c = [int(v) for v in rng.integers(1, 4, size=3)]
+        al = ["None", "Read", "Write"][int(rng.integers(0, 3))]
+        cl = 0 if al == "None" else int(rng.choice([4, 8, 16]))
+        out.append((d, ["Box", "Star"][int(rng.integers(0, 2))], ["Row", "Column"][int(rng.integers(0, 2))],
+                    ["Jacobi", "Variable"][int(rng.integers(0, 2))], r, c[0], c[1], c[2] if d == 3 else 1, al, cl))
+    return out
+
+
+@pytest.mark.parametrize("precision", ["f64", "f32"])
+@pytest.mark.parametrize("cfg", _random_cfgs(8, 11), ids=ref_configs.key)
+def test_kernel_arithmetic_matches_oracle_random(cfg, precision):
+    d, sh, o, c, r, cx, cy, cz, al, cl = cfg
+    spec = O.make_spec(*cfg)
+    n = (20 + 2 * r, 17 + 2 * r, 13 + 2 * r)
+    g = O.geometry(spec, *n)
+    rng = np.random.default_rng(5)
+    shape = (g.grid[1], g.grid[0]) if d == 2 else (g.grid[2], g.grid[1], g.grid[0])
+    dt = np.float64 if precision == "f64" else np.float32
+    a = rng.random(shape).astype(dt)
+    mask = rng.standard_normal(O.stencil_size(spec)) if c == "Variable" else None
+    want = O.sweeps(spec, a, 2, g.right_offset, mask)
+    got = host_tile.sweeps(cfg, a, g.grid, g.left_offset, g.right_offset, 2, mask, precision)
+    assert np.array_equal(got, want)
+
+
+MARCH_CASES = [
+    (2, "Box", 1, (1, 1, 1), (32, 4, 1), (40, 30, 1), "None", 0),
+    (2, "Box", 1, (1, 1, 1), (64, 1, 1), (70, 11, 1), "None", 0),
+    (2, "Star", 3, (2, 1, 1), (16, 2, 1), (61, 45, 1), "Write", 8),
+    (2, "Box", 2, (3, 2, 1), (8, 4, 1), (53, 40, 1), "Read", 16),
+    (2, "Box", 6, (2, 2, 1), (16, 2, 1), (60, 33, 1), "None", 0),
+    (2, "Star", 1, (1, 1, 1), (1, 32, 1), (12, 80, 1), "Write", 16),
+    (3, "Star", 4, (1, 1, 1), (32, 4, 1), (40, 30, 28), "Read", 16),
+    (3, "Star", 4, (2, 2, 1), (16, 4, 1), (44, 29, 21), "Read", 16),
+    (3, "Star", 2, (2, 2, 2), (8, 4, 2), (31, 29, 27), "None", 0),
+    (3, "Box", 1, (1, 3, 1), (16, 2, 3), (35, 26, 22), "Write", 16),
+    (3, "Box", 2, (1, 1, 2), (8, 8, 1), (22, 21, 20), "None", 0),
+]
+
+
+@pytest.mark.parametrize("case", MARCH_CASES, ids=lambda c: "%dD_%s_r%d_c%s_b%s" % (c[0], c[1], c[2], c[3], c[4]))
+@pytest.mark.parametrize("es", [8, 4])
+def test_march_addressing_model(case, es):
+    d, sh, r, c, blk, n, al, cl = case
+    spec = O.make_spec(d, sh, "Row", "Jacobi", r, c[0], c[1], c[2], al, cl)
+    g = O.geometry(spec, *n)
+    grid = g.grid
+    if (grid[0] * es) % 16:
+        grid = (grid[0] + (16 // es - grid[0] % (16 // es)), grid[1], grid[2])  # pitch rule of the planner
+    for seg in (0, 1, 3):
+        for depth in (0, 1, 3):
+            cnt = march_model.simulate(d, sh, r, c, blk, grid, g.left_offset, g.right_offset, al != "None", es=es,
+                                       segments=seg, depth=depth, num_sms=5)
+            assert cnt is None or cnt > 0

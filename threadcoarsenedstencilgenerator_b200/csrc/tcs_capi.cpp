@@ -1,0 +1,919 @@
+// Host half of the B200 stencil engine: the C ABI declared in include/tcs.h.
+//
+// One `tcs_stencil` handle = one stencil parameter set.  tcs_create instantiates the kernel
+// templates of tcs_kernels.cuh for that set with NVRTC (sm_100a cubin, cached on disk keyed by
+// a hash of source + options) and loads the module with the CUDA driver API, reached through
+// cudaGetDriverEntryPoint so that the library itself links only the static CUDA runtime and
+// NVRTC and loads on machines without a GPU driver (host-only entry points work there).
+//
+// Reference behaviour mirrored here (file:line in the reference project):
+//   parameter checks          cuda/benchmark.cpp:430-491, cuda/generate2DStencil_cuda.py:49-60
+//   stencilSize / flops       cuda/benchmark.cpp:62-81
+//   geometry                  cuda/benchmark.cpp:142-179, cuda/benchmark.h:100-123
+//   copyMask                  cuda/generateLaunchUpdateGrid.py:77-82
+//   maxPotentialBlockSize     cuda/generateLaunchUpdateGrid.py:84-89
+//   benchmarkUpdateGrid       cuda/generateLaunchUpdateGrid.py:103-147
+//   launchInit                cuda/generateLaunchUpdateGrid.py:150-158
+
+#include "tcs.h"
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <dlfcn.h>
+#include <nvrtc.h>
+#include <sys/stat.h>
+#include <unistd.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <mutex>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "tcs_kernels_src.inc"  // tcs_kernels_src[], tcs_tile_src[]: the device headers
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+
+// ---- driver API through the runtime's entry-point query --------------------------------------
+struct Driver {
+  decltype(&cuModuleLoadData) ModuleLoadData = nullptr;
+  decltype(&cuModuleUnload) ModuleUnload = nullptr;
+  decltype(&cuModuleGetFunction) ModuleGetFunction = nullptr;
+  decltype(&cuModuleGetGlobal) ModuleGetGlobal = nullptr;
+  decltype(&cuFuncSetAttribute) FuncSetAttribute = nullptr;
+  decltype(&cuFuncGetAttribute) FuncGetAttribute = nullptr;
+  decltype(&cuLaunchKernel) LaunchKernel = nullptr;
+  decltype(&cuTensorMapEncodeTiled) TensorMapEncodeTiled = nullptr;
+  decltype(&cuOccupancyMaxActiveBlocksPerMultiprocessor) OccMaxActive = nullptr;
+  decltype(&cuOccupancyMaxPotentialBlockSize) OccMaxPotential = nullptr;
+  decltype(&cuGetErrorString) GetErrorString = nullptr;
+  bool ok = false;
+  std::string why;
+};
+
+Driver g_drv;
+std::once_flag g_drv_once;
+
+template <class F>
+bool entry(const char* name, F& fn, std::string& why) {
+  void* p = nullptr;
+  cudaDriverEntryPointQueryResult q;
+  cudaError_t e = cudaGetDriverEntryPoint(name, &p, cudaEnableDefault, &q);
+  if (e != cudaSuccess || q != cudaDriverEntryPointSuccess || p == nullptr) {
+    why = std::string("driver entry point unavailable: ") + name;
+    return false;
+  }
+  fn = reinterpret_cast<F>(p);
+  return true;
+}
+
+void load_driver() {
+  Driver d;
+  bool ok = entry("cuModuleLoadData", d.ModuleLoadData, d.why) &&
+            entry("cuModuleUnload", d.ModuleUnload, d.why) &&
+            entry("cuModuleGetFunction", d.ModuleGetFunction, d.why) &&
+            entry("cuModuleGetGlobal", d.ModuleGetGlobal, d.why) &&
+            entry("cuFuncSetAttribute", d.FuncSetAttribute, d.why) &&
+            entry("cuFuncGetAttribute", d.FuncGetAttribute, d.why) &&
+            entry("cuLaunchKernel", d.LaunchKernel, d.why) &&
+            entry("cuTensorMapEncodeTiled", d.TensorMapEncodeTiled, d.why) &&
+            entry("cuOccupancyMaxActiveBlocksPerMultiprocessor", d.OccMaxActive, d.why) &&
+            entry("cuOccupancyMaxPotentialBlockSize", d.OccMaxPotential, d.why) &&
+            entry("cuGetErrorString", d.GetErrorString, d.why);
+  d.ok = ok;
+  g_drv = d;
+}
+
+std::string cu_msg(CUresult r) {
+  const char* s = nullptr;
+  if (g_drv.GetErrorString) g_drv.GetErrorString(r, &s);
+  return s ? std::string(s) : ("CUresult " + std::to_string((int)r));
+}
+
+#define TCS_CU(call)                                                                    \
+  do {                                                                                  \
+    CUresult r_ = (call);                                                               \
+    if (r_ != CUDA_SUCCESS) return fail(TCS_ERR_CUDA, std::string(#call ": ") + cu_msg(r_)); \
+  } while (0)
+
+#define TCS_RT(call)                                                                       \
+  do {                                                                                     \
+    cudaError_t e_ = (call);                                                               \
+    if (e_ != cudaSuccess)                                                                 \
+      return fail(TCS_ERR_CUDA, std::string(#call ": ") + cudaGetErrorString(e_));         \
+  } while (0)
+
+// Make sure a device exists, the primary context is current and the driver table is loaded.
+int ensure_cuda() {
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess || n == 0) {
+    cudaGetLastError();
+    return fail(TCS_ERR_NO_DEVICE, std::string("no CUDA device: ") + cudaGetErrorString(e));
+  }
+  TCS_RT(cudaFree(nullptr));
+  std::call_once(g_drv_once, load_driver);
+  if (!g_drv.ok) return fail(TCS_ERR_CUDA, g_drv.why);
+  return TCS_OK;
+}
+
+// ---- parameter logic -------------------------------------------------------------------------
+int validate(const tcs_spec* s) {
+  if (!s) return fail(TCS_ERR_INVALID_VALUE, "spec is NULL");
+  if (s->dimension != 2 && s->dimension != 3)
+    return fail(TCS_ERR_INVALID_VALUE, "Unknown dimension: either 2D or 3D");
+  if (s->neighbourhood != TCS_BOX && s->neighbourhood != TCS_STAR)
+    return fail(TCS_ERR_INVALID_VALUE, "Unknown stencil-neighbourhood: either 'Box' or 'Star'");
+  if (s->orientation != TCS_ROW && s->orientation != TCS_COLUMN)
+    return fail(TCS_ERR_INVALID_VALUE, "Unknown orientation: either 'Row' or 'Column'");
+  if (s->coefficients != TCS_JACOBI && s->coefficients != TCS_VARIABLE)
+    return fail(TCS_ERR_INVALID_VALUE, "Unknown coefficients: either 'Jacobi' or 'Variable'");
+  if (s->range < 1) return fail(TCS_ERR_INVALID_VALUE, "Stencil range must be greater than zero");
+  if (s->cx < 1 || s->cy < 1 || (s->dimension == 3 && s->cz < 1))
+    return fail(TCS_ERR_INVALID_VALUE, "Coarsening factors have to be greater than zero");
+  if (s->alignment != TCS_ALIGN_NONE && s->alignment != TCS_ALIGN_READ &&
+      s->alignment != TCS_ALIGN_WRITE)
+    return fail(TCS_ERR_INVALID_VALUE, "Unknown alignment: either 'None', 'Write' or 'Read'");
+  if (s->alignment != TCS_ALIGN_NONE && s->cl_size <= 0)
+    return fail(TCS_ERR_INVALID_VALUE, "size of alignment has to be > 0 when alignment is given");
+  if (s->precision != TCS_F64 && s->precision != TCS_F32)
+    return fail(TCS_ERR_INVALID_VALUE, "Unknown precision");
+  // Practical limits of one instantiation (the reference has none but its unrolled code
+  // stops compiling long before these).
+  if (s->range > 16) return fail(TCS_ERR_INVALID_VALUE, "range > 16 is not supported");
+  const int cz = s->dimension == 3 ? s->cz : 1;
+  if (s->cx > 16 || s->cy > 16 || cz > 16 || s->cx * s->cy * cz > 512)
+    return fail(TCS_ERR_INVALID_VALUE, "coarsening tile too large (per axis <= 16, product <= 512)");
+  return TCS_OK;
+}
+
+unsigned stencil_size_of(const tcs_spec& s) {
+  const unsigned w = 2u * s.range + 1u;
+  if (s.neighbourhood == TCS_BOX) return s.dimension == 2 ? w * w : w * w * w;
+  return 2u * s.dimension * s.range + 1u;
+}
+
+unsigned left_offset_of(const tcs_spec& s) {
+  if (s.alignment != TCS_ALIGN_WRITE) return 0;
+  const unsigned cl = (unsigned)s.cl_size, r = (unsigned)s.range;
+  return (r % cl != 0) ? cl - r % cl : 0;
+}
+
+const char* coeff_str(int c) { return c == TCS_JACOBI ? "Jacobi" : "Variable"; }
+const char* shape_str(int s) { return s == TCS_BOX ? "Box" : "Star"; }
+const char* align_str(int a) {
+  return a == TCS_ALIGN_NONE ? "None" : (a == TCS_ALIGN_READ ? "Read" : "Write");
+}
+
+// ---- NVRTC instantiation with an on-disk cubin cache -----------------------------------------
+uint64_t fnv1a(const std::string& s, uint64_t h = 1469598103934665603ull) {
+  for (unsigned char c : s) {
+    h ^= c;
+    h *= 1099511628211ull;
+  }
+  return h;
+}
+
+std::string library_dir() {
+  Dl_info info;
+  if (dladdr(reinterpret_cast<void*>(&tcs_abi_version), &info) && info.dli_fname) {
+    std::string p(info.dli_fname);
+    const size_t k = p.find_last_of('/');
+    if (k != std::string::npos) return p.substr(0, k);
+  }
+  return ".";
+}
+
+std::string cache_dir() {
+  const char* env = std::getenv("TCS_KCACHE");
+  std::string d = (env && *env) ? std::string(env) : library_dir() + "/_kcache";
+  mkdir(d.c_str(), 0775);
+  return d;
+}
+
+std::string instance_macros(const tcs_spec& s) {
+  std::ostringstream m;
+  m << "#define TCS_T " << (s.precision == TCS_F64 ? "double" : "float") << "\n"
+    << "#define TCS_DIM " << s.dimension << "\n"
+    << "#define TCS_SHAPE " << s.neighbourhood << "\n"
+    << "#define TCS_ORIENT " << s.orientation << "\n"
+    << "#define TCS_COEFF " << s.coefficients << "\n"
+    << "#define TCS_R " << s.range << "\n"
+    << "#define TCS_CX " << s.cx << "\n"
+    << "#define TCS_CY " << s.cy << "\n"
+    << "#define TCS_CZ " << (s.dimension == 3 ? s.cz : 1) << "\n";
+  return m.str();
+}
+
+std::mutex g_compile_mu;
+
+int instantiate(const tcs_spec& s, std::vector<char>& cubin, std::string* path_out) {
+  const std::string src = instance_macros(s) + "#include \"tcs_kernels.cuh\"\n";
+  const char* opts[] = {"--gpu-architecture=sm_100a", "--std=c++17", "--fmad=false",
+                        "-lineinfo", "--device-as-default-execution-space"};
+  const int nopts = sizeof(opts) / sizeof(opts[0]);
+  int major = 0, minor = 0;
+  nvrtcVersion(&major, &minor);
+  std::string keysrc = src + "\x01" + tcs_kernels_src + "\x01" + tcs_tile_src + "\x01" +
+                       std::to_string(major) + "." + std::to_string(minor);
+  for (int i = 0; i < nopts; ++i) keysrc += std::string("\x02") + opts[i];
+  char key[32];
+  std::snprintf(key, sizeof(key), "%016llx", (unsigned long long)fnv1a(keysrc));
+  const std::string path = cache_dir() + "/tcs_" + key + ".cubin";
+  if (path_out) *path_out = path;
+
+  std::lock_guard<std::mutex> lock(g_compile_mu);
+  {
+    std::ifstream f(path, std::ios::binary);
+    if (f) {
+      cubin.assign(std::istreambuf_iterator<char>(f), std::istreambuf_iterator<char>());
+      if (!cubin.empty()) return TCS_OK;
+    }
+  }
+  nvrtcProgram prog;
+  const char* hdrs[] = {tcs_kernels_src, tcs_tile_src};
+  const char* hdr_names[] = {"tcs_kernels.cuh", "tcs_tile.cuh"};
+  nvrtcResult r = nvrtcCreateProgram(&prog, src.c_str(), "tcs_instance.cu", 2, hdrs, hdr_names);
+  if (r != NVRTC_SUCCESS) return fail(TCS_ERR_COMPILE, nvrtcGetErrorString(r));
+  r = nvrtcCompileProgram(prog, nopts, opts);
+  if (r != NVRTC_SUCCESS) {
+    size_t n = 0;
+    nvrtcGetProgramLogSize(prog, &n);
+    std::string log(n, '\0');
+    nvrtcGetProgramLog(prog, &log[0]);
+    nvrtcDestroyProgram(&prog);
+    return fail(TCS_ERR_COMPILE, "NVRTC: " + log);
+  }
+  size_t n = 0;
+  nvrtcGetCUBINSize(prog, &n);
+  cubin.resize(n);
+  nvrtcGetCUBIN(prog, cubin.data());
+  nvrtcDestroyProgram(&prog);
+  // atomic publish into the cache
+  const std::string tmp = path + ".tmp." + std::to_string((long long)getpid());
+  {
+    std::ofstream f(tmp, std::ios::binary);
+    f.write(cubin.data(), (std::streamsize)cubin.size());
+  }
+  std::rename(tmp.c_str(), path.c_str());
+  return TCS_OK;
+}
+
+// Host mirror of the device TcsGeo (same layout).
+struct TcsGeo {
+  unsigned long long xdim, ydim, zdim;
+  unsigned x0, x_lim;
+  unsigned y_lim, z_lim;
+  unsigned seg;
+  unsigned nslot;
+  unsigned width;
+  unsigned pad_;
+};
+static_assert(sizeof(TcsGeo) == 56, "TcsGeo layout");
+
+struct MapEntry {
+  const void* ptr;
+  unsigned long long dims[3];
+  unsigned box[3];
+  CUtensorMap map;
+};
+
+}  // namespace
+
+struct tcs_stencil {
+  tcs_spec spec{};
+  unsigned S = 0, flops = 0, left_off = 0;
+  int device = 0;
+  int num_sms = 0;
+  int smem_optin = 0;
+  CUmodule mod = nullptr;
+  CUfunction f_direct = nullptr, f_march = nullptr, f_init = nullptr;
+  CUdeviceptr mask_ptr = 0;
+  size_t mask_bytes = 0;
+  CUdeviceptr status_ptr = 0;
+  int march_smem_attr = 0;
+  int dropin_variant = TCS_VARIANT_AUTO;  // variant used by tcs_benchmark_update_grid
+  unsigned dropin_segments = 0, dropin_depth = 0;
+  std::mutex mu;
+  std::vector<MapEntry> maps;
+};
+
+namespace {
+
+struct Resolved {
+  int variant = 0;
+  TcsGeo geo{};
+  unsigned grid[3] = {1, 1, 1};
+  unsigned block[3] = {1, 1, 1};
+  unsigned smem = 0;
+  unsigned depth = 0;
+  unsigned box[3] = {1, 1, 1};
+  int occ = 0;
+};
+
+int elem_size(const tcs_spec& s) { return s.precision == TCS_F64 ? 8 : 4; }
+
+// Interior geometry from the reference-style (gridSize, rightOffset) pair.
+int make_geo(const tcs_stencil* h, const unsigned grid[3], unsigned right_offset, TcsGeo& g) {
+  const tcs_spec& s = h->spec;
+  const unsigned R = (unsigned)s.range;
+  if (!grid) return fail(TCS_ERR_INVALID_VALUE, "grid is NULL");
+  const unsigned ro = (s.alignment == TCS_ALIGN_NONE) ? 0u : right_offset;
+  const unsigned long long xdim = grid[0], ydim = grid[1];
+  const unsigned long long zdim = (s.dimension == 3) ? grid[2] : 1ull;
+  if (xdim < 2ull * R + h->left_off + ro || ydim < 2ull * R || (s.dimension == 3 && zdim < 2ull * R))
+    return fail(TCS_ERR_INVALID_VALUE, "grid smaller than twice the stencil range plus padding");
+  if (xdim > 0xffffffffull || ydim > 0xffffffffull || zdim > 0xffffffffull)
+    return fail(TCS_ERR_INVALID_VALUE, "grid extent exceeds 32 bits");
+  g = TcsGeo{};
+  g.xdim = xdim;
+  g.ydim = ydim;
+  g.zdim = zdim;
+  g.x0 = R + h->left_off;
+  g.x_lim = (unsigned)(xdim - R - ro);
+  g.y_lim = (unsigned)(ydim - R);
+  g.z_lim = (unsigned)(zdim - (s.dimension == 3 ? R : 0));
+  return TCS_OK;
+}
+
+int check_block(const tcs_stencil* h, const unsigned b[3]) {
+  if (b[0] < 1 || b[1] < 1 || b[2] < 1) return fail(TCS_ERR_INVALID_VALUE, "block dimension of 0");
+  if (h->spec.dimension == 2 && b[2] != 1)
+    return fail(TCS_ERR_INVALID_VALUE, "2D stencils take a block with z = 1");
+  if (b[0] > 1024 || b[1] > 1024 || b[2] > 64 || (unsigned long long)b[0] * b[1] * b[2] > 1024)
+    return fail(TCS_ERR_INVALID_VALUE, "block exceeds the device thread-block limits");
+  return TCS_OK;
+}
+
+unsigned cdiv(unsigned long long a, unsigned long long b) { return (unsigned)((a + b - 1) / b); }
+
+int resolve_direct(tcs_stencil* h, const TcsGeo& g, const tcs_launch* L, Resolved& out) {
+  const tcs_spec& s = h->spec;
+  const unsigned cz = s.dimension == 3 ? (unsigned)s.cz : 1u;
+  int maxthr = 0;
+  TCS_CU(g_drv.FuncGetAttribute(&maxthr, CU_FUNC_ATTRIBUTE_MAX_THREADS_PER_BLOCK, h->f_direct));
+  const unsigned long long nthr = (unsigned long long)L->block[0] * L->block[1] * L->block[2];
+  if (nthr > (unsigned long long)maxthr)
+    return fail(TCS_ERR_UNSUPPORTED, "block has more threads than the direct kernel supports (" +
+                                         std::to_string(maxthr) + ")");
+  out.variant = TCS_VARIANT_DIRECT;
+  out.geo = g;
+  for (int i = 0; i < 3; ++i) out.block[i] = L->block[i];
+  if (L->grid_blocks[0] && L->grid_blocks[1] && L->grid_blocks[2]) {
+    for (int i = 0; i < 3; ++i) out.grid[i] = L->grid_blocks[i];
+  } else {
+    const unsigned long long ex = g.x_lim > g.x0 ? g.x_lim - g.x0 : 0;
+    const unsigned long long ey = g.y_lim - s.range;
+    const unsigned long long ez = s.dimension == 3 ? g.z_lim - s.range : 1;
+    const unsigned long long tx = ex / s.cx, ty = ey / s.cy, tz = s.dimension == 3 ? ez / cz : 1;
+    out.grid[0] = std::max(1u, cdiv(tx, L->block[0]));
+    out.grid[1] = std::max(1u, cdiv(ty, L->block[1]));
+    out.grid[2] = std::max(1u, cdiv(tz, L->block[2]));
+  }
+  if (out.grid[1] > 65535 || out.grid[2] > 65535)
+    return fail(TCS_ERR_UNSUPPORTED, "direct launch grid exceeds 65535 blocks in y or z");
+  int occ = 0;
+  TCS_CU(g_drv.OccMaxActive(&occ, h->f_direct, (int)nthr, 0));
+  out.occ = occ;
+  out.smem = 0;
+  return TCS_OK;
+}
+
+int resolve_march(tcs_stencil* h, const TcsGeo& g, const tcs_launch* L, Resolved& out) {
+  const tcs_spec& s = h->spec;
+  const unsigned R = (unsigned)s.range;
+  const unsigned es = (unsigned)elem_size(s);
+  const unsigned vec = 16u / es;
+  const unsigned cz = s.dimension == 3 ? (unsigned)s.cz : 1u;
+  if ((g.xdim * es) % 16 != 0)
+    return fail(TCS_ERR_UNSUPPORTED, "row pitch is not a multiple of 16 bytes (TMA stride rule)");
+  const unsigned TX = L->block[0] * s.cx;
+  const unsigned W = ((TX + 2 * R + vec - 1 + vec - 1) / vec) * vec;
+  unsigned STEP, rows;
+  if (s.dimension == 2) {
+    STEP = L->block[1] * s.cy;
+    rows = 1;
+  } else {
+    STEP = L->block[2] * cz;
+    rows = L->block[1] * s.cy + 2 * R;
+  }
+  if (W > 256 || STEP > 256 || rows > 256)
+    return fail(TCS_ERR_UNSUPPORTED, "tile exceeds the 256-element TMA box limit");
+  const unsigned plane = W * rows;
+  const unsigned chunk_bytes = STEP * plane * es;
+  const unsigned K = 1 + (2 * R + STEP - 1) / STEP;
+  unsigned depth = L->depth;
+  if (depth == 0) depth = std::max(1u, std::min(4u, cdiv(16384, chunk_bytes)));
+  unsigned smem = 0, nslot = 0;
+  for (;;) {
+    nslot = K + depth;
+    smem = ((nslot * 8 + 127) / 128) * 128 + nslot * chunk_bytes;
+    if (smem <= (unsigned)h->smem_optin || depth == 1) break;
+    --depth;
+  }
+  if (smem > (unsigned)h->smem_optin)
+    return fail(TCS_ERR_UNSUPPORTED, "ring does not fit in shared memory (" +
+                                         std::to_string(smem) + " bytes)");
+  const int nthr = (int)(L->block[0] * L->block[1] * L->block[2]);
+  int maxthr = 0;
+  TCS_CU(g_drv.FuncGetAttribute(&maxthr, CU_FUNC_ATTRIBUTE_MAX_THREADS_PER_BLOCK, h->f_march));
+  if (nthr > maxthr)
+    return fail(TCS_ERR_UNSUPPORTED, "block has more threads than the march kernel supports (" +
+                                         std::to_string(maxthr) + ")");
+  {
+    std::lock_guard<std::mutex> lock(h->mu);
+    if ((int)smem > h->march_smem_attr) {
+      TCS_CU(g_drv.FuncSetAttribute(h->f_march, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES,
+                                    (int)smem));
+      h->march_smem_attr = (int)smem;
+    }
+  }
+  int occ = 0;
+  TCS_CU(g_drv.OccMaxActive(&occ, h->f_march, nthr, smem));
+  if (occ < 1) return fail(TCS_ERR_UNSUPPORTED, "march kernel cannot be resident at this shape");
+
+  const unsigned long long ex = g.x_lim > g.x0 ? g.x_lim - g.x0 : 0;
+  const unsigned long long ey = g.y_lim - R;
+  const unsigned nxt = std::max(1u, cdiv(ex, TX));
+  unsigned nyt = 1;
+  unsigned long long M = ey;
+  if (s.dimension == 3) {
+    nyt = std::max(1u, cdiv(ey, (unsigned long long)L->block[1] * s.cy));
+    M = g.z_lim - R;
+  }
+  unsigned nseg = L->segments;
+  if (nseg == 0) {
+    const unsigned long long slots = (unsigned long long)h->num_sms * (unsigned)occ;
+    const unsigned long long tiles = (unsigned long long)nxt * nyt;
+    nseg = (unsigned)std::max<unsigned long long>(1, slots / std::max<unsigned long long>(1, tiles));
+  }
+  const unsigned max_seg = std::max(1u, cdiv(M, STEP));
+  nseg = std::min(nseg, max_seg);
+  unsigned seg = cdiv(std::max<unsigned long long>(M, 1), nseg);
+  seg = cdiv(seg, STEP) * STEP;
+  nseg = std::max(1u, cdiv(std::max<unsigned long long>(M, 1), seg));
+
+  out.variant = TCS_VARIANT_MARCH;
+  out.geo = g;
+  out.geo.seg = seg;
+  out.geo.nslot = nslot;
+  out.geo.width = W;
+  for (int i = 0; i < 3; ++i) out.block[i] = L->block[i];
+  if (s.dimension == 2) {
+    out.grid[0] = nxt;
+    out.grid[1] = nseg;
+    out.grid[2] = 1;
+    out.box[0] = W;
+    out.box[1] = STEP;
+    out.box[2] = 1;
+  } else {
+    out.grid[0] = nxt;
+    out.grid[1] = nyt;
+    out.grid[2] = nseg;
+    out.box[0] = W;
+    out.box[1] = rows;
+    out.box[2] = STEP;
+  }
+  if (out.grid[1] > 65535 || out.grid[2] > 65535)
+    return fail(TCS_ERR_UNSUPPORTED, "march launch grid exceeds 65535 blocks in y or z");
+  out.smem = smem;
+  out.depth = depth;
+  out.occ = occ;
+  return TCS_OK;
+}
+
+int resolve(tcs_stencil* h, const unsigned grid[3], unsigned right_offset, const tcs_launch* L,
+            Resolved& out) {
+  if (!h || !L) return fail(TCS_ERR_INVALID_VALUE, "NULL handle or launch");
+  TcsGeo g;
+  int rc = make_geo(h, grid, right_offset, g);
+  if (rc) return rc;
+  rc = check_block(h, L->block);
+  if (rc) return rc;
+  if (L->variant == TCS_VARIANT_DIRECT) return resolve_direct(h, g, L, out);
+  if (L->variant == TCS_VARIANT_MARCH) return resolve_march(h, g, L, out);
+  if (L->variant != TCS_VARIANT_AUTO) return fail(TCS_ERR_INVALID_VALUE, "unknown variant");
+  const std::string saved = g_err;
+  rc = resolve_march(h, g, L, out);
+  if (rc == TCS_OK) return rc;
+  if (rc != TCS_ERR_UNSUPPORTED) return rc;
+  g_err = saved;
+  return resolve_direct(h, g, L, out);
+}
+
+int tensor_map(tcs_stencil* h, const void* ptr, const Resolved& r, CUtensorMap** out) {
+  std::lock_guard<std::mutex> lock(h->mu);
+  const unsigned long long dims[3] = {r.geo.xdim, r.geo.ydim, r.geo.zdim};
+  for (auto& m : h->maps) {
+    if (m.ptr == ptr && std::memcmp(m.dims, dims, sizeof(dims)) == 0 &&
+        std::memcmp(m.box, r.box, sizeof(r.box)) == 0) {
+      *out = &m.map;
+      return TCS_OK;
+    }
+  }
+  if (reinterpret_cast<uintptr_t>(ptr) % 16 != 0)
+    return fail(TCS_ERR_INVALID_VALUE, "input buffer is not 16-byte aligned (TMA rule)");
+  const tcs_spec& s = h->spec;
+  const unsigned es = (unsigned)elem_size(s);
+  MapEntry e;
+  e.ptr = ptr;
+  std::memcpy(e.dims, dims, sizeof(dims));
+  std::memcpy(e.box, r.box, sizeof(r.box));
+  const cuuint32_t rank = (cuuint32_t)s.dimension;
+  cuuint64_t gdim[3] = {dims[0], dims[1], dims[2]};
+  cuuint64_t gstride[2] = {dims[0] * es, dims[0] * dims[1] * es};
+  cuuint32_t box[3] = {r.box[0], r.box[1], r.box[2]};
+  cuuint32_t estride[3] = {1, 1, 1};
+  CUresult cr = g_drv.TensorMapEncodeTiled(
+      &e.map, s.precision == TCS_F64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
+      rank, const_cast<void*>(ptr), gdim, gstride, box, estride, CU_TENSOR_MAP_INTERLEAVE_NONE,
+      CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (cr != CUDA_SUCCESS) return fail(TCS_ERR_CUDA, "cuTensorMapEncodeTiled: " + cu_msg(cr));
+  if (h->maps.size() > 64) h->maps.erase(h->maps.begin());
+  h->maps.push_back(e);
+  *out = &h->maps.back().map;
+  return TCS_OK;
+}
+
+int launch_resolved(tcs_stencil* h, const Resolved& r, const void* in, void* out, CUstream st) {
+  if (!in || !out) return fail(TCS_ERR_INVALID_VALUE, "NULL device buffer");
+  if (in == out) return fail(TCS_ERR_INVALID_VALUE, "input and output must be distinct buffers");
+  TcsGeo geo = r.geo;
+  if (r.variant == TCS_VARIANT_DIRECT) {
+    CUdeviceptr pin = (CUdeviceptr)in, pout = (CUdeviceptr)out;
+    void* args[] = {&pin, &pout, &geo};
+    TCS_CU(g_drv.LaunchKernel(h->f_direct, r.grid[0], r.grid[1], r.grid[2], r.block[0],
+                              r.block[1], r.block[2], 0, st, args, nullptr));
+    return TCS_OK;
+  }
+  CUtensorMap* map = nullptr;
+  int rc = tensor_map(h, in, r, &map);
+  if (rc) return rc;
+  CUtensorMap mcopy = *map;
+  CUdeviceptr pout = (CUdeviceptr)out;
+  void* args[] = {&mcopy, &pout, &geo};
+  TCS_CU(g_drv.LaunchKernel(h->f_march, r.grid[0], r.grid[1], r.grid[2], r.block[0], r.block[1],
+                            r.block[2], r.smem, st, args, nullptr));
+  return TCS_OK;
+}
+
+}  // namespace
+
+// =============================================================================================
+extern "C" {
+
+int tcs_abi_version(void) { return TCS_ABI_VERSION; }
+
+const char* tcs_last_error(void) { return g_err.c_str(); }
+
+int tcs_spec_validate(const tcs_spec* spec) { return validate(spec); }
+
+int tcs_stencil_size(const tcs_spec* spec, unsigned* stencil_size, unsigned* flops_per_update) {
+  int rc = validate(spec);
+  if (rc) return rc;
+  const unsigned S = stencil_size_of(*spec);
+  if (stencil_size) *stencil_size = S;
+  if (flops_per_update) *flops_per_update = spec->coefficients == TCS_JACOBI ? S : 2 * S - 1;
+  return TCS_OK;
+}
+
+int tcs_left_offset(const tcs_spec* spec, unsigned* left_offset) {
+  int rc = validate(spec);
+  if (rc) return rc;
+  if (left_offset) *left_offset = left_offset_of(*spec);
+  return TCS_OK;
+}
+
+int tcs_compute_geometry(const tcs_spec* spec, unsigned nx, unsigned ny, unsigned nz,
+                         tcs_geometry* out) {
+  int rc = validate(spec);
+  if (rc) return rc;
+  if (!out) return fail(TCS_ERR_INVALID_VALUE, "geometry output is NULL");
+  const tcs_spec& s = *spec;
+  const unsigned R = (unsigned)s.range;
+  const bool d3 = s.dimension == 3;
+  if (nx == 0 || ny == 0 || (d3 && nz == 0))
+    return fail(TCS_ERR_INVALID_VALUE, "Grid dimensions have to be greater than zero");
+  if (nx < 2 * R || ny < 2 * R || (d3 && nz < 2 * R))
+    return fail(TCS_ERR_INVALID_VALUE, "grid smaller than twice the stencil range");
+  tcs_geometry g{};
+  const unsigned c[3] = {(unsigned)s.cx, (unsigned)s.cy, d3 ? (unsigned)s.cz : 1u};
+  const unsigned n[3] = {nx, ny, d3 ? nz : 1u};
+  for (int i = 0; i < 3; ++i) {
+    if (i == 2 && !d3) {
+      g.grid[2] = 1;
+      g.elements[2] = 1;
+      g.threads[2] = 1;
+      continue;
+    }
+    g.grid[i] = n[i] - (n[i] - 2 * R) % c[i];
+    g.elements[i] = g.grid[i] - 2 * R;
+    g.threads[i] = g.elements[i] / c[i];
+  }
+  unsigned long long xmem = g.grid[0];
+  unsigned right = 0, left = 0;
+  const unsigned long long cl = (unsigned long long)s.cl_size;
+  if (s.alignment == TCS_ALIGN_WRITE) {
+    left = left_offset_of(s);
+    xmem += left;
+    if (xmem % cl != 0) right = (unsigned)(cl - xmem % cl);
+    xmem += right;
+  } else if (s.alignment == TCS_ALIGN_READ) {
+    if (xmem % cl != 0) right = (unsigned)(cl - xmem % cl);
+    xmem += right;
+  }
+  if (xmem > 0xffffffffull) return fail(TCS_ERR_INVALID_VALUE, "padded row exceeds 32 bits");
+  g.grid[0] = (unsigned)xmem;
+  g.left_offset = left;
+  g.right_offset = right;
+  g.n_points = (unsigned long long)g.grid[0] * g.grid[1] * g.grid[2];
+  *out = g;
+  return TCS_OK;
+}
+
+int tcs_create(const tcs_spec* spec, tcs_stencil** out) {
+  int rc = validate(spec);
+  if (rc) return rc;
+  if (!out) return fail(TCS_ERR_INVALID_VALUE, "output handle pointer is NULL");
+  rc = ensure_cuda();
+  if (rc) return rc;
+  std::vector<char> cubin;
+  tcs_spec canon = *spec;
+  if (canon.dimension == 2) canon.cz = 1;
+  rc = instantiate(canon, cubin, nullptr);
+  if (rc) return rc;
+  tcs_stencil* h = new tcs_stencil();
+  h->spec = canon;
+  h->S = stencil_size_of(h->spec);
+  h->flops = h->spec.coefficients == TCS_JACOBI ? h->S : 2 * h->S - 1;
+  h->left_off = left_offset_of(h->spec);
+  auto bail = [&](int code) {
+    if (h->mod) g_drv.ModuleUnload(h->mod);
+    delete h;
+    return code;
+  };
+  if (cudaGetDevice(&h->device) != cudaSuccess) return bail(fail(TCS_ERR_CUDA, "cudaGetDevice"));
+  cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, h->device);
+  cudaDeviceGetAttribute(&h->smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device);
+  CUresult cr = g_drv.ModuleLoadData(&h->mod, cubin.data());
+  if (cr != CUDA_SUCCESS) return bail(fail(TCS_ERR_CUDA, "cuModuleLoadData: " + cu_msg(cr)));
+  if ((cr = g_drv.ModuleGetFunction(&h->f_direct, h->mod, "tcs_direct")) != CUDA_SUCCESS ||
+      (cr = g_drv.ModuleGetFunction(&h->f_march, h->mod, "tcs_march")) != CUDA_SUCCESS ||
+      (cr = g_drv.ModuleGetFunction(&h->f_init, h->mod, "tcs_init")) != CUDA_SUCCESS)
+    return bail(fail(TCS_ERR_CUDA, "cuModuleGetFunction: " + cu_msg(cr)));
+  size_t bytes = 0;
+  if ((cr = g_drv.ModuleGetGlobal(&h->mask_ptr, &h->mask_bytes, h->mod, "tcs_mask")) !=
+          CUDA_SUCCESS ||
+      (cr = g_drv.ModuleGetGlobal(&h->status_ptr, &bytes, h->mod, "tcs_status")) != CUDA_SUCCESS)
+    return bail(fail(TCS_ERR_CUDA, "cuModuleGetGlobal: " + cu_msg(cr)));
+  if (cudaMemset((void*)h->status_ptr, 0, sizeof(unsigned)) != cudaSuccess)
+    return bail(fail(TCS_ERR_CUDA, "clearing the status word failed"));
+  *out = h;
+  return TCS_OK;
+}
+
+int tcs_destroy(tcs_stencil* h) {
+  if (!h) return TCS_OK;
+  if (h->mod && g_drv.ModuleUnload) g_drv.ModuleUnload(h->mod);
+  delete h;
+  return TCS_OK;
+}
+
+int tcs_get_spec(const tcs_stencil* h, tcs_spec* out) {
+  if (!h || !out) return fail(TCS_ERR_INVALID_VALUE, "NULL argument");
+  *out = h->spec;
+  return TCS_OK;
+}
+
+int tcs_copy_mask(tcs_stencil* h, const double* mask, unsigned n) {
+  if (!h) return fail(TCS_ERR_INVALID_VALUE, "NULL handle");
+  if (h->spec.coefficients == TCS_JACOBI) return TCS_OK;  // reference: empty copyMask
+  if (!mask && n) return fail(TCS_ERR_INVALID_VALUE, "NULL mask");
+  if (n > h->S)
+    return fail(TCS_ERR_INVALID_VALUE, "mask larger than the stencil (" + std::to_string(h->S) + ")");
+  if (h->spec.precision == TCS_F64) {
+    TCS_RT(cudaMemcpy((void*)h->mask_ptr, mask, sizeof(double) * n, cudaMemcpyHostToDevice));
+  } else {
+    std::vector<float> f(mask, mask + n);
+    TCS_RT(cudaMemcpy((void*)h->mask_ptr, f.data(), sizeof(float) * n, cudaMemcpyHostToDevice));
+  }
+  TCS_RT(cudaDeviceSynchronize());
+  return TCS_OK;
+}
+
+int tcs_max_potential_block_size(tcs_stencil* h, int* out) {
+  if (!h || !out) return fail(TCS_ERR_INVALID_VALUE, "NULL argument");
+  int min_grid = 0, block = 0;
+  TCS_CU(g_drv.OccMaxPotential(&min_grid, &block, h->f_direct, nullptr, 0, 0));
+  *out = block;
+  return TCS_OK;
+}
+
+int tcs_plan_launch(tcs_stencil* h, const unsigned grid[3], unsigned right_offset,
+                    const tcs_launch* launch, tcs_plan* out) {
+  Resolved r;
+  int rc = resolve(h, grid, right_offset, launch, r);
+  if (rc) return rc;
+  if (out) {
+    tcs_plan p{};
+    p.variant = r.variant;
+    for (int i = 0; i < 3; ++i) {
+      p.grid_blocks[i] = r.grid[i];
+      p.block[i] = r.block[i];
+    }
+    p.dyn_smem = r.smem;
+    p.seg_len = r.geo.seg;
+    p.nslot = r.geo.nslot;
+    p.width = r.geo.width;
+    p.depth = r.depth;
+    p.ctas_per_sm = r.occ;
+    p.num_sms = h->num_sms;
+    *out = p;
+  }
+  return TCS_OK;
+}
+
+int tcs_update_grid(tcs_stencil* h, const unsigned grid[3], unsigned right_offset,
+                    const tcs_launch* launch, const void* in, void* out, void* stream) {
+  Resolved r;
+  int rc = resolve(h, grid, right_offset, launch, r);
+  if (rc) return rc;
+  return launch_resolved(h, r, in, out, (CUstream)stream);
+}
+
+int tcs_sweeps(tcs_stencil* h, const unsigned grid[3], unsigned right_offset,
+               const tcs_launch* launch, void* a, void* b, unsigned n, void* stream,
+               int* result_in_b) {
+  Resolved r;
+  int rc = resolve(h, grid, right_offset, launch, r);
+  if (rc) return rc;
+  void* src = a;
+  void* dst = b;
+  for (unsigned i = 0; i < n; ++i) {
+    rc = launch_resolved(h, r, src, dst, (CUstream)stream);
+    if (rc) return rc;
+    std::swap(src, dst);
+  }
+  if (result_in_b) *result_in_b = (n % 2 == 1) ? 1 : 0;
+  return TCS_OK;
+}
+
+int tcs_time_sweeps(tcs_stencil* h, const unsigned grid[3], unsigned right_offset,
+                    const tcs_launch* launch, void* a, void* b, unsigned n, void* stream,
+                    float* ms) {
+  Resolved r;
+  int rc = resolve(h, grid, right_offset, launch, r);
+  if (rc) return rc;
+  cudaEvent_t e0, e1;
+  TCS_RT(cudaEventCreate(&e0));
+  TCS_RT(cudaEventCreate(&e1));
+  cudaStream_t st = (cudaStream_t)stream;
+  void* src = a;
+  void* dst = b;
+  cudaEventRecord(e0, st);
+  for (unsigned i = 0; i < n; ++i) {
+    rc = launch_resolved(h, r, src, dst, (CUstream)stream);
+    if (rc) break;
+    std::swap(src, dst);
+  }
+  cudaEventRecord(e1, st);
+  cudaError_t se = cudaEventSynchronize(e1);
+  float t = 0.f;
+  if (rc == TCS_OK && se == cudaSuccess) cudaEventElapsedTime(&t, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc) return rc;
+  if (se != cudaSuccess) return fail(TCS_ERR_CUDA, std::string("sweeps: ") + cudaGetErrorString(se));
+  if (ms) *ms = t;
+  return TCS_OK;
+}
+
+int tcs_benchmark_update_grid(tcs_stencil* h, const char* coeff_type, const char* neighbourhood,
+                              unsigned stencil_range, unsigned dimension, const char* alignment,
+                              double max_time, const unsigned grid[3], const unsigned block[3],
+                              const unsigned grid_blocks[3], void* d_array0, void* d_array1,
+                              unsigned right_offset, double* durations, unsigned cap,
+                              unsigned* n_out) {
+  if (!h) return fail(TCS_ERR_INVALID_VALUE, "NULL handle");
+  // runtime sanity check against the baked-in parameters (generateLaunchUpdateGrid.py:106-119)
+  const tcs_spec& s = h->spec;
+  bool passed = true;
+  if (!coeff_type || std::strcmp(coeff_type, coeff_str(s.coefficients)) != 0) passed = false;
+  if (!neighbourhood || std::strcmp(neighbourhood, shape_str(s.neighbourhood)) != 0) passed = false;
+  if (stencil_range != (unsigned)s.range) passed = false;
+  if (dimension != (unsigned)s.dimension) passed = false;
+  if (!alignment || std::strcmp(alignment, align_str(s.alignment)) != 0) passed = false;
+  if (!passed)
+    return fail(TCS_ERR_INVALID_VALUE,
+                "benchmarkUpdateGrid: runtime parameters do not match the instantiated kernel");
+  if (max_time < 0) return fail(TCS_ERR_INVALID_VALUE, "maxTime must be non-negative");
+  tcs_launch L{};
+  for (int i = 0; i < 3; ++i) {
+    L.block[i] = block ? block[i] : 0;
+    L.grid_blocks[i] = grid_blocks ? grid_blocks[i] : 0;
+  }
+  L.variant = h->dropin_variant;
+  L.segments = h->dropin_segments;
+  L.depth = h->dropin_depth;
+  Resolved r;
+  int rc = resolve(h, grid, right_offset, &L, r);
+  if (rc) return rc;
+  using clock = std::chrono::steady_clock;
+  std::vector<clock::time_point> ts;
+  ts.reserve(1024);
+  ts.push_back(clock::now());
+  double runtime = 0.0;
+  void* a0 = d_array0;
+  void* a1 = d_array1;
+  for (unsigned long long it = 1; runtime <= max_time; it *= 2) {
+    for (unsigned long long i = 0; i < it; ++i) {
+      rc = launch_resolved(h, r, a0, a1, nullptr);
+      if (rc) return rc;
+      TCS_RT(cudaDeviceSynchronize());
+      std::swap(a0, a1);
+      ts.push_back(clock::now());
+    }
+    runtime = std::chrono::duration<double>(ts.back() - ts.front()).count();
+  }
+  const unsigned n = (unsigned)(ts.size() - 1);
+  for (unsigned i = 0; i < n && i < cap; ++i)
+    durations[i] = std::chrono::duration<double>(ts[i + 1] - ts[i]).count();
+  if (n_out) *n_out = n;
+  return TCS_OK;
+}
+
+int tcs_launch_init(tcs_stencil* h, const unsigned grid[3], const unsigned block[3],
+                    const unsigned grid_blocks[3], void* d_array, unsigned right_offset) {
+  if (!h || !grid || !block || !grid_blocks || !d_array)
+    return fail(TCS_ERR_INVALID_VALUE, "NULL argument");
+  const tcs_spec& s = h->spec;
+  unsigned long long xdim = grid[0], ydim = grid[1], zdim = s.dimension == 3 ? grid[2] : 1;
+  unsigned x_shift = h->left_off;
+  unsigned long long x_end = (s.alignment == TCS_ALIGN_NONE) ? xdim : xdim - right_offset;
+  CUdeviceptr p = (CUdeviceptr)d_array;
+  void* args[] = {&p, &xdim, &ydim, &zdim, &x_shift, &x_end};
+  TCS_CU(g_drv.LaunchKernel(h->f_init, grid_blocks[0], grid_blocks[1], grid_blocks[2], block[0],
+                            block[1], block[2], 0, nullptr, args, nullptr));
+  TCS_RT(cudaDeviceSynchronize());
+  return TCS_OK;
+}
+
+int tcs_device_status(tcs_stencil* h, unsigned* status, int clear) {
+  if (!h) return fail(TCS_ERR_INVALID_VALUE, "NULL handle");
+  unsigned v = 0;
+  TCS_RT(cudaMemcpy(&v, (void*)h->status_ptr, sizeof(v), cudaMemcpyDeviceToHost));
+  if (clear) TCS_RT(cudaMemset((void*)h->status_ptr, 0, sizeof(unsigned)));
+  if (status) *status = v;
+  return TCS_OK;
+}
+
+int tcs_set_dropin_launch(tcs_stencil* h, int variant, unsigned segments, unsigned depth) {
+  if (!h) return fail(TCS_ERR_INVALID_VALUE, "NULL handle");
+  if (variant != TCS_VARIANT_AUTO && variant != TCS_VARIANT_DIRECT && variant != TCS_VARIANT_MARCH)
+    return fail(TCS_ERR_INVALID_VALUE, "unknown variant");
+  h->dropin_variant = variant;
+  h->dropin_segments = segments;
+  h->dropin_depth = depth;
+  return TCS_OK;
+}
+
+int tcs_precompile(const tcs_spec* spec, char* cubin_path, unsigned path_cap) {
+  int rc = validate(spec);
+  if (rc) return rc;
+  tcs_spec s = *spec;
+  if (s.dimension == 2) s.cz = 1;
+  std::vector<char> cubin;
+  std::string path;
+  rc = instantiate(s, cubin, &path);
+  if (rc) return rc;
+  if (cubin_path && path_cap) {
+    std::strncpy(cubin_path, path.c_str(), path_cap - 1);
+    cubin_path[path_cap - 1] = '\0';
+  }
+  return TCS_OK;
+}
+
+int tcs_device_sm_count(int* out) {
+  int rc = ensure_cuda();
+  if (rc) return rc;
+  int dev = 0;
+  TCS_RT(cudaGetDevice(&dev));
+  TCS_RT(cudaDeviceGetAttribute(out, cudaDevAttrMultiProcessorCount, dev));
+  return TCS_OK;
+}
+
+}  // extern "C"

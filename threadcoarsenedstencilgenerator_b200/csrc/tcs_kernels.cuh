@@ -1,0 +1,310 @@
+// Thread-coarsened structured-grid stencil sweeps for sm_100a.
+//
+// This header is the device half of the engine. The host layer (tcs_capi.cpp) compiles it
+// with NVRTC once per stencil parameter set, prepending the TCS_* macros below, exactly as the
+// reference bakes one parameter set into one generated `kernels.cu`
+// (cuda/generate2DStencil_cuda.py:225-318, cuda/generate3DStencil_cuda.py:245-383).
+//
+// Required macros (set by the host, one module per parameter set):
+//   TCS_T       double | float       element type of the grid
+//   TCS_DIM     2 | 3
+//   TCS_SHAPE   0 Box | 1 Star       neighbourhood
+//   TCS_ORIENT  0 Row | 1 Column     footprint traversal order
+//   TCS_COEFF   0 Jacobi | 1 Variable
+//   TCS_R       stencil range >= 1
+//   TCS_CX, TCS_CY, TCS_CZ           per-thread coarsening factors (TCS_CZ = 1 in 2D)
+//
+// Arithmetic contract.  Every output point accumulates its S terms in the order in which the
+// reference's generated kernel visits them, with the reference's first-term initialisation and
+// FMA contraction (the module is compiled with --fmad=false, so only the explicit fma() calls
+// below fuse): Jacobi `acc = v0; acc = acc + v_k; out = acc * fl(1/S)`, Variable
+// `acc = v0 * m0; acc = fma(v_k, m_k, acc)`.  The FP64 result is therefore bit-identical to the
+// reference kernel compiled by nvcc with its default -fmad=true.
+//
+// Two sweep kernels share that per-thread arithmetic:
+//   tcs_direct  one thread per coarsened tile, operands read through L1 (the reference's
+//               launch geometry; used for the drop-in grid/block contract and as the
+//               fallback when a tile does not fit the TMA constraints);
+//   tcs_march   one CTA per (x[,y]) tile column marching along the slowest axis; the input
+//               planes stream into a shared-memory ring through TMA
+//               (cp.async.bulk.tensor, no multicast) behind mbarriers, so each input element
+//               crosses HBM once per sweep and every footprint read is a shared-memory hit.
+//
+// Every mbarrier wait is bounded (TCS_WAIT_LIMIT cycles).  On expiry the CTA records
+// TCS_DEV_TIMEOUT in `tcs_status`, waits (bounded again) for its own bulk copies and returns;
+// the host reads `tcs_status` after the sweep.
+
+#ifndef TCS_T
+#error "TCS_T must be defined by the instantiation layer"
+#endif
+
+#include "tcs_tile.cuh"
+
+#define TCS_DEV_TIMEOUT 1u
+#ifndef TCS_WAIT_LIMIT
+#define TCS_WAIT_LIMIT 4000000000LL
+#endif
+
+// Device-side status word (bit TCS_DEV_TIMEOUT: a bounded wait expired).
+__device__ tcs_u32 tcs_status;
+
+// Launch geometry, passed by value.  Units are grid points; xdim is the padded row pitch.
+struct TcsGeo {
+  tcs_u64 xdim, ydim, zdim;   // gridSize after truncation/alignment (zdim = 1 in 2D)
+  tcs_u32 x0, x_lim;          // interior x range [x0, x_lim) = [R + leftOff, xdim - R - rightOff)
+  tcs_u32 y_lim, z_lim;       // interior is y < y_lim, z < z_lim (lower bound R)
+  tcs_u32 seg;                // tcs_march: outputs along the march axis per CTA
+  tcs_u32 nslot;              // tcs_march: ring slots (chunks of one step each)
+  tcs_u32 width;              // tcs_march: shared-memory row width W in elements
+  tcs_u32 pad_;
+};
+
+// Opaque CUtensorMap (128 bytes, 64-byte aligned), passed as a __grid_constant__ parameter.
+struct __align__(64) TcsTmaMap {
+  tcs_u64 w[16];
+};
+
+namespace tcs {
+
+// ---- mbarrier / TMA primitives (inline PTX) -------------------------------------------------
+
+__device__ __forceinline__ tcs_u32 smem_addr(const void* p) {
+  return (tcs_u32)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(tcs_u32 bar, tcs_u32 count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void fence_barrier_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(tcs_u32 bar, tcs_u32 bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(tcs_u32 bar, tcs_u32 parity) {
+  tcs_u32 done;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(done)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+
+// Bounded wait for the phase with the given parity; returns true when the limit expired.
+__device__ __forceinline__ bool mbar_wait_bounded(tcs_u32 bar, tcs_u32 parity, long long limit) {
+  if (mbar_try_wait(bar, parity)) return false;
+  const long long t0 = clock64();
+  while (!mbar_try_wait(bar, parity)) {
+    if (clock64() - t0 > limit) return true;
+  }
+  return false;
+}
+
+__device__ __forceinline__ void tma_prefetch_map(const TcsTmaMap* map) {
+  asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<tcs_u64>(map)) : "memory");
+}
+
+__device__ __forceinline__ void tma_load_2d(tcs_u32 dst, const TcsTmaMap* map, tcs_u32 bar, int x,
+                                            int y) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3}], [%4];" ::"r"(dst),
+      "l"(reinterpret_cast<tcs_u64>(map)), "r"(x), "r"(y), "r"(bar)
+      : "memory");
+}
+
+__device__ __forceinline__ void tma_load_3d(tcs_u32 dst, const TcsTmaMap* map, tcs_u32 bar, int x,
+                                            int y, int z) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(dst),
+      "l"(reinterpret_cast<tcs_u64>(map)), "r"(x), "r"(y), "r"(z), "r"(bar)
+      : "memory");
+}
+
+}  // namespace tcs
+
+// ---- tcs_direct: the reference's launch geometry, operands through L1 -------------------------
+// Thread origin and tile guard as in cuda/generate2DStencil_cuda.py:78-104 and
+// cuda/generate3DStencil_cuda.py:81-114 (x0 already includes the Write left offset).
+extern "C" __global__ void tcs_direct(const T* __restrict__ in, T* __restrict__ out, const TcsGeo g) {
+  using namespace tcs;
+  const tcs_u64 x = (tcs_u64)(blockIdx.x * blockDim.x + threadIdx.x) * CX + g.x0;
+  const tcs_u64 y = (tcs_u64)(blockIdx.y * blockDim.y + threadIdx.y) * CY + R;
+  const tcs_u64 z = (DIM == 3) ? (tcs_u64)(blockIdx.z * blockDim.z + threadIdx.z) * CZ + R : 0;
+  if (x + (CX - 1) < g.x_lim && y + (CY - 1) < g.y_lim &&
+      (DIM == 2 || z + (CZ - 1) < g.z_lim)) {
+    const tcs_i64 xdim = (tcs_i64)g.xdim;
+    const tcs_i64 plane = (tcs_i64)(g.xdim * g.ydim);
+    const tcs_u64 base = x + y * g.xdim + z * (tcs_u64)plane;
+    const T* __restrict__ p = in + base;
+    auto ld = [&](int gx, int gy, int gz) {
+      return __ldg(p + (tcs_i64)gx + (tcs_i64)gy * xdim + (tcs_i64)gz * plane);
+    };
+    T acc[NE];
+    traverse(ld, acc);
+    store(out + base, acc, g.xdim, (tcs_u64)plane);
+  }
+}
+
+// ---- tcs_march: TMA-fed shared-memory ring, one CTA per tile column ---------------------------
+// CTA tile per step: (blockDim.x*CX) x (blockDim.y*CY) in 2D (march along y, step = blockDim.y*CY
+// rows) and (blockDim.x*CX) x (blockDim.y*CY) x (blockDim.z*CZ) in 3D (march along z).  Chunk j of
+// the ring holds the `step` input planes starting at (segment start - R + j*step); a step needs
+// K = 1 + ceil(2R/step) consecutive chunks and the ring keeps nslot >= K+1 of them, so the load of
+// chunk s+nslot-1 overlaps the arithmetic of step s.
+extern "C" __global__ void tcs_march(const __grid_constant__ TcsTmaMap tmap, T* __restrict__ out, const TcsGeo g) {
+  using namespace tcs;
+  extern __shared__ __align__(128) unsigned char tcs_smem[];
+  const tcs_u32 nslot = g.nslot;
+  const tcs_u32 W = g.width;
+  const tcs_u32 TX = blockDim.x * CX;
+#if TCS_DIM == 2
+  const tcs_u32 STEP = blockDim.y * CY;
+  const tcs_u32 plane_elems = W;
+  const tcs_u32 mlim = g.y_lim;
+  const tcs_u32 ms = R + blockIdx.y * g.seg;
+  const tcs_u32 Y0 = 0;
+#else
+  const tcs_u32 TY = blockDim.y * CY;
+  const tcs_u32 STEP = blockDim.z * CZ;
+  const tcs_u32 plane_elems = W * (TY + 2 * R);
+  const tcs_u32 mlim = g.z_lim;
+  const tcs_u32 ms = R + blockIdx.z * g.seg;
+  const tcs_u32 Y0 = R + blockIdx.y * TY;
+#endif
+  if (ms >= mlim) return;
+  const tcs_u32 me = min(ms + g.seg, mlim);
+  const tcs_u32 nsteps = (me - ms + STEP - 1) / STEP;
+  const tcs_u32 nchunks = (me - ms + 2 * R + STEP - 1) / STEP;
+  const tcs_u32 K = 1 + (2 * R + STEP - 1) / STEP;
+  const tcs_u32 ring_planes = nslot * STEP;
+  const tcs_u32 chunk_elems = STEP * plane_elems;
+  const tcs_u32 chunk_bytes = chunk_elems * (tcs_u32)sizeof(T);
+
+  const tcs_u32 X0 = g.x0 + blockIdx.x * TX;
+  const tcs_u32 xl = (X0 - R) & ~(tcs_u32)(VEC - 1);
+  const tcs_u32 tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+
+  const tcs_u32 bars = smem_addr(tcs_smem);
+  const tcs_u32 bar_bytes = ((nslot * 8u + 127u) / 128u) * 128u;
+  T* ring = reinterpret_cast<T*>(tcs_smem + bar_bytes);
+  const tcs_u32 ring_s = smem_addr(ring);
+
+  auto issue = [&](tcs_u32 j) {
+    const tcs_u32 slot = j % nslot;
+    const tcs_u32 bar = bars + 8u * slot;
+    mbar_expect_tx(bar, chunk_bytes);
+#if TCS_DIM == 2
+    tma_load_2d(ring_s + slot * chunk_bytes, &tmap, bar, (int)xl, (int)(ms - R + j * STEP));
+#else
+    tma_load_3d(ring_s + slot * chunk_bytes, &tmap, bar, (int)xl, (int)(Y0 - R),
+                (int)(ms - R + j * STEP));
+#endif
+  };
+
+  if (tid == 0) {
+    for (tcs_u32 i = 0; i < nslot; ++i) mbar_init(bars + 8u * i, 1u);
+    fence_barrier_init();
+    tma_prefetch_map(&tmap);
+  }
+  __syncthreads();
+  if (tid == 0) {
+    const tcs_u32 pro = min(nslot - 1, nchunks);
+    for (tcs_u32 j = 0; j < pro; ++j) issue(j);
+  }
+
+  const tcs_u32 x = X0 + threadIdx.x * CX;
+  const tcs_u32 col = x - xl;  // ring column of the thread's gx = 0
+#if TCS_DIM == 3
+  const tcs_u32 y = Y0 + threadIdx.y * CY;
+  const tcs_u32 row0 = threadIdx.y * CY + R;  // row in a plane of the thread's gy = 0
+  const bool lane_ok = (x + (CX - 1) < g.x_lim) && (y + (CY - 1) < g.y_lim);
+  const tcs_u32 tm = threadIdx.z * CZ;
+#else
+  const bool lane_ok = (x + (CX - 1) < g.x_lim);
+  const tcs_u32 tm = threadIdx.y * CY;
+#endif
+  const tcs_u64 plane_g = g.xdim * g.ydim;
+
+  tcs_u32 ring_base = 0;  // ring plane index of march position (ms - R + s*STEP)
+  for (tcs_u32 s = 0; s < nsteps; ++s) {
+    const tcs_u32 jlo = (s == 0) ? 0u : s + K - 1;
+    const tcs_u32 jhi = min(s + K - 1, nchunks - 1);
+    bool expired = false;
+    for (tcs_u32 j = jlo; j <= jhi; ++j)
+      expired |= mbar_wait_bounded(bars + 8u * (j % nslot), (j / nslot) & 1u, TCS_WAIT_LIMIT);
+    if (__syncthreads_or(expired)) {
+      if (tid == 0) {
+        atomicOr(&tcs_status, TCS_DEV_TIMEOUT);
+        // drain this CTA's own copies in flight (bounded as well)
+        const tcs_u32 issued_hi = min(s + nslot - 2, nchunks - 1);
+        for (tcs_u32 j = jlo; j <= issued_hi; ++j)
+          (void)mbar_wait_bounded(bars + 8u * (j % nslot), (j / nslot) & 1u, TCS_WAIT_LIMIT);
+      }
+      return;
+    }
+    if (tid == 0) {
+      const tcs_u32 j = s + nslot - 1;
+      if (j < nchunks) issue(j);
+    }
+
+    const tcs_u32 m = ms + s * STEP + tm;  // first output of this thread along the march axis
+    const bool ok = lane_ok && (m + ((DIM == 3 ? CZ : CY) - 1) < me);
+    if (ok) {
+      tcs_u32 pb = ring_base + tm;  // ring plane of the thread's footprint start (offset -R)
+      if (pb >= ring_planes) pb -= ring_planes;
+      T acc[NE];
+#if TCS_DIM == 2
+      auto ld = [&](int gx, int gy, int) {
+        tcs_u32 rr = pb + (tcs_u32)(gy + R);
+        if (rr >= ring_planes) rr -= ring_planes;
+        return ring[rr * W + col + gx];
+      };
+      traverse(ld, acc);
+      store(out + (tcs_u64)x + (tcs_u64)m * g.xdim, acc, g.xdim, plane_g);
+#else
+      auto ld = [&](int gx, int gy, int gz) {
+        tcs_u32 pp = pb + (tcs_u32)(gz + R);
+        if (pp >= ring_planes) pp -= ring_planes;
+        return ring[pp * plane_elems + (row0 + gy) * W + col + gx];
+      };
+      traverse(ld, acc);
+      store(out + (tcs_u64)x + (tcs_u64)y * g.xdim + (tcs_u64)m * plane_g, acc, g.xdim, plane_g);
+#endif
+    }
+    ring_base += STEP;
+    if (ring_base >= ring_planes) ring_base -= ring_planes;
+  }
+}
+
+// ---- tcs_init: the reference's initial pattern -----------------------------------------------
+// 2D: border columns x < R (right of the Write left offset) and rows y < R are 1.0, else 0.0
+// (cuda/generate2DStencil_cuda.py:321-350).  3D: those and planes z < R are 0.75 / 0.25 by the
+// parity of the linear index, else 0.0 (cuda/generate3DStencil_cuda.py:386-430).  x_shift is the
+// Write left offset (0 otherwise); x_end is xdim - rightOffset for Read/Write and xdim for None.
+extern "C" __global__ void tcs_init(T* __restrict__ a, const tcs_u64 xdim, const tcs_u64 ydim,
+                                    const tcs_u64 zdim, const tcs_u32 x_shift,
+                                    const tcs_u64 x_end) {
+  using namespace tcs;
+  const tcs_u64 x = (tcs_u64)(blockIdx.x * blockDim.x + threadIdx.x) + x_shift;
+  const tcs_u64 y = (tcs_u64)(blockIdx.y * blockDim.y + threadIdx.y);
+  const tcs_u64 z = (DIM == 3) ? (tcs_u64)(blockIdx.z * blockDim.z + threadIdx.z) : 0;
+  if (x < x_end && y < ydim && z < zdim) {
+    const tcs_u64 idx = x + y * xdim + z * xdim * ydim;
+    const bool border = (x - x_shift < (tcs_u64)R) || (y < (tcs_u64)R) || (DIM == 3 && z < (tcs_u64)R);
+    if (DIM == 2) {
+      a[idx] = border ? T(1.0) : T(0.0);
+    } else {
+      a[idx] = border ? ((idx % 2 == 0) ? T(0.75) : T(0.25)) : T(0.0);
+    }
+  }
+}

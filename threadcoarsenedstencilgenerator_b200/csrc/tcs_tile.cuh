@@ -1,0 +1,293 @@
+// Per-thread arithmetic of the thread-coarsened stencil sweep (included by tcs_kernels.cuh).
+//
+// Everything here is plain C++ on registers: the footprint traversal of one thread tile in the
+// reference generator's order, the mask layout, the first-term initialisation and the fused
+// multiply-adds.  The caller supplies a loader `ld(gx, gy, gz)` returning the grid value at a
+// thread-relative offset (from global memory, a shared-memory ring, ...).  With the TCS_* macros
+// fixed at compile time every loop unrolls and every branch folds, which turns this into the
+// straight-line register code the reference generates as text
+// (cuda/generate2DStencil_cuda.py:107-198, cuda/generate3DStencil_cuda.py:116-218).
+//
+// The header has no CUDA-only dependencies besides the __device__/__constant__ qualifiers and the
+// __fma_rn intrinsics, so a host harness can compile it with those mapped to plain C++.
+
+#pragma once
+
+#ifndef TCS_T
+#error "TCS_T must be defined by the instantiation layer"
+#endif
+
+typedef unsigned long long tcs_u64;
+typedef unsigned int tcs_u32;
+typedef long long tcs_i64;
+typedef TCS_T T;
+
+namespace tcs {
+constexpr int DIM = TCS_DIM;
+constexpr int SHAPE = TCS_SHAPE;
+constexpr int ORIENT = TCS_ORIENT;
+constexpr int COEFF = TCS_COEFF;
+constexpr int R = TCS_R;
+constexpr int CX = TCS_CX;
+constexpr int CY = TCS_CY;
+constexpr int CZ = (TCS_DIM == 3) ? TCS_CZ : 1;
+constexpr int NE = CX * CY * CZ;            // outputs per thread
+constexpr int W1 = 2 * R + 1;
+// stencilSize as in cuda/generate2DStencil_cuda.py:63-67 and cuda/generate3DStencil_cuda.py:66-70
+constexpr int S = (SHAPE == 0) ? (DIM == 2 ? W1 * W1 : W1 * W1 * W1) : (2 * DIM * R + 1);
+constexpr int VEC = 16 / (int)sizeof(T);    // elements per 16-byte TMA granule
+}  // namespace tcs
+
+// Stencil coefficients (Variable); the reference's `__constant__ double d_mask[S]`.
+__constant__ T tcs_mask[tcs::S];
+
+namespace tcs {
+
+__device__ __forceinline__ constexpr int iabs(int v) { return v < 0 ? -v : v; }
+
+// Fused multiply-add with a single rounding, for either element type.
+__device__ __forceinline__ double fmat(double a, double b, double c) { return __fma_rn(a, b, c); }
+__device__ __forceinline__ float fmat(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+
+// Linear mask index of relative offset (rx, ry[, rz]); calcMaskAddress in
+// cuda/generate2DStencil_cuda.py:120-144 and cuda/generate3DStencil_cuda.py:132-169.
+__device__ __forceinline__ constexpr int mask_index(int rx, int ry, int rz) {
+  if (SHAPE == 0) {
+    return (DIM == 2) ? (rx + R) + (ry + R) * W1 : (rx + R) + (ry + R) * W1 + (rz + R) * W1 * W1;
+  }
+  if (DIM == 2) {
+    if (rx == 0 && ry < 0) return ry + R;
+    if (ry == 0) return rx + 2 * R;
+    return ry + 3 * R;  // rx == 0 && ry > 0
+  }
+  if (rz < 0) return rz + R;
+  if (rz == 0 && rx == 0 && ry < 0) return ry + 2 * R;
+  if (rz == 0 && ry == 0) return rx + 3 * R;
+  if (rz == 0 && rx == 0 && ry > 0) return ry + 4 * R;
+  return rz + 5 * R;  // rz > 0
+}
+
+// Does the grid point at offset (rx, ry, rz) from an output belong to its neighbourhood?
+// (printAdditions, cuda/generate2DStencil_cuda.py:175-186, cuda/generate3DStencil_cuda.py:201-212)
+__device__ __forceinline__ constexpr bool contributes(int rx, int ry, int rz) {
+  if (SHAPE == 0) return iabs(rx) <= R && iabs(ry) <= R && (DIM == 2 || iabs(rz) <= R);
+  if (DIM == 2) return (iabs(rx) <= R && ry == 0) || (iabs(ry) <= R && rx == 0);
+  return (iabs(rx) <= R && ry == 0 && rz == 0) || (iabs(ry) <= R && rx == 0 && rz == 0) ||
+         (iabs(rz) <= R && rx == 0 && ry == 0);
+}
+
+// Is it the first term of that output (initialised, not added)?
+// (cuda/generate2DStencil_cuda.py:179,188-195, cuda/generate3DStencil_cuda.py:205,214)
+__device__ __forceinline__ constexpr bool is_first(int rx, int ry, int rz) {
+  if (SHAPE == 0) return rx == -R && ry == -R && (DIM == 2 || rz == -R);
+  if (DIM == 2) return (ORIENT == 1) ? (ry == 0 && rx == -R) : (rx == 0 && ry == -R);
+  return rx == 0 && ry == 0 && rz == -R;
+}
+
+// The second term of every output in the reference's per-output order (that order does not
+// depend on the coarsening factors: it is the traversal of a 1x1[x1] tile).
+__device__ __forceinline__ constexpr bool is_second(int rx, int ry, int rz) {
+  if (SHAPE == 0) {
+    if (DIM == 2)
+      return (ORIENT == 0) ? (rx == -R + 1 && ry == -R) : (rx == -R && ry == -R + 1);
+    return (ORIENT == 0) ? (rx == -R + 1 && ry == -R && rz == -R) : (rx == -R && ry == -R + 1 && rz == -R);
+  }
+  if (DIM == 2) {
+    if (ORIENT == 0) return (R >= 2) ? (rx == 0 && ry == -R + 1) : (rx == -1 && ry == 0);
+    return (R >= 2) ? (rx == -R + 1 && ry == 0) : (rx == 0 && ry == -1);
+  }
+  if (R >= 2) return rx == 0 && ry == 0 && rz == -R + 1;
+  return (ORIENT == 0) ? (rx == 0 && ry == -1 && rz == 0) : (rx == -1 && ry == 0 && rz == 0);
+}
+
+// Mask index of the first term of every output.
+__device__ __forceinline__ constexpr int first_mask_index() {
+  if (SHAPE == 0) return mask_index(-R, -R, -R);
+  if (DIM == 2) return (ORIENT == 1) ? mask_index(-R, 0, 0) : mask_index(0, -R, 0);
+  return mask_index(0, 0, -R);
+}
+
+// Apply the value loaded from thread-relative (gx, gy, gz) to every output it touches.
+// Variable stencils keep the first value v0 of an output until its second term arrives and
+// then form fma(v0, m0, v1*m1): the nvcc -fmad=true fusion of the reference's
+// `result = v0*m0; result += v1*m1;` (an add of two products fuses its left operand).
+template <class LD>
+__device__ __forceinline__ void point(const LD& ld, T (&acc)[NE], T (&p0)[NE], int gx, int gy,
+                                      int gz) {
+  const T v = ld(gx, gy, gz);
+#pragma unroll
+  for (int ez = 0; ez < CZ; ++ez) {
+#pragma unroll
+    for (int ey = 0; ey < CY; ++ey) {
+#pragma unroll
+      for (int ex = 0; ex < CX; ++ex) {
+        const int rx = gx - ex, ry = gy - ey, rz = gz - ez;
+        if (contributes(rx, ry, rz)) {
+          const int e = ex + ey * CX + ez * CX * CY;
+          const bool first = is_first(rx, ry, rz);
+          if (COEFF == 0) {
+            acc[e] = first ? v : acc[e] + v;
+          } else if (first) {
+            p0[e] = v;
+          } else if (is_second(rx, ry, rz)) {
+            acc[e] = fmat(p0[e], tcs_mask[first_mask_index()], v * tcs_mask[mask_index(rx, ry, rz)]);
+          } else {
+            acc[e] = fmat(v, tcs_mask[mask_index(rx, ry, rz)], acc[e]);
+          }
+        }
+      }
+    }
+  }
+}
+
+// Footprint traversal of one thread tile in the reference's order
+// (cuda/generate2DStencil_cuda.py:244-297, cuda/generate3DStencil_cuda.py:265-360).
+template <class LD>
+__device__ __forceinline__ void traverse(const LD& ld, T (&acc)[NE]) {
+  T p0[NE];
+#pragma unroll
+  for (int e = 0; e < NE; ++e) {
+    acc[e] = T(0);
+    p0[e] = T(0);
+  }
+  if (DIM == 2) {
+    if (SHAPE == 0) {
+      if (ORIENT == 1) {
+#pragma unroll
+        for (int gx = -R; gx < R + CX; ++gx)
+#pragma unroll
+          for (int gy = -R; gy < R + CY; ++gy) point(ld, acc, p0, gx, gy, 0);
+      } else {
+#pragma unroll
+        for (int gy = -R; gy < R + CY; ++gy)
+#pragma unroll
+          for (int gx = -R; gx < R + CX; ++gx) point(ld, acc, p0, gx, gy, 0);
+      }
+    } else {
+      if (ORIENT == 1) {
+#pragma unroll
+        for (int gx = -R; gx < 0; ++gx)
+#pragma unroll
+          for (int gy = 0; gy < CY; ++gy) point(ld, acc, p0, gx, gy, 0);
+#pragma unroll
+        for (int gx = 0; gx < CX; ++gx)
+#pragma unroll
+          for (int gy = -R; gy < R + CY; ++gy) point(ld, acc, p0, gx, gy, 0);
+#pragma unroll
+        for (int gx = CX; gx < CX + R; ++gx)
+#pragma unroll
+          for (int gy = 0; gy < CY; ++gy) point(ld, acc, p0, gx, gy, 0);
+      } else {
+#pragma unroll
+        for (int gy = -R; gy < 0; ++gy)
+#pragma unroll
+          for (int gx = 0; gx < CX; ++gx) point(ld, acc, p0, gx, gy, 0);
+#pragma unroll
+        for (int gy = 0; gy < CY; ++gy)
+#pragma unroll
+          for (int gx = -R; gx < R + CX; ++gx) point(ld, acc, p0, gx, gy, 0);
+#pragma unroll
+        for (int gy = CY; gy < CY + R; ++gy)
+#pragma unroll
+          for (int gx = 0; gx < CX; ++gx) point(ld, acc, p0, gx, gy, 0);
+      }
+    }
+  } else {
+    if (SHAPE == 0) {
+#pragma unroll
+      for (int gz = -R; gz < R + CZ; ++gz) {
+        if (ORIENT == 1) {
+#pragma unroll
+          for (int gx = -R; gx < R + CX; ++gx)
+#pragma unroll
+            for (int gy = -R; gy < R + CY; ++gy) point(ld, acc, p0, gx, gy, gz);
+        } else {
+#pragma unroll
+          for (int gy = -R; gy < R + CY; ++gy)
+#pragma unroll
+            for (int gx = -R; gx < R + CX; ++gx) point(ld, acc, p0, gx, gy, gz);
+        }
+      }
+    } else {
+      // in front of the intersection
+#pragma unroll
+      for (int gz = -R; gz < 0; ++gz) {
+        if (ORIENT == 1) {
+#pragma unroll
+          for (int gx = 0; gx < CX; ++gx)
+#pragma unroll
+            for (int gy = 0; gy < CY; ++gy) point(ld, acc, p0, gx, gy, gz);
+        } else {
+#pragma unroll
+          for (int gy = 0; gy < CY; ++gy)
+#pragma unroll
+            for (int gx = 0; gx < CX; ++gx) point(ld, acc, p0, gx, gy, gz);
+        }
+      }
+      // the cross in the centre slices
+#pragma unroll
+      for (int gz = 0; gz < CZ; ++gz) {
+        if (ORIENT == 1) {
+#pragma unroll
+          for (int gx = -R; gx < 0; ++gx)
+#pragma unroll
+            for (int gy = 0; gy < CY; ++gy) point(ld, acc, p0, gx, gy, gz);
+#pragma unroll
+          for (int gx = 0; gx < CX; ++gx)
+#pragma unroll
+            for (int gy = -R; gy < R + CY; ++gy) point(ld, acc, p0, gx, gy, gz);
+#pragma unroll
+          for (int gx = CX; gx < CX + R; ++gx)
+#pragma unroll
+            for (int gy = 0; gy < CY; ++gy) point(ld, acc, p0, gx, gy, gz);
+        } else {
+#pragma unroll
+          for (int gy = -R; gy < 0; ++gy)
+#pragma unroll
+            for (int gx = 0; gx < CX; ++gx) point(ld, acc, p0, gx, gy, gz);
+#pragma unroll
+          for (int gy = 0; gy < CY; ++gy)
+#pragma unroll
+            for (int gx = -R; gx < R + CX; ++gx) point(ld, acc, p0, gx, gy, gz);
+#pragma unroll
+          for (int gy = CY; gy < CY + R; ++gy)
+#pragma unroll
+            for (int gx = 0; gx < CX; ++gx) point(ld, acc, p0, gx, gy, gz);
+        }
+      }
+      // behind the intersection
+#pragma unroll
+      for (int gz = CZ; gz < CZ + R; ++gz) {
+        if (ORIENT == 1) {
+#pragma unroll
+          for (int gx = 0; gx < CX; ++gx)
+#pragma unroll
+            for (int gy = 0; gy < CY; ++gy) point(ld, acc, p0, gx, gy, gz);
+        } else {
+#pragma unroll
+          for (int gy = 0; gy < CY; ++gy)
+#pragma unroll
+            for (int gx = 0; gx < CX; ++gx) point(ld, acc, p0, gx, gy, gz);
+        }
+      }
+    }
+  }
+}
+
+// Write the tile back; Jacobi scales by c = fl(1/S) (cuda/generate2DStencil_cuda.py:300-315).
+__device__ __forceinline__ void store(T* __restrict__ o, const T (&acc)[NE], tcs_u64 xdim,
+                                      tcs_u64 plane) {
+  constexpr T c = T(1) / T(S);
+#pragma unroll
+  for (int ez = 0; ez < CZ; ++ez)
+#pragma unroll
+    for (int ey = 0; ey < CY; ++ey)
+#pragma unroll
+      for (int ex = 0; ex < CX; ++ex) {
+        const int e = ex + ey * CX + ez * CX * CY;
+        const T v = (COEFF == 0) ? acc[e] * c : acc[e];
+        o[(tcs_i64)ex + (tcs_i64)ey * (tcs_i64)xdim + (tcs_i64)ez * (tcs_i64)plane] = v;
+      }
+}
+
+}  // namespace tcs

@@ -1,0 +1,177 @@
+"""`Stencil`: one instantiated parameter set on the current CUDA device.
+
+The object is the engine-side counterpart of one generated ``kernels.cu`` +
+``launchUpdateGrid.cu`` pair of the reference (cuda/RunBenchmark.sh:118-129): creating it
+instantiates the sm_100a kernels for the spec (NVRTC, cubin cache) and loads them.  Device
+buffers are any objects exposing ``data_ptr()`` (torch tensors) or raw integer addresses; torch is
+used only to own device memory and streams.
+"""
+
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+
+from . import _lib
+from .spec import Geometry, StencilSpec
+
+
+def _ptr(buf) -> int:
+    if isinstance(buf, int):
+        return buf
+    if hasattr(buf, "data_ptr"):
+        return int(buf.data_ptr())
+    raise TypeError("expected a device tensor or an integer device address, got %r" % type(buf))
+
+
+def _stream(stream) -> int | None:
+    if stream is None:
+        return None
+    if isinstance(stream, int):
+        return stream
+    return int(stream.cuda_stream)
+
+
+@dataclass
+class Launch:
+    """Launch parameters of a sweep (see tcs_launch in include/tcs.h)."""
+
+    block: tuple = (128, 1, 1)
+    variant: str = "auto"          # auto | direct | march
+    grid_blocks: tuple = (0, 0, 0)  # direct only; zeros: cover the interior
+    segments: int = 0               # march: CTAs along the march axis per tile column (0 = auto)
+    depth: int = 0                  # march: chunks in flight (0 = auto)
+
+    _VARIANTS = {"auto": _lib.VARIANT_AUTO, "direct": _lib.VARIANT_DIRECT, "march": _lib.VARIANT_MARCH}
+
+    def to_c(self) -> _lib.CLaunch:
+        b = tuple(self.block) + (1,) * (3 - len(self.block))
+        g = tuple(self.grid_blocks) + (0,) * (3 - len(self.grid_blocks))
+        return _lib.CLaunch(_lib.U3(*b), _lib.U3(*g), self._VARIANTS[self.variant], int(self.segments),
+                            int(self.depth))
+
+
+@dataclass
+class Plan:
+    variant: str
+    grid_blocks: tuple
+    block: tuple
+    dyn_smem: int
+    seg_len: int
+    nslot: int
+    width: int
+    depth: int
+    ctas_per_sm: int
+    num_sms: int
+
+
+class Stencil:
+    """Kernels of one StencilSpec, loaded on the current device."""
+
+    def __init__(self, spec: StencilSpec):
+        self.spec = spec
+        self._lib = _lib.load()
+        h = ctypes.c_void_p()
+        _lib.check(self._lib.tcs_create(ctypes.byref(spec.to_c()), ctypes.byref(h)))
+        self._h = h
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) is not None and self._h.value:
+            self._lib.tcs_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- reference helper functions (cuda/launchUpdateGrid.h:16-18) -----------------------------
+    def copy_mask(self, mask) -> None:
+        vals = [float(v) for v in mask]
+        arr = (ctypes.c_double * len(vals))(*vals)
+        _lib.check(self._lib.tcs_copy_mask(self._h, arr, len(vals)))
+
+    def max_potential_block_size(self) -> int:
+        v = ctypes.c_int()
+        _lib.check(self._lib.tcs_max_potential_block_size(self._h, ctypes.byref(v)))
+        return v.value
+
+    # -- sweeps ---------------------------------------------------------------------------------
+    def geometry(self, nx: int, ny: int, nz: int = 1) -> Geometry:
+        return self.spec.geometry(nx, ny, nz)
+
+    def plan(self, geom: Geometry, launch: Launch) -> Plan:
+        p = _lib.CPlan()
+        _lib.check(self._lib.tcs_plan_launch(self._h, _lib.U3(*geom.grid), geom.right_offset,
+                                             ctypes.byref(launch.to_c()), ctypes.byref(p)))
+        names = {v: k for k, v in Launch._VARIANTS.items()}
+        return Plan(names[p.variant], tuple(p.grid_blocks), tuple(p.block), p.dyn_smem, p.seg_len, p.nslot,
+                    p.width, p.depth, p.ctas_per_sm, p.num_sms)
+
+    def update_grid(self, geom: Geometry, src, dst, launch: Launch | None = None, stream=None) -> None:
+        """One sweep dst = stencil(src) over the interior (asynchronous)."""
+        launch = launch or Launch()
+        _lib.check(self._lib.tcs_update_grid(self._h, _lib.U3(*geom.grid), geom.right_offset,
+                                             ctypes.byref(launch.to_c()), _ptr(src), _ptr(dst), _stream(stream)))
+
+    def sweeps(self, geom: Geometry, a, b, n: int, launch: Launch | None = None, stream=None):
+        """n ping-pong sweeps starting from a; returns the buffer holding the result."""
+        launch = launch or Launch()
+        in_b = ctypes.c_int()
+        _lib.check(self._lib.tcs_sweeps(self._h, _lib.U3(*geom.grid), geom.right_offset,
+                                        ctypes.byref(launch.to_c()), _ptr(a), _ptr(b), int(n), _stream(stream),
+                                        ctypes.byref(in_b)))
+        return b if in_b.value else a
+
+    def time_sweeps(self, geom: Geometry, a, b, n: int, launch: Launch | None = None, stream=None) -> float:
+        """n ping-pong sweeps timed with CUDA events; returns milliseconds."""
+        launch = launch or Launch()
+        ms = ctypes.c_float()
+        _lib.check(self._lib.tcs_time_sweeps(self._h, _lib.U3(*geom.grid), geom.right_offset,
+                                             ctypes.byref(launch.to_c()), _ptr(a), _ptr(b), int(n),
+                                             _stream(stream), ctypes.byref(ms)))
+        return ms.value
+
+    def device_status(self, clear: bool = True) -> int:
+        v = ctypes.c_uint()
+        _lib.check(self._lib.tcs_device_status(self._h, ctypes.byref(v), 1 if clear else 0))
+        return v.value
+
+    def set_dropin_launch(self, variant: str = "auto", segments: int = 0, depth: int = 0) -> None:
+        _lib.check(self._lib.tcs_set_dropin_launch(self._h, Launch._VARIANTS[variant], segments, depth))
+
+    # -- reference host interface (cuda/launchUpdateGrid.h:13-14) -------------------------------
+    def benchmark_update_grid(self, coeff_type: str, neighbourhood: str, stencil_range: int, dimension: int,
+                              alignment: str, max_time: float, grid_size, block_size, grid_blocks, d_array0,
+                              d_array1, right_offset: int, cap: int = 1 << 20) -> list:
+        dur = (ctypes.c_double * cap)()
+        n = ctypes.c_uint()
+        _lib.check(self._lib.tcs_benchmark_update_grid(
+            self._h, coeff_type.encode(), neighbourhood.encode(), int(stencil_range), int(dimension),
+            alignment.encode(), float(max_time), _lib.U3(*_dim3(grid_size)), _lib.U3(*_dim3(block_size)),
+            _lib.U3(*_dim3(grid_blocks)), _ptr(d_array0), _ptr(d_array1), int(right_offset), dur, cap,
+            ctypes.byref(n)))
+        return list(dur[: min(n.value, cap)])
+
+    def launch_init(self, grid_size, block_size, grid_blocks, d_array, right_offset: int) -> None:
+        _lib.check(self._lib.tcs_launch_init(self._h, _lib.U3(*_dim3(grid_size)), _lib.U3(*_dim3(block_size)),
+                                             _lib.U3(*_dim3(grid_blocks)), _ptr(d_array), int(right_offset)))
+
+
+def _dim3(v) -> tuple:
+    v = tuple(int(x) for x in v)
+    return v + (1,) * (3 - len(v))
+
+
+def precompile(spec: StencilSpec) -> str:
+    """Instantiate the kernels of ``spec`` into the cubin cache (NVRTC only, no GPU needed)."""
+    buf = ctypes.create_string_buffer(1024)
+    _lib.check(_lib.load().tcs_precompile(ctypes.byref(spec.to_c()), buf, 1024))
+    return buf.value.decode()
+
+
+def device_sm_count() -> int:
+    v = ctypes.c_int()
+    _lib.check(_lib.load().tcs_device_sm_count(ctypes.byref(v)))
+    return v.value
