@@ -1,0 +1,366 @@
+"""Benchmark of the B200 stencil engine (one JSON line on rank 0).
+
+Default workload: 3D Star Variable stencil, range 4 (25 points), FP64, 512^3 grid, Read alignment to
+16 points, seeded synthetic data (numpy default_rng; mask N(0,1) normalised to sum 1, values
+U[0,1)).  A step is one sweep of the whole grid; `value` is the whole-job GLup/s (interior points
+x steps / device time, max over ranks), with both 1 GiB buffers resident in HBM (inputs larger than
+L2, so no flush is needed between sweeps).  `e2e` runs the reference's job shape through the
+public Python API with host buffers: upload the grid from pinned memory, the workload's sweeps,
+download the result, timed with CUDA events around all of it.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--workload NAME] [--impl ours|reference]
+
+Multi-GPU: the stencil does not shard in this engine (replicas only); each rank runs the same
+workload on its own GPU and `value` sums the ranks' work over the slowest rank's time.
+--impl reference times the reference's own arithmetic on the host cores: the CPU restatement of
+the reference kernel (OpenMP, all host threads), the same metric and workload.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+FALLBACK_HBM_GBS = 6650.0
+
+
+def _peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d.get("hbm_gbs", FALLBACK_HBM_GBS)), "measured"
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def _dist():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def _traffic(workload: str):
+    p = ROOT / "profiles" / "traffic.json"
+    if p.exists():
+        d = json.loads(p.read_text()).get(workload)
+        if d:
+            return d.get("dram_bytes_per_launch")
+    return None
+
+
+def cpu_baseline(w, geom, a, mask, budget_s: float = 12.0) -> dict:
+    """The oracle's OpenMP loop (all host threads) on the same grid: whole-grid sweeps until the
+    time budget is spent."""
+    import numpy as np
+
+    import oracle as O
+
+    d, sh, o, c = w.spec.dimension, w.spec.neighbourhood, w.spec.orientation, w.spec.coefficients
+    ospec = O.make_spec(d, sh, o, c, w.spec.range, w.spec.cx, w.spec.cy, w.spec.cz, w.spec.alignment, w.spec.cl_size)
+    out = np.array(a, copy=True)
+    threads = O.max_threads()
+    t0 = time.perf_counter()
+    n = 0
+    while True:
+        O.cpu_sweep(ospec, a, out, geom.right_offset, mask, threads=threads)
+        n += 1
+        if time.perf_counter() - t0 > budget_s or n >= 200:
+            break
+    dt = time.perf_counter() - t0
+    glups = geom.interior_points * n / dt / 1e9
+    return {"value": glups, "unit": "GLup/s", "cores": threads, "kind": "port",
+            "sample": "%d full sweeps of the %s grid (%.1f s, OpenMP over rows, x innermost)" % (
+                n, "x".join(str(v) for v in w.grid[:w.spec.dimension]), dt)}
+
+
+def reference_gpu_timing(w, geom, steps: int = 20) -> dict | None:
+    """The reference's own generated kernel (built by oracle/build_ref.py for sm_100a) on this GPU."""
+    import ctypes
+
+    from oracle import ref_configs
+
+    if not w.reference:
+        return None
+    (cx, cy, cz), block = w.reference
+    s = w.spec
+    cfg = (s.dimension, s.neighbourhood, s.orientation, s.coefficients, s.range, cx, cy, cz, s.alignment, s.cl_size)
+    lib_path = ROOT / "oracle" / "_ref" / ref_configs.key(cfg) / "libref.so"
+    if not lib_path.exists():
+        return None
+    rspec = s.replace(cx=cx, cy=cy, cz=cz)
+    g = rspec.geometry(*w.grid)
+    lib = ctypes.CDLL(str(lib_path))
+    u3 = ctypes.c_uint * 3
+    gb = tuple(max(1, -(-g.threads[i] // block[i])) for i in range(3))
+    import numpy as np
+
+    m = w.make_mask()
+    mm = np.zeros(1) if m is None else np.ascontiguousarray(m)
+    ms = ctypes.c_float()
+    rc = lib.ref_time(ctypes.c_uint(s.dimension), u3(*g.grid), u3(*block), u3(*gb), ctypes.c_uint(g.right_offset),
+                      mm.ctypes.data_as(ctypes.c_void_p), ctypes.c_uint(0 if m is None else mm.size),
+                      ctypes.c_uint(3), ctypes.c_uint(steps), ctypes.byref(ms))
+    if rc != 0:
+        return None
+    glups = g.interior_points * steps / (ms.value / 1e3) / 1e9
+    return {"value": glups, "unit": "GLup/s", "kernel": "reference generated updateGrid (nvcc -arch=sm_100a)",
+            "coarsening": [cx, cy, cz], "block": list(block)}
+
+
+def run_ours(args) -> dict | None:
+    import numpy as np
+    import torch
+
+    import threadcoarsenedstencilgenerator_b200 as tcs
+    from threadcoarsenedstencilgenerator_b200.workloads import WORKLOADS
+
+    world, rank, local = _dist()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    w = WORKLOADS[args.workload]
+    spec = w.tuned_spec()
+    launch = w.tuned_launch()
+    geom = spec.geometry(*w.grid)
+    st = tcs.Stencil(spec)
+    mask = w.make_mask()
+    if mask is not None:
+        st.copy_mask(mask)
+    a = w.make_input(geom)
+    host = torch.from_numpy(a).pin_memory()
+    x = host.to("cuda", non_blocking=False)
+    y = x.clone()
+    plan = st.plan(geom, launch)
+    stream = torch.cuda.current_stream()
+    for _ in range(args.warmup):
+        st.update_grid(geom, x, y, launch, stream)
+        x, y = y, x
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        st.update_grid(geom, x, y, launch, stream)
+        x, y = y, x
+    e1.record(stream)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    ms = e0.elapsed_time(e1)
+    clocks = sampler.stop()
+    if st.device_status() != 0:
+        raise RuntimeError("device status word set during the timed sweeps")
+    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    points = geom.interior_points
+    value = world * points * args.steps / (ms_max / 1e3) / 1e9
+
+    # e2e: the reference's job shape through the public API with host buffers
+    e2e_steps = max(1, args.e2e_steps)
+    out_host = torch.empty_like(host).pin_memory()
+    torch.cuda.synchronize()
+    f0 = torch.cuda.Event(enable_timing=True)
+    f1 = torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    for _ in range(e2e_steps):
+        x.copy_(host, non_blocking=True)
+        y.copy_(x)  # both buffers carry the fixed border
+        res = st.sweeps(geom, x, y, w.sweeps, launch, stream)
+        out_host.copy_(res, non_blocking=True)
+    f1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = f0.elapsed_time(f1)
+    te = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_value = world * points * w.sweeps * e2e_steps / (float(te.item()) / 1e3) / 1e9
+    nbytes = host.numel() * host.element_size()
+
+    ref_gpu = None
+    cpu = None
+    if rank == 0 and world == 1:
+        ref_gpu = reference_gpu_timing(w, geom)
+        if not args.no_cpu_baseline:
+            cpu = cpu_baseline(w, geom, a, mask)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return None
+
+    peak, peak_kind = _peaks()
+    bytes_per_launch = 2 * spec.itemsize * points  # algorithmic: one read + one write per point
+    achieved = bytes_per_launch / ((ms / args.steps) / 1e3) / 1e9
+    traffic = _traffic(args.workload)
+    line = {
+        "metric": "GLup/s (FP64 stencil sweep, %s)" % w.name,
+        "value": value,
+        "unit": "GLup/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms_max / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64" if spec.precision == "f64" else "f32",
+        "data": "synthetic (numpy default_rng seed %d)" % w.seed,
+        "config": {
+            "workload": w.name, "grid": list(w.grid[:spec.dimension]), "neighbourhood": spec.neighbourhood,
+            "coefficients": spec.coefficients, "range": spec.range, "alignment": spec.alignment,
+            "cl_size": spec.cl_size, "coarsening": list(spec.coarsening), "block": list(plan.block),
+            "variant": plan.variant, "loader": plan.loader, "segments": plan.grid_blocks[-1 if spec.dimension == 3 else 1],
+            "parallelism": "replicas" if world > 1 else "single-gpu",
+            "l2": "inputs larger than L2 (2 x %.2f GiB)" % (nbytes / 2**30),
+        },
+        "gpu_launches": args.steps,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": traffic, "peak_source": "%s (MEASURED_PEAKS.json hbm_gbs)" % peak_kind
+                     if peak_kind == "measured" else "fallback 6.65 TB/s",
+                     "algorithmic_bytes_per_launch": bytes_per_launch},
+        "e2e": {"value": e2e_value, "unit": "GLup/s", "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
+                "job": "upload grid, %d sweeps, download result (per step)" % w.sweeps, "steps": e2e_steps},
+        "clocks": clocks,
+        "cpu_baseline": cpu,
+        "reference_gpu": ref_gpu,
+    }
+    return line
+
+
+def run_reference(args) -> dict | None:
+    """The reference's own stencil arithmetic on the host cores (oracle OpenMP restatement)."""
+    import numpy as np
+
+    import oracle as O
+    from threadcoarsenedstencilgenerator_b200.workloads import WORKLOADS
+
+    world, rank, local = _dist()
+    if rank != 0:
+        return None
+    w = WORKLOADS[args.workload]
+    spec = w.spec
+    geom = spec.geometry(*w.grid)
+    a = w.make_input(geom)
+    mask = w.make_mask()
+    ospec = O.make_spec(spec.dimension, spec.neighbourhood, spec.orientation, spec.coefficients, spec.range, spec.cx,
+                        spec.cy, spec.cz, spec.alignment, spec.cl_size)
+    out = a.copy()
+    threads = O.max_threads()
+    for _ in range(args.warmup):
+        O.cpu_sweep(ospec, a, out, geom.right_offset, mask, threads=threads)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        O.cpu_sweep(ospec, a, out, geom.right_offset, mask, threads=threads)
+        a, out = out, a
+    dt = time.perf_counter() - t0
+    value = geom.interior_points * args.steps / dt / 1e9
+    return {
+        "metric": "GLup/s (FP64 stencil sweep, %s)" % w.name, "value": value, "unit": "GLup/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3 / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (numpy default_rng seed %d)" % w.seed,
+        "config": {"workload": w.name, "grid": list(w.grid[:spec.dimension])}, "impl": "reference",
+        "cpu_baseline": {"value": value, "unit": "GLup/s", "cores": threads, "kind": "port",
+                         "sample": "%d full sweeps of the grid, OpenMP restatement of the reference kernel" % args.steps},
+        "e2e": {"value": value, "unit": "GLup/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main() -> int:
+    from threadcoarsenedstencilgenerator_b200.workloads import DEFAULT_WORKLOAD, WORKLOADS
+
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+    line = run_reference(args) if args.impl == "reference" else run_ours(args)
+    if line is not None:
+        print(json.dumps(line))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -95,6 +95,7 @@ typedef struct tcs_plan {
   unsigned nslot;           /* march: ring slots */
   unsigned width;           /* march: shared-memory row width in elements */
   unsigned depth;           /* march: chunks in flight */
+  unsigned loader;          /* march: 0 = TMA tensor copies, 1 = cp.async element copies */
   int ctas_per_sm;          /* occupancy of the resolved kernel at this shape */
   int num_sms;
 } tcs_plan;

@@ -124,3 +124,48 @@ extern "C" int ref_time(unsigned dim, const unsigned grid[3], const unsigned blo
 }
 
 extern "C" int ref_max_potential_block_size(void) { return maxPotentialBlockSize(); }
+
+// Same as ref_time, but both buffers start from `host_in` instead of the init pattern.
+extern "C" int ref_time_data(unsigned dim, const unsigned grid[3], const unsigned block[3],
+                             const unsigned grid_blocks[3], unsigned right_offset,
+                             const double* mask, unsigned mask_n, const double* host_in,
+                             unsigned warmup, unsigned nsweeps, float* ms_total) {
+  const size_t n = (size_t)grid[0] * grid[1] * (dim == 3 ? grid[2] : 1);
+  double *a = nullptr, *b = nullptr;
+  if (ck(cudaMalloc(&a, n * sizeof(double))) || ck(cudaMalloc(&b, n * sizeof(double)))) return 2;
+  const dim3 gs(grid[0], grid[1], dim == 3 ? grid[2] : 1);
+  const dim3 bs(block[0], block[1], block[2]);
+  const dim3 gb(grid_blocks[0], grid_blocks[1], grid_blocks[2]);
+  int rc = 0;
+  if (ck(cudaMemcpy(a, host_in, n * sizeof(double), cudaMemcpyHostToDevice)) ||
+      ck(cudaMemcpy(b, host_in, n * sizeof(double), cudaMemcpyHostToDevice)))
+    rc = 2;
+  if (!rc && mask && mask_n) copyMask(const_cast<double*>(mask), mask_n);
+  for (unsigned i = 0; i < warmup && !rc; ++i) {
+    launch_update(gs, bs, gb, a, b, right_offset);
+    double* t = a;
+    a = b;
+    b = t;
+  }
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaEventRecord(e0);
+  for (unsigned i = 0; i < nsweeps && !rc; ++i) {
+    launch_update(gs, bs, gb, a, b, right_offset);
+    double* t = a;
+    a = b;
+    b = t;
+  }
+  cudaEventRecord(e1);
+  if (!rc && ck(cudaEventSynchronize(e1))) rc = 2;
+  if (!rc && ck(cudaGetLastError())) rc = 2;
+  float ms = 0.f;
+  if (!rc) cudaEventElapsedTime(&ms, e0, e1);
+  if (ms_total) *ms_total = ms;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(a);
+  cudaFree(b);
+  return rc;
+}

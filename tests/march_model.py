@@ -23,15 +23,14 @@ def plan(dim, R, c, block, grid, x0, x_lim, y_lim, z_lim, es, smem_optin=232448,
     """resolve_march: returns None when unsupported, else the launch parameters."""
     cx, cy, cz = c
     vec = 16 // es
-    xdim = grid[0]
-    if (xdim * es) % 16:
-        return None
     TX = block[0] * cx
-    W = cdiv(TX + 2 * R + vec - 1, vec) * vec
     if dim == 2:
         STEP, rows = block[1] * cy, 1
     else:
         STEP, rows = block[2] * cz, block[1] * cy + 2 * R
+    W = cdiv(TX + 2 * R + vec - 1, vec) * vec
+    while (STEP * W * rows * es) % 128:
+        W += vec
     if W > 256 or STEP > 256 or rows > 256:
         return None
     plane = W * rows
@@ -41,7 +40,7 @@ def plan(dim, R, c, block, grid, x0, x_lim, y_lim, z_lim, es, smem_optin=232448,
         depth = max(1, min(4, cdiv(16384, chunk_bytes)))
     while True:
         nslot = K + depth
-        smem = cdiv(nslot * 8, 128) * 128 + nslot * chunk_bytes
+        smem = cdiv(nslot * 8, 128) * 128 + 128 + nslot * chunk_bytes
         if smem <= smem_optin or depth == 1:
             break
         depth -= 1
@@ -109,7 +108,13 @@ def simulate(dim, shape, R, c, block, grid, left_offset, right_offset, aligned, 
     rows = p["rows"]
     bar_bytes = cdiv(nslot * 8, 128) * 128
     ring_elems = nslot * STEP * plane
-    assert bar_bytes + ring_elems * es == p["smem"]
+    assert bar_bytes + 128 + ring_elems * es == p["smem"]
+    # TMA destinations: the ring starts on a 128-byte boundary and every slot is a multiple of 128 B
+    assert (STEP * plane * es) % 128 == 0, "TMA destination not 128-byte aligned"
+    # the ring, placed after the barriers and rounded up to 128 bytes, ends inside the allocation
+    for base in (0, 16, 64):  # possible dynamic shared-memory base offsets (mod 128)
+        ring_off = ((base + bar_bytes + 127) // 128) * 128 - base
+        assert ring_off + ring_elems * es <= p["smem"]
     chunk_elems = STEP * plane
     ring_planes = nslot * STEP
     TX = block[0] * cx

@@ -61,6 +61,9 @@ MARCH_CASES = [
     (2, "Box", 2, (3, 2, 1), (8, 4, 1), (53, 40, 1), "Read", 16),
     (2, "Box", 6, (2, 2, 1), (16, 2, 1), (60, 33, 1), "None", 0),
     (2, "Star", 1, (1, 1, 1), (1, 32, 1), (12, 80, 1), "Write", 16),
+    # shapes whose natural chunk size is not a multiple of 128 bytes (TMA destination rule)
+    (2, "Box", 1, (1, 1, 1), (128, 2, 1), (300, 20, 1), "None", 0),
+    (2, "Box", 2, (2, 3, 1), (8, 4, 1), (37, 29, 1), "None", 0),
     (3, "Star", 4, (1, 1, 1), (32, 4, 1), (40, 30, 28), "Read", 16),
     (3, "Star", 4, (2, 2, 1), (16, 4, 1), (44, 29, 21), "Read", 16),
     (3, "Star", 2, (2, 2, 2), (8, 4, 2), (31, 29, 27), "None", 0),
@@ -76,8 +79,6 @@ def test_march_addressing_model(case, es):
     spec = O.make_spec(d, sh, "Row", "Jacobi", r, c[0], c[1], c[2], al, cl)
     g = O.geometry(spec, *n)
     grid = g.grid
-    if (grid[0] * es) % 16:
-        grid = (grid[0] + (16 // es - grid[0] % (16 // es)), grid[1], grid[2])  # pitch rule of the planner
     for seg in (0, 1, 3):
         for depth in (0, 1, 3):
             cnt = march_model.simulate(d, sh, r, c, blk, grid, g.left_offset, g.right_offset, al != "None", es=es,

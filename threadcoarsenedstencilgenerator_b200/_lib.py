@@ -87,6 +87,7 @@ class CPlan(ctypes.Structure):
         ("nslot", ctypes.c_uint),
         ("width", ctypes.c_uint),
         ("depth", ctypes.c_uint),
+        ("loader", ctypes.c_uint),
         ("ctas_per_sm", ctypes.c_int),
         ("num_sms", ctypes.c_int),
     ]

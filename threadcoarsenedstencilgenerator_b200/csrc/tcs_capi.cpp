@@ -280,7 +280,7 @@ struct TcsGeo {
   unsigned seg;
   unsigned nslot;
   unsigned width;
-  unsigned pad_;
+  unsigned loader;
 };
 static_assert(sizeof(TcsGeo) == 56, "TcsGeo layout");
 
@@ -398,10 +398,9 @@ int resolve_march(tcs_stencil* h, const TcsGeo& g, const tcs_launch* L, Resolved
   const unsigned es = (unsigned)elem_size(s);
   const unsigned vec = 16u / es;
   const unsigned cz = s.dimension == 3 ? (unsigned)s.cz : 1u;
-  if ((g.xdim * es) % 16 != 0)
-    return fail(TCS_ERR_UNSUPPORTED, "row pitch is not a multiple of 16 bytes (TMA stride rule)");
+  // TMA needs a row pitch that is a multiple of 16 bytes; other pitches use the cp.async loader.
+  const unsigned loader = ((g.xdim * es) % 16 == 0) ? 0u : 1u;
   const unsigned TX = L->block[0] * s.cx;
-  const unsigned W = ((TX + 2 * R + vec - 1 + vec - 1) / vec) * vec;
   unsigned STEP, rows;
   if (s.dimension == 2) {
     STEP = L->block[1] * s.cy;
@@ -410,6 +409,11 @@ int resolve_march(tcs_stencil* h, const TcsGeo& g, const tcs_launch* L, Resolved
     STEP = L->block[2] * cz;
     rows = L->block[1] * s.cy + 2 * R;
   }
+  // Row width W: the tile plus its halo plus the alignment shift of the TMA x coordinate, in
+  // whole 16-byte granules, widened until a chunk (STEP planes of W x rows) is a multiple of
+  // 128 bytes: every TMA destination (one chunk per ring slot) must be 128-byte aligned.
+  unsigned W = ((TX + 2 * R + vec - 1 + vec - 1) / vec) * vec;
+  while ((STEP * W * rows * es) % 128 != 0) W += vec;
   if (W > 256 || STEP > 256 || rows > 256)
     return fail(TCS_ERR_UNSUPPORTED, "tile exceeds the 256-element TMA box limit");
   const unsigned plane = W * rows;
@@ -420,7 +424,8 @@ int resolve_march(tcs_stencil* h, const TcsGeo& g, const tcs_launch* L, Resolved
   unsigned smem = 0, nslot = 0;
   for (;;) {
     nslot = K + depth;
-    smem = ((nslot * 8 + 127) / 128) * 128 + nslot * chunk_bytes;
+    // barriers, then 128 bytes of slack so the ring can start on a 128-byte boundary
+    smem = ((nslot * 8 + 127) / 128) * 128 + 128 + nslot * chunk_bytes;
     if (smem <= (unsigned)h->smem_optin || depth == 1) break;
     --depth;
   }
@@ -471,6 +476,7 @@ int resolve_march(tcs_stencil* h, const TcsGeo& g, const tcs_launch* L, Resolved
   out.geo.seg = seg;
   out.geo.nslot = nslot;
   out.geo.width = W;
+  out.geo.loader = loader;
   for (int i = 0; i < 3; ++i) out.block[i] = L->block[i];
   if (s.dimension == 2) {
     out.grid[0] = nxt;
@@ -560,12 +566,18 @@ int launch_resolved(tcs_stencil* h, const Resolved& r, const void* in, void* out
                               r.block[1], r.block[2], 0, st, args, nullptr));
     return TCS_OK;
   }
-  CUtensorMap* map = nullptr;
-  int rc = tensor_map(h, in, r, &map);
-  if (rc) return rc;
-  CUtensorMap mcopy = *map;
-  CUdeviceptr pout = (CUdeviceptr)out;
-  void* args[] = {&mcopy, &pout, &geo};
+  // The TMA loader also needs a 16-byte aligned base address; otherwise copy with cp.async.
+  if (geo.loader == 0 && reinterpret_cast<uintptr_t>(in) % 16 != 0) geo.loader = 1;
+  alignas(64) CUtensorMap mcopy;
+  std::memset(&mcopy, 0, sizeof(mcopy));
+  if (geo.loader == 0) {
+    CUtensorMap* map = nullptr;
+    int rc = tensor_map(h, in, r, &map);
+    if (rc) return rc;
+    mcopy = *map;
+  }
+  CUdeviceptr pin = (CUdeviceptr)in, pout = (CUdeviceptr)out;
+  void* args[] = {&mcopy, &pin, &pout, &geo};
   TCS_CU(g_drv.LaunchKernel(h->f_march, r.grid[0], r.grid[1], r.grid[2], r.block[0], r.block[1],
                             r.block[2], r.smem, st, args, nullptr));
   return TCS_OK;
@@ -740,6 +752,7 @@ int tcs_plan_launch(tcs_stencil* h, const unsigned grid[3], unsigned right_offse
     p.nslot = r.geo.nslot;
     p.width = r.geo.width;
     p.depth = r.depth;
+    p.loader = r.geo.loader;
     p.ctas_per_sm = r.occ;
     p.num_sms = h->num_sms;
     *out = p;

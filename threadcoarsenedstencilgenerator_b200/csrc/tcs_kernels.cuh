@@ -42,7 +42,7 @@
 
 #define TCS_DEV_TIMEOUT 1u
 #ifndef TCS_WAIT_LIMIT
-#define TCS_WAIT_LIMIT 4000000000LL
+#define TCS_WAIT_LIMIT 1000000000LL
 #endif
 
 // Device-side status word (bit TCS_DEV_TIMEOUT: a bounded wait expired).
@@ -56,7 +56,7 @@ struct TcsGeo {
   tcs_u32 seg;                // tcs_march: outputs along the march axis per CTA
   tcs_u32 nslot;              // tcs_march: ring slots (chunks of one step each)
   tcs_u32 width;              // tcs_march: shared-memory row width W in elements
-  tcs_u32 pad_;
+  tcs_u32 loader;             // tcs_march: 0 = TMA tensor copies, 1 = cp.async element copies
 };
 
 // Opaque CUtensorMap (128 bytes, 64-byte aligned), passed as a __grid_constant__ parameter.
@@ -130,6 +130,27 @@ __device__ __forceinline__ void tma_load_3d(tcs_u32 dst, const TcsTmaMap* map, t
       : "memory");
 }
 
+// Element copy global -> shared through the async copy unit (8 or 4 bytes); src_bytes = 0
+// writes zeros (the fill for points outside the grid).
+__device__ __forceinline__ void cp_async_elem(tcs_u32 dst, const T* src, tcs_u32 src_bytes) {
+  if (sizeof(T) == 8) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(dst), "l"(src), "r"(src_bytes)
+                 : "memory");
+  } else {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(dst), "l"(src), "r"(src_bytes)
+                 : "memory");
+  }
+}
+
+// The mbarrier receives one arrival once all of this thread's prior cp.async copies landed.
+__device__ __forceinline__ void cp_async_arrive(tcs_u32 bar) {
+  asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(bar) : "memory");
+}
+
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.wait_all;" ::: "memory");
+}
+
 }  // namespace tcs
 
 // ---- tcs_direct: the reference's launch geometry, operands through L1 -------------------------
@@ -155,32 +176,39 @@ extern "C" __global__ void tcs_direct(const T* __restrict__ in, T* __restrict__ 
   }
 }
 
-// ---- tcs_march: TMA-fed shared-memory ring, one CTA per tile column ---------------------------
+// ---- tcs_march: shared-memory ring fed by TMA (or cp.async), one CTA per tile column ---------
 // CTA tile per step: (blockDim.x*CX) x (blockDim.y*CY) in 2D (march along y, step = blockDim.y*CY
 // rows) and (blockDim.x*CX) x (blockDim.y*CY) x (blockDim.z*CZ) in 3D (march along z).  Chunk j of
-// the ring holds the `step` input planes starting at (segment start - R + j*step); a step needs
-// K = 1 + ceil(2R/step) consecutive chunks and the ring keeps nslot >= K+1 of them, so the load of
-// chunk s+nslot-1 overlaps the arithmetic of step s.
-extern "C" __global__ void tcs_march(const __grid_constant__ TcsTmaMap tmap, T* __restrict__ out, const TcsGeo g) {
+// the ring holds the `step` input planes starting at (segment start - R + j*step), each plane the
+// tile plus its halo; a step needs K = 1 + ceil(2R/step) consecutive chunks and the ring keeps
+// nslot >= K+1 of them, so the loads of the next nslot-K chunks overlap the arithmetic of a step.
+// Loader 0 copies a chunk with one cp.async.bulk.tensor (TMA, issued by thread 0, no multicast);
+// loader 1 — for row pitches or base addresses outside the TMA rules — has every thread copy
+// elements with cp.async and signal the same mbarrier through cp.async.mbarrier.arrive.
+extern "C" __global__ void tcs_march(const __grid_constant__ TcsTmaMap tmap,
+                                     const T* __restrict__ in, T* __restrict__ out,
+                                     const TcsGeo g) {
   using namespace tcs;
   extern __shared__ __align__(128) unsigned char tcs_smem[];
   const tcs_u32 nslot = g.nslot;
   const tcs_u32 W = g.width;
   const tcs_u32 TX = blockDim.x * CX;
+  const bool use_tma = (g.loader == 0);
 #if TCS_DIM == 2
   const tcs_u32 STEP = blockDim.y * CY;
-  const tcs_u32 plane_elems = W;
+  const tcs_u32 rows = 1;
   const tcs_u32 mlim = g.y_lim;
   const tcs_u32 ms = R + blockIdx.y * g.seg;
   const tcs_u32 Y0 = 0;
 #else
   const tcs_u32 TY = blockDim.y * CY;
   const tcs_u32 STEP = blockDim.z * CZ;
-  const tcs_u32 plane_elems = W * (TY + 2 * R);
+  const tcs_u32 rows = TY + 2 * R;
   const tcs_u32 mlim = g.z_lim;
   const tcs_u32 ms = R + blockIdx.z * g.seg;
   const tcs_u32 Y0 = R + blockIdx.y * TY;
 #endif
+  const tcs_u32 plane_elems = W * rows;
   if (ms >= mlim) return;
   const tcs_u32 me = min(ms + g.seg, mlim);
   const tcs_u32 nsteps = (me - ms + STEP - 1) / STEP;
@@ -192,34 +220,62 @@ extern "C" __global__ void tcs_march(const __grid_constant__ TcsTmaMap tmap, T* 
 
   const tcs_u32 X0 = g.x0 + blockIdx.x * TX;
   const tcs_u32 xl = (X0 - R) & ~(tcs_u32)(VEC - 1);
+  const tcs_u32 nthreads = blockDim.x * blockDim.y * blockDim.z;
   const tcs_u32 tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
 
+  // Layout: nslot mbarriers, then the ring on a 128-byte boundary (TMA destinations must be
+  // 128-byte aligned; the planner makes every chunk a multiple of 128 bytes).
   const tcs_u32 bars = smem_addr(tcs_smem);
   const tcs_u32 bar_bytes = ((nslot * 8u + 127u) / 128u) * 128u;
-  T* ring = reinterpret_cast<T*>(tcs_smem + bar_bytes);
-  const tcs_u32 ring_s = smem_addr(ring);
+  const tcs_u32 ring_s = (bars + bar_bytes + 127u) & ~127u;
+  T* ring = reinterpret_cast<T*>(tcs_smem + (ring_s - bars));
 
+  // Copy chunk j into its ring slot.  TMA: thread 0 only.  cp.async: every thread.
   auto issue = [&](tcs_u32 j) {
     const tcs_u32 slot = j % nslot;
     const tcs_u32 bar = bars + 8u * slot;
-    mbar_expect_tx(bar, chunk_bytes);
+    const tcs_u32 m0 = ms - R + j * STEP;  // first plane of the chunk along the march axis
+    if (use_tma) {
+      mbar_expect_tx(bar, chunk_bytes);
 #if TCS_DIM == 2
-    tma_load_2d(ring_s + slot * chunk_bytes, &tmap, bar, (int)xl, (int)(ms - R + j * STEP));
+      tma_load_2d(ring_s + slot * chunk_bytes, &tmap, bar, (int)xl, (int)m0);
 #else
-    tma_load_3d(ring_s + slot * chunk_bytes, &tmap, bar, (int)xl, (int)(Y0 - R),
-                (int)(ms - R + j * STEP));
+      tma_load_3d(ring_s + slot * chunk_bytes, &tmap, bar, (int)xl, (int)(Y0 - R), (int)m0);
 #endif
+    } else {
+      const tcs_u32 dst0 = ring_s + slot * chunk_bytes;
+      for (tcs_u32 q = tid; q < chunk_elems; q += nthreads) {
+        const tcs_u32 xx = xl + q % W;
+#if TCS_DIM == 2
+        const tcs_u64 yy = m0 + q / W;
+        const bool inside = xx < g.xdim && yy < g.ydim;
+        const tcs_u64 gi = inside ? (tcs_u64)xx + yy * g.xdim : 0;
+#else
+        const tcs_u64 yy = (Y0 - R) + (q / W) % rows;
+        const tcs_u64 zz = m0 + q / plane_elems;
+        const bool inside = xx < g.xdim && yy < g.ydim && zz < g.zdim;
+        const tcs_u64 gi = inside ? (tcs_u64)xx + yy * g.xdim + zz * g.xdim * g.ydim : 0;
+#endif
+        cp_async_elem(dst0 + q * (tcs_u32)sizeof(T), in + gi, inside ? (tcs_u32)sizeof(T) : 0u);
+      }
+      cp_async_arrive(bar);
+    }
   };
 
   if (tid == 0) {
-    for (tcs_u32 i = 0; i < nslot; ++i) mbar_init(bars + 8u * i, 1u);
+    for (tcs_u32 i = 0; i < nslot; ++i) mbar_init(bars + 8u * i, use_tma ? 1u : nthreads);
     fence_barrier_init();
-    tma_prefetch_map(&tmap);
+    if (use_tma) tma_prefetch_map(&tmap);
   }
   __syncthreads();
-  if (tid == 0) {
+  {
     const tcs_u32 pro = min(nslot - 1, nchunks);
-    for (tcs_u32 j = 0; j < pro; ++j) issue(j);
+    if (use_tma) {
+      if (tid == 0)
+        for (tcs_u32 j = 0; j < pro; ++j) issue(j);
+    } else {
+      for (tcs_u32 j = 0; j < pro; ++j) issue(j);
+    }
   }
 
   const tcs_u32 x = X0 + threadIdx.x * CX;
@@ -243,18 +299,28 @@ extern "C" __global__ void tcs_march(const __grid_constant__ TcsTmaMap tmap, T* 
     for (tcs_u32 j = jlo; j <= jhi; ++j)
       expired |= mbar_wait_bounded(bars + 8u * (j % nslot), (j / nslot) & 1u, TCS_WAIT_LIMIT);
     if (__syncthreads_or(expired)) {
-      if (tid == 0) {
-        atomicOr(&tcs_status, TCS_DEV_TIMEOUT);
-        // drain this CTA's own copies in flight (bounded as well)
-        const tcs_u32 issued_hi = min(s + nslot - 2, nchunks - 1);
-        for (tcs_u32 j = jlo; j <= issued_hi; ++j)
-          (void)mbar_wait_bounded(bars + 8u * (j % nslot), (j / nslot) & 1u, TCS_WAIT_LIMIT);
+      if (use_tma) {
+        if (tid == 0) {
+          atomicOr(&tcs_status, TCS_DEV_TIMEOUT);
+          // drain this CTA's own bulk copies in flight (bounded as well)
+          const tcs_u32 issued_hi = min(s + nslot - 2, nchunks - 1);
+          for (tcs_u32 j = jlo; j <= issued_hi; ++j)
+            (void)mbar_wait_bounded(bars + 8u * (j % nslot), (j / nslot) & 1u, TCS_WAIT_LIMIT);
+        }
+      } else {
+        if (tid == 0) atomicOr(&tcs_status, TCS_DEV_TIMEOUT);
+        cp_async_wait_all();
       }
       return;
     }
-    if (tid == 0) {
+    {
       const tcs_u32 j = s + nslot - 1;
-      if (j < nchunks) issue(j);
+      if (j < nchunks) {
+        if (!use_tma)
+          issue(j);
+        else if (tid == 0)
+          issue(j);
+      }
     }
 
     const tcs_u32 m = ms + s * STEP + tm;  // first output of this thread along the march axis

@@ -107,170 +107,133 @@ __device__ __forceinline__ constexpr int first_mask_index() {
   return mask_index(0, 0, -R);
 }
 
-// Apply the value loaded from thread-relative (gx, gy, gz) to every output it touches.
-// Variable stencils keep the first value v0 of an output until its second term arrives and
-// then form fma(v0, m0, v1*m1): the nvcc -fmad=true fusion of the reference's
+// Compile-time loops.  Every footprint offset and element index below is a template constant,
+// so the traversal is straight-line code by construction (the reference generates it as text);
+// relying on #pragma unroll for these deep nests leaves outer loops rolled and turns offsets,
+// mask indices and first-term tests into run-time arithmetic.
+template <int V>
+struct ic {
+  static constexpr int value = V;
+};
+
+template <int I, int N, class F>
+__device__ __forceinline__ void static_for(F&& f) {
+  if constexpr (I < N) {
+    f(ic<I>{});
+    static_for<I + 1, N>(f);
+  }
+}
+
+// Apply the value v loaded from thread-relative (GX, GY, GZ) to every output it touches.
+// Variable stencils keep the first value v0 of an output in its accumulator until the second
+// term arrives and then form fma(v0, m0, v1*m1): the nvcc -fmad=true fusion of the reference's
 // `result = v0*m0; result += v1*m1;` (an add of two products fuses its left operand).
-template <class LD>
-__device__ __forceinline__ void point(const LD& ld, T (&acc)[NE], T (&p0)[NE], int gx, int gy,
-                                      int gz) {
-  const T v = ld(gx, gy, gz);
-#pragma unroll
-  for (int ez = 0; ez < CZ; ++ez) {
-#pragma unroll
-    for (int ey = 0; ey < CY; ++ey) {
-#pragma unroll
-      for (int ex = 0; ex < CX; ++ex) {
-        const int rx = gx - ex, ry = gy - ey, rz = gz - ez;
-        if (contributes(rx, ry, rz)) {
-          const int e = ex + ey * CX + ez * CX * CY;
-          const bool first = is_first(rx, ry, rz);
-          if (COEFF == 0) {
-            acc[e] = first ? v : acc[e] + v;
-          } else if (first) {
-            p0[e] = v;
-          } else if (is_second(rx, ry, rz)) {
-            acc[e] = fmat(p0[e], tcs_mask[first_mask_index()], v * tcs_mask[mask_index(rx, ry, rz)]);
+template <int GX, int GY, int GZ>
+__device__ __forceinline__ void apply(T (&acc)[NE], const T v) {
+  static_for<0, CZ>([&](auto ez) {
+    static_for<0, CY>([&](auto ey) {
+      static_for<0, CX>([&](auto ex) {
+        constexpr int rx = GX - decltype(ex)::value;
+        constexpr int ry = GY - decltype(ey)::value;
+        constexpr int rz = GZ - decltype(ez)::value;
+        constexpr int e = decltype(ex)::value + decltype(ey)::value * CX + decltype(ez)::value * CX * CY;
+        if constexpr (contributes(rx, ry, rz)) {
+          if constexpr (is_first(rx, ry, rz)) {
+            acc[e] = v;
+          } else if constexpr (COEFF == 0) {
+            acc[e] = acc[e] + v;
+          } else if constexpr (is_second(rx, ry, rz)) {
+            acc[e] = fmat(acc[e], tcs_mask[first_mask_index()], v * tcs_mask[mask_index(rx, ry, rz)]);
           } else {
             acc[e] = fmat(v, tcs_mask[mask_index(rx, ry, rz)], acc[e]);
           }
         }
-      }
-    }
-  }
+      });
+    });
+  });
+}
+
+template <int GX, int GY, int GZ, class LD>
+__device__ __forceinline__ void point(const LD& ld, T (&acc)[NE]) {
+  apply<GX, GY, GZ>(acc, ld(GX, GY, GZ));
 }
 
 // Footprint traversal of one thread tile in the reference's order
 // (cuda/generate2DStencil_cuda.py:244-297, cuda/generate3DStencil_cuda.py:265-360).
+// Loops run over [-R, ...) as [0, ...) shifted by R.
+template <int GZ, class LD>
+__device__ __forceinline__ void traverse_slice(const LD& ld, T (&acc)[NE]) {
+  // one z slice of a Box stencil (or the whole 2D Box stencil with GZ = 0)
+  if constexpr (ORIENT == 1) {
+    static_for<0, 2 * R + CX>([&](auto ix) {
+      static_for<0, 2 * R + CY>([&](auto iy) {
+        point<decltype(ix)::value - R, decltype(iy)::value - R, GZ>(ld, acc);
+      });
+    });
+  } else {
+    static_for<0, 2 * R + CY>([&](auto iy) {
+      static_for<0, 2 * R + CX>([&](auto ix) {
+        point<decltype(ix)::value - R, decltype(iy)::value - R, GZ>(ld, acc);
+      });
+    });
+  }
+}
+
+template <int GZ, class LD>
+__device__ __forceinline__ void traverse_cross(const LD& ld, T (&acc)[NE]) {
+  // the in-slice cross of a Star stencil
+  if constexpr (ORIENT == 1) {
+    static_for<0, R>([&](auto i) {  // gx in [-R, 0)
+      static_for<0, CY>([&](auto gy) { point<decltype(i)::value - R, decltype(gy)::value, GZ>(ld, acc); });
+    });
+    static_for<0, CX>([&](auto gx) {  // gy in [-R, R + CY)
+      static_for<0, 2 * R + CY>([&](auto i) { point<decltype(gx)::value, decltype(i)::value - R, GZ>(ld, acc); });
+    });
+    static_for<0, R>([&](auto i) {  // gx in [CX, CX + R)
+      static_for<0, CY>([&](auto gy) { point<CX + decltype(i)::value, decltype(gy)::value, GZ>(ld, acc); });
+    });
+  } else {
+    static_for<0, R>([&](auto i) {  // gy in [-R, 0)
+      static_for<0, CX>([&](auto gx) { point<decltype(gx)::value, decltype(i)::value - R, GZ>(ld, acc); });
+    });
+    static_for<0, CY>([&](auto gy) {  // gx in [-R, R + CX)
+      static_for<0, 2 * R + CX>([&](auto i) { point<decltype(i)::value - R, decltype(gy)::value, GZ>(ld, acc); });
+    });
+    static_for<0, R>([&](auto i) {  // gy in [CY, CY + R)
+      static_for<0, CX>([&](auto gx) { point<decltype(gx)::value, CY + decltype(i)::value, GZ>(ld, acc); });
+    });
+  }
+}
+
+template <int GZ, class LD>
+__device__ __forceinline__ void traverse_column(const LD& ld, T (&acc)[NE]) {
+  // the thread's own columns in a z slice outside the centre (Star, 3D)
+  if constexpr (ORIENT == 1) {
+    static_for<0, CX>([&](auto gx) {
+      static_for<0, CY>([&](auto gy) { point<decltype(gx)::value, decltype(gy)::value, GZ>(ld, acc); });
+    });
+  } else {
+    static_for<0, CY>([&](auto gy) {
+      static_for<0, CX>([&](auto gx) { point<decltype(gx)::value, decltype(gy)::value, GZ>(ld, acc); });
+    });
+  }
+}
+
 template <class LD>
 __device__ __forceinline__ void traverse(const LD& ld, T (&acc)[NE]) {
-  T p0[NE];
 #pragma unroll
-  for (int e = 0; e < NE; ++e) {
-    acc[e] = T(0);
-    p0[e] = T(0);
-  }
-  if (DIM == 2) {
-    if (SHAPE == 0) {
-      if (ORIENT == 1) {
-#pragma unroll
-        for (int gx = -R; gx < R + CX; ++gx)
-#pragma unroll
-          for (int gy = -R; gy < R + CY; ++gy) point(ld, acc, p0, gx, gy, 0);
-      } else {
-#pragma unroll
-        for (int gy = -R; gy < R + CY; ++gy)
-#pragma unroll
-          for (int gx = -R; gx < R + CX; ++gx) point(ld, acc, p0, gx, gy, 0);
-      }
-    } else {
-      if (ORIENT == 1) {
-#pragma unroll
-        for (int gx = -R; gx < 0; ++gx)
-#pragma unroll
-          for (int gy = 0; gy < CY; ++gy) point(ld, acc, p0, gx, gy, 0);
-#pragma unroll
-        for (int gx = 0; gx < CX; ++gx)
-#pragma unroll
-          for (int gy = -R; gy < R + CY; ++gy) point(ld, acc, p0, gx, gy, 0);
-#pragma unroll
-        for (int gx = CX; gx < CX + R; ++gx)
-#pragma unroll
-          for (int gy = 0; gy < CY; ++gy) point(ld, acc, p0, gx, gy, 0);
-      } else {
-#pragma unroll
-        for (int gy = -R; gy < 0; ++gy)
-#pragma unroll
-          for (int gx = 0; gx < CX; ++gx) point(ld, acc, p0, gx, gy, 0);
-#pragma unroll
-        for (int gy = 0; gy < CY; ++gy)
-#pragma unroll
-          for (int gx = -R; gx < R + CX; ++gx) point(ld, acc, p0, gx, gy, 0);
-#pragma unroll
-        for (int gy = CY; gy < CY + R; ++gy)
-#pragma unroll
-          for (int gx = 0; gx < CX; ++gx) point(ld, acc, p0, gx, gy, 0);
-      }
-    }
+  for (int e = 0; e < NE; ++e) acc[e] = T(0);
+  if constexpr (DIM == 2) {
+    if constexpr (SHAPE == 0)
+      traverse_slice<0>(ld, acc);
+    else
+      traverse_cross<0>(ld, acc);
+  } else if constexpr (SHAPE == 0) {
+    static_for<0, 2 * R + CZ>([&](auto iz) { traverse_slice<decltype(iz)::value - R>(ld, acc); });
   } else {
-    if (SHAPE == 0) {
-#pragma unroll
-      for (int gz = -R; gz < R + CZ; ++gz) {
-        if (ORIENT == 1) {
-#pragma unroll
-          for (int gx = -R; gx < R + CX; ++gx)
-#pragma unroll
-            for (int gy = -R; gy < R + CY; ++gy) point(ld, acc, p0, gx, gy, gz);
-        } else {
-#pragma unroll
-          for (int gy = -R; gy < R + CY; ++gy)
-#pragma unroll
-            for (int gx = -R; gx < R + CX; ++gx) point(ld, acc, p0, gx, gy, gz);
-        }
-      }
-    } else {
-      // in front of the intersection
-#pragma unroll
-      for (int gz = -R; gz < 0; ++gz) {
-        if (ORIENT == 1) {
-#pragma unroll
-          for (int gx = 0; gx < CX; ++gx)
-#pragma unroll
-            for (int gy = 0; gy < CY; ++gy) point(ld, acc, p0, gx, gy, gz);
-        } else {
-#pragma unroll
-          for (int gy = 0; gy < CY; ++gy)
-#pragma unroll
-            for (int gx = 0; gx < CX; ++gx) point(ld, acc, p0, gx, gy, gz);
-        }
-      }
-      // the cross in the centre slices
-#pragma unroll
-      for (int gz = 0; gz < CZ; ++gz) {
-        if (ORIENT == 1) {
-#pragma unroll
-          for (int gx = -R; gx < 0; ++gx)
-#pragma unroll
-            for (int gy = 0; gy < CY; ++gy) point(ld, acc, p0, gx, gy, gz);
-#pragma unroll
-          for (int gx = 0; gx < CX; ++gx)
-#pragma unroll
-            for (int gy = -R; gy < R + CY; ++gy) point(ld, acc, p0, gx, gy, gz);
-#pragma unroll
-          for (int gx = CX; gx < CX + R; ++gx)
-#pragma unroll
-            for (int gy = 0; gy < CY; ++gy) point(ld, acc, p0, gx, gy, gz);
-        } else {
-#pragma unroll
-          for (int gy = -R; gy < 0; ++gy)
-#pragma unroll
-            for (int gx = 0; gx < CX; ++gx) point(ld, acc, p0, gx, gy, gz);
-#pragma unroll
-          for (int gy = 0; gy < CY; ++gy)
-#pragma unroll
-            for (int gx = -R; gx < R + CX; ++gx) point(ld, acc, p0, gx, gy, gz);
-#pragma unroll
-          for (int gy = CY; gy < CY + R; ++gy)
-#pragma unroll
-            for (int gx = 0; gx < CX; ++gx) point(ld, acc, p0, gx, gy, gz);
-        }
-      }
-      // behind the intersection
-#pragma unroll
-      for (int gz = CZ; gz < CZ + R; ++gz) {
-        if (ORIENT == 1) {
-#pragma unroll
-          for (int gx = 0; gx < CX; ++gx)
-#pragma unroll
-            for (int gy = 0; gy < CY; ++gy) point(ld, acc, p0, gx, gy, gz);
-        } else {
-#pragma unroll
-          for (int gy = 0; gy < CY; ++gy)
-#pragma unroll
-            for (int gx = 0; gx < CX; ++gx) point(ld, acc, p0, gx, gy, gz);
-        }
-      }
-    }
+    static_for<0, R>([&](auto iz) { traverse_column<decltype(iz)::value - R>(ld, acc); });   // in front
+    static_for<0, CZ>([&](auto gz) { traverse_cross<decltype(gz)::value>(ld, acc); });      // centre
+    static_for<0, R>([&](auto iz) { traverse_column<CZ + decltype(iz)::value>(ld, acc); });  // behind
   }
 }
 

@@ -1,0 +1,98 @@
+"""Named benchmark workloads: the stencil configurations the engine is measured on.
+
+Each workload fixes a parameter set, a grid, the number of sweeps of one run, how the seeded
+synthetic input and mask are drawn, and the launch the engine uses for it (the autotuner's choice,
+see ``tuned.json``).  Inputs are numpy ``default_rng(seed)`` draws, so the oracle and the engine
+see identical data.
+"""
+
+from __future__ import annotations
+
+import json
+from dataclasses import dataclass, field
+from pathlib import Path
+
+import numpy as np
+
+from .spec import StencilSpec
+from .stencil import Launch
+
+TUNED_PATH = Path(__file__).resolve().parent / "tuned.json"
+
+
+@dataclass(frozen=True)
+class Workload:
+    name: str
+    spec: StencilSpec
+    grid: tuple                  # raw grid size (nx, ny, nz) before truncation/padding
+    sweeps: int                  # sweeps of one run
+    value_range: tuple = (0.0, 1.0)
+    mask_kind: str | None = None  # "normal_sum1" | "normal_over_S" | None
+    seed: int = 2024
+    launch: Launch = field(default_factory=Launch)
+    reference: tuple = ()        # (coarsening, block) of the reference kernel timed beside it
+
+    def geometry(self):
+        return self.spec.geometry(*self.grid)
+
+    def make_input(self, geom, dtype=np.float64) -> np.ndarray:
+        rng = np.random.default_rng(self.seed)
+        lo, hi = self.value_range
+        a = rng.random(geom.shape, dtype=np.float64 if dtype == np.float64 else np.float32)
+        if (lo, hi) != (0.0, 1.0):
+            a = a * (hi - lo) + lo
+        return a.astype(dtype, copy=False)
+
+    def make_mask(self) -> np.ndarray | None:
+        if self.mask_kind is None or self.spec.coefficients == "Jacobi":
+            return None
+        S = self.spec.stencil_size
+        rng = np.random.default_rng(self.seed + 1)
+        m = rng.standard_normal(S)
+        if self.mask_kind == "normal_sum1":
+            return m / m.sum()
+        return m / S
+
+    def tuned_launch(self) -> Launch:
+        """Launch chosen by the autotuner for this workload (falls back to the built-in default)."""
+        if TUNED_PATH.exists():
+            t = json.loads(TUNED_PATH.read_text()).get(self.name)
+            if t:
+                return Launch(block=tuple(t["block"]), variant=t.get("variant", "auto"),
+                              segments=int(t.get("segments", 0)), depth=int(t.get("depth", 0)))
+        return self.launch
+
+    def tuned_spec(self) -> StencilSpec:
+        """Parameter set with the coarsening chosen by the autotuner (same stencil arithmetic)."""
+        if TUNED_PATH.exists():
+            t = json.loads(TUNED_PATH.read_text()).get(self.name)
+            if t and "coarsening" in t:
+                c = t["coarsening"]
+                return self.spec.replace(cx=c[0], cy=c[1], cz=c[2] if self.spec.dimension == 3 else 1)
+        return self.spec
+
+
+WORKLOADS = {
+    # 2D Box Jacobi r1 (9-point mean), FP64, 4096^2, coarsening 1x1, no alignment, 100 sweeps
+    "2d_box_jacobi_r1_4096": Workload(
+        name="2d_box_jacobi_r1_4096",
+        spec=StencilSpec(dimension=2, neighbourhood="Box", orientation="Row", coefficients="Jacobi", range=1),
+        grid=(4096, 4096, 1), sweeps=100, launch=Launch(block=(64, 4, 1), variant="march"),
+        reference=((1, 1, 1), (128, 1, 1))),
+    # 3D Star Variable r4 (25-point), FP64, 512^3, Read alignment to 16 points, 50 sweeps
+    "3d_star_var_r4_512": Workload(
+        name="3d_star_var_r4_512",
+        spec=StencilSpec(dimension=3, neighbourhood="Star", orientation="Row", coefficients="Variable", range=4,
+                         cx=1, cy=2, cz=2, alignment="Read", cl_size=16),
+        grid=(512, 512, 512), sweeps=50, mask_kind="normal_sum1", launch=Launch(block=(32, 8, 1), variant="march"),
+        reference=((1, 1, 1), (32, 4, 1))),
+    # 2D Box Variable r6 (169-point), FP64, 16384x8192, mask N(0,1)/169, values U[-1,1], 200 sweeps
+    "2d_box_var_r6_16384x8192": Workload(
+        name="2d_box_var_r6_16384x8192",
+        spec=StencilSpec(dimension=2, neighbourhood="Box", orientation="Row", coefficients="Variable", range=6,
+                         cx=2, cy=4),
+        grid=(16384, 8192, 1), sweeps=200, value_range=(-1.0, 1.0), mask_kind="normal_over_S",
+        launch=Launch(block=(32, 4, 1), variant="march"), reference=((2, 2, 1), (64, 2, 1))),
+}
+
+DEFAULT_WORKLOAD = "3d_star_var_r4_512"
