@@ -45,9 +45,11 @@ extern "C" {
 #define TCS_F32 1 /* single-precision grids */
 
 /* Kernel variants. */
-#define TCS_VARIANT_AUTO 0   /* march when the tile fits its TMA/shared-memory limits, else direct */
+#define TCS_VARIANT_AUTO 0   /* pipe, else march, else direct: the first that supports the shape */
 #define TCS_VARIANT_DIRECT 1 /* reference launch geometry, operands through L1 */
 #define TCS_VARIANT_MARCH 2  /* TMA-fed shared-memory ring, CTAs march along the slowest axis */
+#define TCS_VARIANT_PIPE 3   /* persistent streaming sweep, 2R+1 output planes in flight per thread
+                                (3D, and 2D Row orientation; march-axis block dimension 1) */
 
 typedef struct tcs_stencil tcs_stencil; /* opaque handle: one instantiated parameter set */
 
@@ -82,7 +84,8 @@ typedef struct tcs_launch {
   unsigned grid_blocks[3];  /* direct variant: CTA grid; zeros = ceil(gridThreads / block) */
   int variant;              /* TCS_VARIANT_* */
   unsigned segments;        /* march: CTAs along the march axis per tile column (0 = auto) */
-  unsigned depth;           /* march: chunks in flight ahead of the current step (0 = auto) */
+  unsigned depth;           /* march/pipe: chunks in flight ahead of the current step (0 = auto) */
+  unsigned chunk;           /* pipe: planes per ring chunk (0 = auto) */
 } tcs_launch;
 
 /* Resolved launch of one sweep (what tcs_update_grid will run). */
@@ -91,9 +94,10 @@ typedef struct tcs_plan {
   unsigned grid_blocks[3];
   unsigned block[3];
   unsigned dyn_smem;        /* dynamic shared memory per CTA in bytes */
-  unsigned seg_len;         /* march: outputs along the march axis per CTA */
+  unsigned seg_len;         /* march: outputs along the march axis per CTA; pipe: work items per CTA */
   unsigned nslot;           /* march: ring slots */
-  unsigned width;           /* march: shared-memory row width in elements */
+  unsigned width;           /* march/pipe: shared-memory row width in elements */
+  unsigned chunk;           /* pipe: planes per ring chunk */
   unsigned depth;           /* march: chunks in flight */
   unsigned loader;          /* march: 0 = TMA tensor copies, 1 = cp.async element copies */
   int ctas_per_sm;          /* occupancy of the resolved kernel at this shape */
@@ -179,6 +183,11 @@ int tcs_set_dropin_launch(tcs_stencil* h, int variant, unsigned segments, unsign
 /* Instantiate the kernels of a parameter set into the cubin cache without a GPU (NVRTC only);
  * writes the cache path.  Used by the build step so GPU runs start warm. */
 int tcs_precompile(const tcs_spec* spec, char* cubin_path, unsigned path_cap);
+
+/* Same for the pipelined sweep of a launch shape (block bx x by, `chunk` planes per ring slot,
+ * 0 = the planner's default). */
+int tcs_precompile_pipe(const tcs_spec* spec, unsigned bx, unsigned by, unsigned chunk,
+                        char* cubin_path, unsigned path_cap);
 
 /* Number of SMs of the current device. */
 int tcs_device_sm_count(int* out);

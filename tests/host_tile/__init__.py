@@ -19,20 +19,20 @@ _OR = {"Row": 0, "Column": 1}
 _CO = {"Jacobi": 0, "Variable": 1}
 
 
-def build(cfg, precision="f64") -> ctypes.CDLL:
+def build(cfg, precision="f64", source="tile_host.cpp") -> ctypes.CDLL:
     d, sh, o, c, r, cx, cy, cz, al, cl = cfg
     macros = {
         "TCS_T": "double" if precision == "f64" else "float",
         "TCS_DIM": d, "TCS_SHAPE": _SH[sh], "TCS_ORIENT": _OR[o], "TCS_COEFF": _CO[c], "TCS_R": r,
         "TCS_CX": cx, "TCS_CY": cy, "TCS_CZ": cz if d == 3 else 1,
     }
-    src = (HERE / "tile_host.cpp").read_bytes() + (CSRC / "tcs_tile.cuh").read_bytes()
+    src = (HERE / source).read_bytes() + (CSRC / "tcs_tile.cuh").read_bytes()
     tag = hashlib.sha1(src + repr(sorted(macros.items())).encode()).hexdigest()[:16]
     OUT.mkdir(parents=True, exist_ok=True)
     so = OUT / ("tile_%s.so" % tag)
     if not so.exists():
         cmd = ["g++", "-O1", "-std=c++17", "-ffp-contract=off", "-Wno-unknown-pragmas", "-shared", "-fPIC",
-               "-I", str(CSRC)] + ["-D%s=%s" % kv for kv in macros.items()] + [str(HERE / "tile_host.cpp"),
+               "-I", str(CSRC)] + ["-D%s=%s" % kv for kv in macros.items()] + [str(HERE / source),
                                                                               "-o", str(so) + ".tmp"]
         proc = subprocess.run(cmd, capture_output=True, text=True)
         if proc.returncode != 0:
@@ -52,5 +52,24 @@ def sweeps(cfg, a: np.ndarray, grid, left_offset, right_offset, n: int, mask=Non
         lib.tile_sweep(u3(*grid), ctypes.c_uint(left_offset), ctypes.c_uint(right_offset),
                        ctypes.c_int(0 if al == "None" else 1), x.ctypes.data_as(ctypes.c_void_p),
                        y.ctypes.data_as(ctypes.c_void_p), m.ctypes.data_as(ctypes.c_void_p))
+        x, y = y, x
+    return x
+
+
+def pipe_sweeps(cfg, a: np.ndarray, grid, left_offset, right_offset, n: int, mask=None, precision="f64",
+                piece: int = 1 << 30, unroll: int = 0):
+    """n sweeps through the host build of the pipelined sweep (pieces of `piece` planes)."""
+    lib = build(cfg, precision, "pipe_host.cpp")
+    d, sh, o, c, r, cx, cy, cz, al, cl = cfg
+    unroll = unroll or 2 * r + 1
+    x = np.ascontiguousarray(a).copy()
+    y = x.copy()
+    m = np.ascontiguousarray(np.zeros(1) if mask is None else np.asarray(mask, dtype=np.float64))
+    u3 = ctypes.c_uint * 3
+    for _ in range(n):
+        lib.pipe_sweep(u3(*grid), ctypes.c_uint(left_offset), ctypes.c_uint(right_offset),
+                       ctypes.c_int(0 if al == "None" else 1), x.ctypes.data_as(ctypes.c_void_p),
+                       y.ctypes.data_as(ctypes.c_void_p), m.ctypes.data_as(ctypes.c_void_p), ctypes.c_uint(piece),
+                       ctypes.c_uint(unroll))
         x, y = y, x
     return x

@@ -1,0 +1,87 @@
+// Host build of the pipelined sweep's per-thread arithmetic (test harness).
+//
+// Drives tcs::pipe_plane (threadcoarsenedstencilgenerator_b200/csrc/tcs_tile.cuh) exactly as the
+// tcs_pipe kernel does: every thread tile streams the input planes ms-R .. me+R-1 of its column,
+// keeps 2R+1 output planes in flight in the slots (t - k) mod (2R+1), and stores output pi - 2R
+// after input plane pi.  Pieces start at arbitrary planes (`piece` splits the march axis) to
+// exercise the pipeline restart.  Built with -ffp-contract=off like tile_host.cpp.
+#include <cmath>
+#include <cstring>
+
+#define __device__
+#define __host__
+#define __forceinline__ inline
+#define __constant__
+static inline double __fma_rn(double a, double b, double c) { return std::fma(a, b, c); }
+static inline float __fmaf_rn(float a, float b, float c) { return std::fmaf(a, b, c); }
+
+#include "tcs_tile.cuh"
+
+// Plane reader with the kernel's interface (pairs are just two scalar loads here).
+struct HostPlane {
+  const T* b;
+  long long pitch;
+  static constexpr bool pair_aligned(int gx) { return ((gx % 2) + 2) % 2 == 0; }
+  template <int GX, int GY>
+  T one() const {
+    return b[GX + GY * pitch];
+  }
+  template <int GX, int GY>
+  void two(T& a, T& c) const {
+    a = b[GX + GY * pitch];
+    c = b[GX + 1 + GY * pitch];
+  }
+};
+
+extern "C" int pipe_sweep(const unsigned grid[3], unsigned left_offset, unsigned right_offset,
+                          int aligned, const T* in, T* out, const double* mask, unsigned piece,
+                          unsigned unroll) {
+  using namespace tcs;
+  constexpr int NP2 = 2 * R + 1;
+  if (COEFF == 1)
+    for (int k = 0; k < S; ++k) tcs_mask[k] = (T)mask[k];
+  const long long xdim = grid[0], ydim = grid[1], zdim = DIM == 3 ? grid[2] : 1;
+  const long long plane = DIM == 3 ? xdim * ydim : xdim;  // stride of the march axis
+  const long long x_lim = xdim - R - (aligned ? right_offset : 0);
+  const long long y_lim = ydim - R, z_lim = DIM == 3 ? zdim - R : 1;
+  const long long m_lim = DIM == 3 ? z_lim : y_lim;       // march-axis interior bound
+  const long long y_step = DIM == 3 ? CY : 1;
+  const long long y_end = DIM == 3 ? y_lim : R + 1;
+  for (long long y = R; DIM == 3 ? (y + CY - 1 < y_end) : (y < y_end); y += y_step)
+    for (long long x = R + left_offset; x + CX - 1 < x_lim; x += CX)
+      for (long long ms = R; ms < m_lim; ms += piece) {
+        const long long me = (ms + piece < m_lim) ? ms + piece : m_lim;
+        const long long np = me - ms + 2 * R;
+        T acc[NP2][NEP];
+        // super-steps of `unroll` planes; slots re-aligned after each, as in tcs_pipe
+        for (long long pi = 0; pi < np; ++pi) {
+          const long long p = ms - R + pi;
+          const T* base = in + x + (DIM == 3 ? y * xdim : 0) + p * plane;
+          const HostPlane ld{base, xdim};
+          const int t = (int)(pi % unroll);
+          auto slot = [&](auto kk) -> T(&)[NEP] {
+            constexpr int k = decltype(kk)::value;
+            return acc[((t - k) % NP2 + NP2) % NP2];
+          };
+          pipe_plane(ld, slot);
+          const long long op = pi - 2 * R;
+          if (op >= 0 && op < me - ms) {
+            T(&done)[NEP] = acc[((t - 2 * R) % NP2 + NP2) % NP2];
+            constexpr T c = T(1) / T(S);
+            T* o = out + x + (DIM == 3 ? y * xdim : 0) + (ms + op) * plane;
+            for (int ey = 0; ey < (DIM == 3 ? CY : 1); ++ey)
+              for (int ex = 0; ex < CX; ++ex) {
+                const int e = ex + ey * CX;
+                o[ex + ey * xdim] = (COEFF == 0) ? done[e] * c : done[e];
+              }
+          }
+          if (t == (int)unroll - 1 && unroll % NP2 != 0) {
+            T tmp[NP2][NEP];
+            std::memcpy(tmp, acc, sizeof(acc));
+            for (int m = 0; m < NP2; ++m)
+              for (int e = 0; e < NEP; ++e) acc[m][e] = tmp[(m + unroll) % NP2][e];
+          }
+        }
+      }
+  return 0;
+}

@@ -10,6 +10,7 @@
 #include <cstring>
 
 #define __device__
+#define __host__
 #define __forceinline__ inline
 #define __constant__
 static inline double __fma_rn(double a, double b, double c) { return std::fma(a, b, c); }

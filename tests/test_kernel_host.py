@@ -10,6 +10,7 @@ import pytest
 
 import host_tile
 import march_model
+import pipe_model
 import oracle as O
 from oracle import ref_configs
 from make_golden import fixture_input, HERE as GOLDEN
@@ -83,4 +84,61 @@ def test_march_addressing_model(case, es):
         for depth in (0, 1, 3):
             cnt = march_model.simulate(d, sh, r, c, blk, grid, g.left_offset, g.right_offset, al != "None", es=es,
                                        segments=seg, depth=depth, num_sms=5)
+            assert cnt is None or cnt > 0
+
+
+PIPE_CFGS = [c for c in ref_configs.PARITY if not (c[0] == 2 and c[2] == "Column")]
+
+
+@pytest.mark.parametrize("cfg", PIPE_CFGS, ids=ref_configs.key)
+def test_pipe_arithmetic_matches_reference_fixture(cfg):
+    f = np.load(GOLDEN / ("%s.npz" % ref_configs.key(cfg)))
+    spec, raw, g, a, mask = fixture_input(cfg, int(f["seed"]))
+    for piece, unroll in ((1 << 30, 0), (5, 1), (7, 2), (4, 3)):
+        if unroll > 2 * cfg[4] + 1:
+            continue
+        out = host_tile.pipe_sweeps(cfg, a, g.grid, g.left_offset, g.right_offset, int(f["nsweeps"]), mask,
+                                    piece=piece, unroll=unroll)
+        assert np.array_equal(out, f["out"])
+
+
+@pytest.mark.parametrize("precision", ["f64", "f32"])
+@pytest.mark.parametrize("cfg", [c for c in _random_cfgs(10, 17) if not (c[0] == 2 and c[2] == "Column")],
+                         ids=ref_configs.key)
+def test_pipe_arithmetic_matches_oracle_random(cfg, precision):
+    d, sh, o, c, r, cx, cy, cz, al, cl = cfg
+    spec = O.make_spec(*cfg)
+    g = O.geometry(spec, 20 + 2 * r, 17 + 2 * r, 13 + 2 * r)
+    rng = np.random.default_rng(8)
+    shape = (g.grid[1], g.grid[0]) if d == 2 else (g.grid[2], g.grid[1], g.grid[0])
+    a = rng.random(shape).astype(np.float64 if precision == "f64" else np.float32)
+    mask = rng.standard_normal(O.stencil_size(spec)) if c == "Variable" else None
+    want = O.sweeps(spec, a, 2, g.right_offset, mask)
+    got = host_tile.pipe_sweeps(cfg, a, g.grid, g.left_offset, g.right_offset, 2, mask, precision, piece=6,
+                                unroll=1 + (r % 2))
+    assert np.array_equal(got, want)
+
+
+PIPE_CASES = [
+    (2, "Box", 1, (1, 1, 1), (32, 1, 1), (70, 23, 1), "None", 0),
+    (2, "Box", 6, (2, 1, 1), (16, 1, 1), (80, 40, 1), "None", 0),
+    (2, "Star", 3, (2, 1, 1), (8, 1, 1), (61, 45, 1), "Write", 8),
+    (2, "Star", 1, (1, 1, 1), (64, 1, 1), (37, 29, 1), "Read", 16),
+    (3, "Star", 4, (2, 2, 1), (8, 4, 1), (44, 29, 21), "Read", 16),
+    (3, "Star", 2, (1, 2, 1), (16, 2, 1), (31, 29, 27), "None", 0),
+    (3, "Box", 1, (2, 1, 1), (8, 3, 1), (35, 26, 22), "Write", 16),
+    (3, "Box", 2, (1, 1, 1), (16, 8, 1), (22, 21, 20), "None", 0),
+]
+
+
+@pytest.mark.parametrize("case", PIPE_CASES, ids=lambda c: "%dD_%s_r%d_c%s_b%s" % (c[0], c[1], c[2], c[3], c[4]))
+@pytest.mark.parametrize("es", [8, 4])
+def test_pipe_addressing_model(case, es):
+    d, sh, r, c, blk, n, al, cl = case
+    spec = O.make_spec(d, sh, "Row", "Jacobi", r, c[0], c[1], c[2], al, cl)
+    g = O.geometry(spec, *n)
+    for nctas in (0, 1, 3, 7):
+        for chunk, depth in ((0, 0), (1, 1), (4, 2)):
+            cnt = pipe_model.simulate(d, sh, r, c, blk, g.grid, g.left_offset, g.right_offset, al != "None",
+                                      es=es, num_sms=2, occ=2, chunk=chunk, depth=depth, nctas=nctas)
             assert cnt is None or cnt > 0

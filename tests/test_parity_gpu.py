@@ -17,8 +17,10 @@ from make_golden import fixture_input, HERE as GOLDEN
 
 pytestmark = pytest.mark.gpu
 
-BLOCKS_2D = [(8, 4, 1), (32, 4, 1), (64, 1, 1), (16, 8, 1), (1, 32, 1)]
-BLOCKS_3D = [(8, 4, 2), (32, 4, 1), (16, 4, 2), (8, 8, 1), (64, 2, 1)]
+BLOCKS_2D = [(8, 4, 1), (32, 4, 1), (64, 1, 1), (16, 8, 1), (1, 32, 1), (32, 1, 1), (16, 1, 1)]
+BLOCKS_3D = [(8, 4, 2), (32, 4, 1), (16, 4, 2), (8, 8, 1), (64, 2, 1), (16, 2, 1)]
+PIPE_BLOCKS_2D = [(64, 1, 1), (32, 1, 1), (16, 1, 1)]
+PIPE_BLOCKS_3D = [(32, 4, 1), (8, 8, 1), (16, 2, 1)]
 
 
 @pytest.fixture(scope="module")
@@ -38,7 +40,7 @@ def _run_all_variants(tcs, cfg, a, g, n, mask, precision="f64"):
     assert geom.grid == tuple(g.grid)
     results = []
     blocks = BLOCKS_2D if cfg[0] == 2 else BLOCKS_3D
-    for variant in ("direct", "march"):
+    for variant in ("direct", "march", "pipe"):
         for b in blocks:
             launch = tcs.Launch(block=b, variant=variant)
             try:
@@ -49,6 +51,8 @@ def _run_all_variants(tcs, cfg, a, g, n, mask, precision="f64"):
             results.append(((variant, b), res, host))
     assert st.device_status() == 0
     assert any(v == "march" for (v, _), _, _ in results), "no march shape ran for %s" % (cfg,)
+    if not (cfg[0] == 2 and cfg[2] == "Column"):
+        assert any(v == "pipe" for (v, _), _, _ in results), "no pipe shape ran for %s" % (cfg,)
     return geom, results
 
 

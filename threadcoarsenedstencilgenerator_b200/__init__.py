@@ -8,7 +8,7 @@ include/tcs.h via ctypes), ``LaunchUpdateGrid`` (the reference's launchUpdateGri
 
 from ._lib import CudaErrorInvalidValue, TcsError, UnsupportedLaunch
 from .spec import Geometry, StencilSpec
-from .stencil import Launch, Plan, Stencil, device_sm_count, precompile
+from .stencil import Launch, Plan, Stencil, device_sm_count, precompile, precompile_pipe
 from .launch import LaunchUpdateGrid
 
 __all__ = [
@@ -23,4 +23,5 @@ __all__ = [
     "UnsupportedLaunch",
     "device_sm_count",
     "precompile",
+    "precompile_pipe",
 ]

@@ -22,6 +22,7 @@ TCS_ERR_NO_DEVICE = 6
 VARIANT_AUTO = 0
 VARIANT_DIRECT = 1
 VARIANT_MARCH = 2
+VARIANT_PIPE = 3
 
 
 class TcsError(RuntimeError):
@@ -74,6 +75,7 @@ class CLaunch(ctypes.Structure):
         ("variant", ctypes.c_int),
         ("segments", ctypes.c_uint),
         ("depth", ctypes.c_uint),
+        ("chunk", ctypes.c_uint),
     ]
 
 
@@ -86,6 +88,7 @@ class CPlan(ctypes.Structure):
         ("seg_len", ctypes.c_uint),
         ("nslot", ctypes.c_uint),
         ("width", ctypes.c_uint),
+        ("chunk", ctypes.c_uint),
         ("depth", ctypes.c_uint),
         ("loader", ctypes.c_uint),
         ("ctas_per_sm", ctypes.c_int),
@@ -123,6 +126,7 @@ SIGNATURES = {
     "tcs_device_status": [_vp, _P(_u), _i],
     "tcs_set_dropin_launch": [_vp, _i, _u, _u],
     "tcs_precompile": [_P(CSpec), ctypes.c_char_p, _u],
+    "tcs_precompile_pipe": [_P(CSpec), _u, _u, _u, ctypes.c_char_p, _u],
     "tcs_device_sm_count": [_P(_i)],
 }
 _RESTYPE = {"tcs_last_error": ctypes.c_char_p}

@@ -204,8 +204,20 @@ std::string cache_dir() {
   return d;
 }
 
-std::string instance_macros(const tcs_spec& s) {
+// Compile-time launch shape of a pipelined-sweep module (tcs_pipe).
+struct PipeKey {
+  unsigned bx, by, ch, lshift, unroll;
+  bool operator==(const PipeKey& o) const {
+    return bx == o.bx && by == o.by && ch == o.ch && lshift == o.lshift && unroll == o.unroll;
+  }
+};
+
+std::string instance_macros(const tcs_spec& s, const PipeKey* pk) {
   std::ostringstream m;
+  if (pk)
+    m << "#define TCS_PIPE 1\n#define TCS_BX " << pk->bx << "\n#define TCS_BY " << pk->by
+      << "\n#define TCS_CH " << pk->ch << "\n#define TCS_LSHIFT " << pk->lshift
+      << "\n#define TCS_UNROLL " << pk->unroll << "\n";
   m << "#define TCS_T " << (s.precision == TCS_F64 ? "double" : "float") << "\n"
     << "#define TCS_DIM " << s.dimension << "\n"
     << "#define TCS_SHAPE " << s.neighbourhood << "\n"
@@ -220,8 +232,9 @@ std::string instance_macros(const tcs_spec& s) {
 
 std::mutex g_compile_mu;
 
-int instantiate(const tcs_spec& s, std::vector<char>& cubin, std::string* path_out) {
-  const std::string src = instance_macros(s) + "#include \"tcs_kernels.cuh\"\n";
+int instantiate(const tcs_spec& s, const PipeKey* pk, std::vector<char>& cubin,
+                std::string* path_out) {
+  const std::string src = instance_macros(s, pk) + "#include \"tcs_kernels.cuh\"\n";
   const char* opts[] = {"--gpu-architecture=sm_100a", "--std=c++17", "--fmad=false",
                         "-lineinfo", "--device-as-default-execution-space"};
   const int nopts = sizeof(opts) / sizeof(opts[0]);
@@ -284,6 +297,28 @@ struct TcsGeo {
 };
 static_assert(sizeof(TcsGeo) == 56, "TcsGeo layout");
 
+// Host mirror of the device TcsPipeGeo (same layout).
+struct TcsPipeGeo {
+  unsigned long long xdim, ydim, zdim;
+  unsigned long long total, per_cta;
+  unsigned x0, x_lim;
+  unsigned y_lim, z_lim;
+  unsigned ntx, m;
+  unsigned nslot, loader;
+};
+static_assert(sizeof(TcsPipeGeo) == 72, "TcsPipeGeo layout");
+
+// One loaded pipelined-sweep module (its own constant mask and status word).
+struct PipeMod {
+  PipeKey key;
+  CUmodule mod = nullptr;
+  CUfunction f = nullptr;
+  CUdeviceptr mask_ptr = 0;
+  size_t mask_bytes = 0;
+  CUdeviceptr status_ptr = 0;
+  int smem_attr = 0;
+};
+
 struct MapEntry {
   const void* ptr;
   unsigned long long dims[3];
@@ -307,6 +342,8 @@ struct tcs_stencil {
   int march_smem_attr = 0;
   int dropin_variant = TCS_VARIANT_AUTO;  // variant used by tcs_benchmark_update_grid
   unsigned dropin_segments = 0, dropin_depth = 0;
+  std::vector<double> mask_host;          // last mask uploaded (copied into new pipe modules)
+  std::vector<PipeMod*> pipes;            // pipelined-sweep modules, one per launch shape
   std::mutex mu;
   std::vector<MapEntry> maps;
 };
@@ -316,6 +353,9 @@ namespace {
 struct Resolved {
   int variant = 0;
   TcsGeo geo{};
+  TcsPipeGeo pgeo{};
+  PipeMod* pipe = nullptr;
+  unsigned chunk = 0;
   unsigned grid[3] = {1, 1, 1};
   unsigned block[3] = {1, 1, 1};
   unsigned smem = 0;
@@ -501,6 +541,212 @@ int resolve_march(tcs_stencil* h, const TcsGeo& g, const tcs_launch* L, Resolved
   return TCS_OK;
 }
 
+int upload_mask(tcs_stencil* h, CUdeviceptr dst) {
+  const unsigned n = (unsigned)h->mask_host.size();
+  if (n == 0 || h->spec.coefficients == TCS_JACOBI) return TCS_OK;
+  if (h->spec.precision == TCS_F64) {
+    TCS_RT(cudaMemcpy((void*)dst, h->mask_host.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
+  } else {
+    std::vector<float> f(h->mask_host.begin(), h->mask_host.end());
+    TCS_RT(cudaMemcpy((void*)dst, f.data(), sizeof(float) * n, cudaMemcpyHostToDevice));
+  }
+  return TCS_OK;
+}
+
+// Pipelined-sweep module for a launch shape: instantiate (NVRTC, cached) and load on first use.
+int pipe_module(tcs_stencil* h, const PipeKey& key, PipeMod** out) {
+  std::lock_guard<std::mutex> lock(h->mu);
+  for (PipeMod* p : h->pipes)
+    if (p->key == key) {
+      *out = p;
+      return TCS_OK;
+    }
+  std::vector<char> cubin;
+  int rc = instantiate(h->spec, &key, cubin, nullptr);
+  if (rc) return rc;
+  PipeMod* pm = new PipeMod();
+  pm->key = key;
+  CUresult cr = g_drv.ModuleLoadData(&pm->mod, cubin.data());
+  if (cr != CUDA_SUCCESS) {
+    delete pm;
+    return fail(TCS_ERR_CUDA, "cuModuleLoadData (pipe): " + cu_msg(cr));
+  }
+  size_t bytes = 0;
+  if ((cr = g_drv.ModuleGetFunction(&pm->f, pm->mod, "tcs_pipe")) != CUDA_SUCCESS ||
+      (cr = g_drv.ModuleGetGlobal(&pm->mask_ptr, &pm->mask_bytes, pm->mod, "tcs_mask")) != CUDA_SUCCESS ||
+      (cr = g_drv.ModuleGetGlobal(&pm->status_ptr, &bytes, pm->mod, "tcs_status")) != CUDA_SUCCESS) {
+    g_drv.ModuleUnload(pm->mod);
+    delete pm;
+    return fail(TCS_ERR_CUDA, "pipe module symbols: " + cu_msg(cr));
+  }
+  cudaMemset((void*)pm->status_ptr, 0, sizeof(unsigned));
+  rc = upload_mask(h, pm->mask_ptr);
+  if (rc) {
+    g_drv.ModuleUnload(pm->mod);
+    delete pm;
+    return rc;
+  }
+  h->pipes.push_back(pm);
+  *out = pm;
+  return TCS_OK;
+}
+
+// Default planes per ring chunk (a power of two): one plane in 3D, about 4 KB of rows in 2D.
+unsigned pipe_auto_chunk(const tcs_spec& s, unsigned tx) {
+  const unsigned es = (unsigned)elem_size(s), vec = 16u / es;
+  if (s.dimension == 3) return 1u;
+  const unsigned row_bytes = (tx + 2u * (unsigned)s.range + vec) * es;
+  const unsigned want = std::max(1u, std::min(16u, cdiv(4096, row_bytes)));
+  unsigned ch = 1;
+  while (ch * 2 <= want) ch *= 2;
+  return ch;
+}
+
+// Input planes per unrolled loop body: as many as fit an instruction budget of about 2000
+// fused multiply-adds (one plane applies S terms to each of the thread's outputs), at most 2R+1.
+unsigned pipe_auto_unroll(const tcs_spec& s) {
+  const unsigned S = stencil_size_of(s);
+  const unsigned nep = (unsigned)s.cx * (s.dimension == 3 ? (unsigned)s.cy : 1u);
+  const unsigned n = 2u * (unsigned)s.range + 1u;
+  return std::max(1u, std::min(n, 2000u / std::max(1u, S * nep)));
+}
+
+// Compile-time row width of a pipe instantiation (tcs::pipe_width in tcs_kernels.cuh).
+unsigned pipe_width(unsigned tx, unsigned R, unsigned lshift, unsigned vec, unsigned ch,
+                    unsigned rows, unsigned es) {
+  unsigned w = ((tx + 2 * R + lshift + vec - 1) / vec) * vec;
+  while ((ch * rows * w * es) % 128 != 0) w += vec;
+  return w;
+}
+
+int resolve_pipe(tcs_stencil* h, const TcsGeo& g, const tcs_launch* L, Resolved& out) {
+  const tcs_spec& s = h->spec;
+  const unsigned R = (unsigned)s.range;
+  const unsigned es = (unsigned)elem_size(s);
+  const unsigned vec = 16u / es;
+  if (s.dimension == 2 && s.orientation == TCS_COLUMN)
+    return fail(TCS_ERR_UNSUPPORTED, "2D Column orientation is not pipelined");
+  if (s.dimension == 2 && (L->block[1] != 1 || L->block[2] != 1))
+    return fail(TCS_ERR_UNSUPPORTED, "pipe: 2D blocks are (bx, 1, 1)");
+  if (s.dimension == 3 && L->block[2] != 1)
+    return fail(TCS_ERR_UNSUPPORTED, "pipe: 3D blocks are (bx, by, 1)");
+  const unsigned TX = L->block[0] * s.cx;
+  if (TX % vec != 0) return fail(TCS_ERR_UNSUPPORTED, "pipe: tile width not a multiple of 16 bytes");
+  const unsigned TY = s.dimension == 3 ? L->block[1] * s.cy : 1;
+  const unsigned rows = s.dimension == 3 ? TY + 2 * R : 1;
+  const unsigned lshift = h->left_off % vec;
+  const unsigned ch = L->chunk ? L->chunk : pipe_auto_chunk(s, TX);
+  if ((ch & (ch - 1)) != 0) return fail(TCS_ERR_UNSUPPORTED, "pipe: planes per chunk must be a power of two");
+  const unsigned W = pipe_width(TX, R, lshift, vec, ch, rows, es);
+  if (W > 256 || rows > 256 || ch > 256)
+    return fail(TCS_ERR_UNSUPPORTED, "pipe: tile exceeds the 256-element TMA box limit");
+  const unsigned chunk_bytes = ch * rows * W * es;
+  PipeKey key{L->block[0], s.dimension == 3 ? L->block[1] : 1u, ch, lshift, pipe_auto_unroll(s)};
+  PipeMod* pm = nullptr;
+  int rc = pipe_module(h, key, &pm);
+  if (rc) return rc;
+  const int nthr = (int)(L->block[0] * L->block[1]);
+  int maxthr = 0;
+  TCS_CU(g_drv.FuncGetAttribute(&maxthr, CU_FUNC_ATTRIBUTE_MAX_THREADS_PER_BLOCK, pm->f));
+  if (nthr > maxthr) return fail(TCS_ERR_UNSUPPORTED, "pipe: block exceeds the kernel's thread limit");
+  const unsigned bar_area = 256;  // barriers + alignment slack, rounded
+  unsigned depth = L->depth;
+  if (depth == 0) {
+    // Enough chunks in flight to keep about 96 KB of input moving per SM at the occupancy the
+    // registers allow, within the shared memory those CTAs share.
+    int occ_r = 0;
+    TCS_CU(g_drv.OccMaxActive(&occ_r, pm->f, nthr, 0));
+    occ_r = std::max(1, occ_r);
+    const unsigned smem_sm = 228u * 1024u;
+    depth = 2;
+    for (unsigned d = 2; d <= 16; ++d) {
+      const unsigned per_cta = bar_area + (1 + d) * chunk_bytes;
+      const unsigned fit = std::min<unsigned>((unsigned)occ_r, smem_sm / per_cta);
+      if (fit == 0 || per_cta > (unsigned)h->smem_optin) break;
+      depth = d;
+      if ((unsigned long long)fit * d * chunk_bytes >= 96ull * 1024ull &&
+          fit >= std::min<unsigned>((unsigned)occ_r, 2u))
+        break;
+    }
+  }
+  unsigned smem = 0, nslot = 0;
+  for (;;) {
+    nslot = 1 + depth;
+    smem = ((nslot * 8 + 127) / 128) * 128 + 128 + nslot * chunk_bytes;
+    if (smem <= (unsigned)h->smem_optin || depth == 1) break;
+    --depth;
+  }
+  if (smem > (unsigned)h->smem_optin)
+    return fail(TCS_ERR_UNSUPPORTED, "pipe: ring does not fit in shared memory");
+  {
+    std::lock_guard<std::mutex> lock(h->mu);
+    if ((int)smem > pm->smem_attr) {
+      TCS_CU(g_drv.FuncSetAttribute(pm->f, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, (int)smem));
+      pm->smem_attr = (int)smem;
+    }
+  }
+  int occ = 0;
+  TCS_CU(g_drv.OccMaxActive(&occ, pm->f, nthr, smem));
+  if (occ < 1) return fail(TCS_ERR_UNSUPPORTED, "pipe kernel cannot be resident at this shape");
+  const unsigned long long ex = g.x_lim > g.x0 ? g.x_lim - g.x0 : 0;
+  const unsigned long long ey = g.y_lim - R;
+  const unsigned ntx = std::max(1u, cdiv(ex, TX));
+  unsigned nty = 1;
+  unsigned long long M = ey;
+  if (s.dimension == 3) {
+    nty = std::max(1u, cdiv(ey, TY));
+    M = g.z_lim - R;
+  }
+  const unsigned long long total = (unsigned long long)ntx * nty * M;
+  unsigned long long nctas = (unsigned long long)h->num_sms * (unsigned)occ;
+  if (L->segments) nctas = L->segments;  // explicit CTA count
+  const unsigned long long per = std::max<unsigned long long>(1, (total + nctas - 1) / nctas);
+  const unsigned long long grid = std::max<unsigned long long>(1, (total + per - 1) / per);
+  if (grid > 0x7fffffffull) return fail(TCS_ERR_UNSUPPORTED, "pipe grid too large");
+  out.variant = TCS_VARIANT_PIPE;
+  out.geo = g;
+  out.geo.width = W;
+  out.geo.nslot = nslot;
+  out.pipe = pm;
+  out.chunk = ch;
+  TcsPipeGeo& pg = out.pgeo;
+  pg = TcsPipeGeo{};
+  pg.xdim = g.xdim;
+  pg.ydim = g.ydim;
+  pg.zdim = g.zdim;
+  pg.total = total;
+  pg.per_cta = per;
+  pg.x0 = g.x0;
+  pg.x_lim = g.x_lim;
+  pg.y_lim = g.y_lim;
+  pg.z_lim = g.z_lim;
+  pg.ntx = ntx;
+  pg.m = (unsigned)M;
+  pg.nslot = nslot;
+  pg.loader = ((g.xdim * es) % 16 == 0) ? 0u : 1u;
+  out.geo.loader = pg.loader;
+  out.geo.seg = (unsigned)std::min<unsigned long long>(per, 0xffffffffull);
+  out.grid[0] = (unsigned)grid;
+  out.grid[1] = 1;
+  out.grid[2] = 1;
+  out.block[0] = L->block[0];
+  out.block[1] = s.dimension == 3 ? L->block[1] : 1;
+  out.block[2] = 1;
+  if (s.dimension == 2) {
+    out.box[0] = W;
+    out.box[1] = ch;
+    out.box[2] = 1;
+  } else {
+    out.box[0] = W;
+    out.box[1] = rows;
+    out.box[2] = ch;
+  }
+  out.smem = smem;
+  out.depth = depth;
+  out.occ = occ;
+  return TCS_OK;
+}
+
 int resolve(tcs_stencil* h, const unsigned grid[3], unsigned right_offset, const tcs_launch* L,
             Resolved& out) {
   if (!h || !L) return fail(TCS_ERR_INVALID_VALUE, "NULL handle or launch");
@@ -511,8 +757,12 @@ int resolve(tcs_stencil* h, const unsigned grid[3], unsigned right_offset, const
   if (rc) return rc;
   if (L->variant == TCS_VARIANT_DIRECT) return resolve_direct(h, g, L, out);
   if (L->variant == TCS_VARIANT_MARCH) return resolve_march(h, g, L, out);
+  if (L->variant == TCS_VARIANT_PIPE) return resolve_pipe(h, g, L, out);
   if (L->variant != TCS_VARIANT_AUTO) return fail(TCS_ERR_INVALID_VALUE, "unknown variant");
   const std::string saved = g_err;
+  rc = resolve_pipe(h, g, L, out);
+  if (rc == TCS_OK) return rc;
+  if (rc != TCS_ERR_UNSUPPORTED) return rc;
   rc = resolve_march(h, g, L, out);
   if (rc == TCS_OK) return rc;
   if (rc != TCS_ERR_UNSUPPORTED) return rc;
@@ -564,6 +814,23 @@ int launch_resolved(tcs_stencil* h, const Resolved& r, const void* in, void* out
     void* args[] = {&pin, &pout, &geo};
     TCS_CU(g_drv.LaunchKernel(h->f_direct, r.grid[0], r.grid[1], r.grid[2], r.block[0],
                               r.block[1], r.block[2], 0, st, args, nullptr));
+    return TCS_OK;
+  }
+  if (r.variant == TCS_VARIANT_PIPE) {
+    TcsPipeGeo pg = r.pgeo;
+    if (pg.loader == 0 && reinterpret_cast<uintptr_t>(in) % 16 != 0) pg.loader = 1;
+    alignas(64) CUtensorMap pmap;
+    std::memset(&pmap, 0, sizeof(pmap));
+    if (pg.loader == 0) {
+      CUtensorMap* map = nullptr;
+      int rc = tensor_map(h, in, r, &map);
+      if (rc) return rc;
+      pmap = *map;
+    }
+    CUdeviceptr pin = (CUdeviceptr)in, pout = (CUdeviceptr)out;
+    void* args[] = {&pmap, &pin, &pout, &pg};
+    TCS_CU(g_drv.LaunchKernel(r.pipe->f, r.grid[0], 1, 1, r.block[0], r.block[1], 1, r.smem, st,
+                              args, nullptr));
     return TCS_OK;
   }
   // The TMA loader also needs a 16-byte aligned base address; otherwise copy with cp.async.
@@ -666,13 +933,14 @@ int tcs_create(const tcs_spec* spec, tcs_stencil** out) {
   std::vector<char> cubin;
   tcs_spec canon = *spec;
   if (canon.dimension == 2) canon.cz = 1;
-  rc = instantiate(canon, cubin, nullptr);
+  rc = instantiate(canon, nullptr, cubin, nullptr);
   if (rc) return rc;
   tcs_stencil* h = new tcs_stencil();
   h->spec = canon;
   h->S = stencil_size_of(h->spec);
   h->flops = h->spec.coefficients == TCS_JACOBI ? h->S : 2 * h->S - 1;
   h->left_off = left_offset_of(h->spec);
+  h->mask_host.assign(h->S, 0.0);
   auto bail = [&](int code) {
     if (h->mod) g_drv.ModuleUnload(h->mod);
     delete h;
@@ -700,6 +968,10 @@ int tcs_create(const tcs_spec* spec, tcs_stencil** out) {
 
 int tcs_destroy(tcs_stencil* h) {
   if (!h) return TCS_OK;
+  for (PipeMod* p : h->pipes) {
+    if (p->mod && g_drv.ModuleUnload) g_drv.ModuleUnload(p->mod);
+    delete p;
+  }
   if (h->mod && g_drv.ModuleUnload) g_drv.ModuleUnload(h->mod);
   delete h;
   return TCS_OK;
@@ -717,11 +989,12 @@ int tcs_copy_mask(tcs_stencil* h, const double* mask, unsigned n) {
   if (!mask && n) return fail(TCS_ERR_INVALID_VALUE, "NULL mask");
   if (n > h->S)
     return fail(TCS_ERR_INVALID_VALUE, "mask larger than the stencil (" + std::to_string(h->S) + ")");
-  if (h->spec.precision == TCS_F64) {
-    TCS_RT(cudaMemcpy((void*)h->mask_ptr, mask, sizeof(double) * n, cudaMemcpyHostToDevice));
-  } else {
-    std::vector<float> f(mask, mask + n);
-    TCS_RT(cudaMemcpy((void*)h->mask_ptr, f.data(), sizeof(float) * n, cudaMemcpyHostToDevice));
+  std::copy(mask, mask + n, h->mask_host.begin());
+  int rc = upload_mask(h, h->mask_ptr);
+  if (rc) return rc;
+  for (PipeMod* p : h->pipes) {
+    rc = upload_mask(h, p->mask_ptr);
+    if (rc) return rc;
   }
   TCS_RT(cudaDeviceSynchronize());
   return TCS_OK;
@@ -751,6 +1024,7 @@ int tcs_plan_launch(tcs_stencil* h, const unsigned grid[3], unsigned right_offse
     p.seg_len = r.geo.seg;
     p.nslot = r.geo.nslot;
     p.width = r.geo.width;
+    p.chunk = r.chunk;
     p.depth = r.depth;
     p.loader = r.geo.loader;
     p.ctas_per_sm = r.occ;
@@ -887,9 +1161,14 @@ int tcs_launch_init(tcs_stencil* h, const unsigned grid[3], const unsigned block
 
 int tcs_device_status(tcs_stencil* h, unsigned* status, int clear) {
   if (!h) return fail(TCS_ERR_INVALID_VALUE, "NULL handle");
-  unsigned v = 0;
+  unsigned v = 0, w = 0;
   TCS_RT(cudaMemcpy(&v, (void*)h->status_ptr, sizeof(v), cudaMemcpyDeviceToHost));
   if (clear) TCS_RT(cudaMemset((void*)h->status_ptr, 0, sizeof(unsigned)));
+  for (PipeMod* p : h->pipes) {
+    TCS_RT(cudaMemcpy(&w, (void*)p->status_ptr, sizeof(w), cudaMemcpyDeviceToHost));
+    if (clear) TCS_RT(cudaMemset((void*)p->status_ptr, 0, sizeof(unsigned)));
+    v |= w;
+  }
   if (status) *status = v;
   return TCS_OK;
 }
@@ -911,7 +1190,32 @@ int tcs_precompile(const tcs_spec* spec, char* cubin_path, unsigned path_cap) {
   if (s.dimension == 2) s.cz = 1;
   std::vector<char> cubin;
   std::string path;
-  rc = instantiate(s, cubin, &path);
+  rc = instantiate(s, nullptr, cubin, &path);
+  if (rc) return rc;
+  if (cubin_path && path_cap) {
+    std::strncpy(cubin_path, path.c_str(), path_cap - 1);
+    cubin_path[path_cap - 1] = '\0';
+  }
+  return TCS_OK;
+}
+
+int tcs_precompile_pipe(const tcs_spec* spec, unsigned bx, unsigned by, unsigned chunk,
+                        char* cubin_path, unsigned path_cap) {
+  int rc = validate(spec);
+  if (rc) return rc;
+  tcs_spec s = *spec;
+  if (s.dimension == 2) s.cz = 1;
+  if (s.dimension == 2 && s.orientation == TCS_COLUMN)
+    return fail(TCS_ERR_UNSUPPORTED, "2D Column orientation is not pipelined");
+  const unsigned vec = 16u / (unsigned)elem_size(s);
+  if (bx == 0 || (bx * (unsigned)s.cx) % vec != 0)
+    return fail(TCS_ERR_UNSUPPORTED, "pipe: unsupported block");
+  if (chunk == 0) chunk = pipe_auto_chunk(s, bx * (unsigned)s.cx);
+  if ((chunk & (chunk - 1)) != 0) return fail(TCS_ERR_UNSUPPORTED, "pipe: chunk not a power of two");
+  PipeKey key{bx, s.dimension == 3 ? by : 1u, chunk, left_offset_of(s) % vec, pipe_auto_unroll(s)};
+  std::vector<char> cubin;
+  std::string path;
+  rc = instantiate(s, &key, cubin, &path);
   if (rc) return rc;
   if (cubin_path && path_cap) {
     std::strncpy(cubin_path, path.c_str(), path_cap - 1);

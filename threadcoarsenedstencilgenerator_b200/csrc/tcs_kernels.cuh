@@ -153,6 +153,7 @@ __device__ __forceinline__ void cp_async_wait_all() {
 
 }  // namespace tcs
 
+#ifndef TCS_PIPE
 // ---- tcs_direct: the reference's launch geometry, operands through L1 -------------------------
 // Thread origin and tile guard as in cuda/generate2DStencil_cuda.py:78-104 and
 // cuda/generate3DStencil_cuda.py:81-114 (x0 already includes the Write left offset).
@@ -374,3 +375,289 @@ extern "C" __global__ void tcs_init(T* __restrict__ a, const tcs_u64 xdim, const
     }
   }
 }
+#endif  // !TCS_PIPE
+
+#ifdef TCS_PIPE
+// ---- tcs_pipe: pipelined streaming sweep -------------------------------------------------------
+// Persistent CTAs.  The work is the list of (tile, output plane) pairs, tiles being BX*CX columns
+// (2D) or BX*CX x BY*CY columns (3D) and planes running along the slowest axis; each CTA takes an
+// equal contiguous share and sweeps it as one or two pieces (tile, [ms, me)).  A piece streams the
+// input planes ms-R .. me+R-1 through a shared-memory ring (chunks of TCS_CH planes copied by TMA,
+// or by cp.async when the row pitch breaks the TMA rules), and every thread keeps the 2R+1 output
+// planes that the current input plane touches in registers: plane p adds its terms to the outputs
+// p-R .. p+R (march-axis offset outermost in the reference's per-output order, so each output
+// still accumulates in exactly the reference order) and completes output p-R.  Each input element
+// is read from HBM once and from shared memory once per thread that needs it; with the plane loop
+// unrolled by 2R+1 every register slot and every shared-memory offset is a compile-time constant.
+namespace tcs {
+constexpr int BX = TCS_BX;
+constexpr int BY = (DIM == 3) ? TCS_BY : 1;
+constexpr int CHP = TCS_CH;          // planes per chunk
+constexpr int LSHIFT = TCS_LSHIFT;   // (left offset) mod VEC: x position of the tile in its granule
+constexpr int TXP = BX * CX;
+constexpr int TYP = (DIM == 3) ? BY * CY : 1;
+constexpr int ROWS = (DIM == 3) ? TYP + 2 * R : 1;
+constexpr int pipe_width() {
+  int w = ((TXP + 2 * R + LSHIFT + VEC - 1) / VEC) * VEC;
+  while ((CHP * ROWS * w * (int)sizeof(T)) % 128 != 0) w += VEC;
+  return w;
+}
+constexpr int PW = pipe_width();     // shared-memory row width (elements)
+constexpr int PLANE = PW * ROWS;     // elements per plane
+constexpr int CHUNK = CHP * PLANE;   // elements per ring slot
+constexpr int NP2 = 2 * R + 1;       // pipeline depth (output planes in flight)
+constexpr int UNR = TCS_UNROLL;      // input planes per unrolled loop body (<= NP2)
+static_assert(!(DIM == 2 && ORIENT == 1), "2D Column orientation is not pipelined");
+static_assert(UNR >= 1 && UNR <= NP2, "unroll depth must be in [1, 2R+1]");
+static_assert((CHP & (CHP - 1)) == 0, "planes per chunk must be a power of two");
+static_assert(TXP % VEC == 0, "tile width must be a multiple of the 16-byte granule");
+// Columns whose element index is even for every thread: the thread origin sits at ring column
+// LSHIFT + R + tx*CX and every row, plane and chunk starts on a 16-byte boundary, so with CX even
+// the pair (gx, gx+1) is 16-byte (8-byte for float) aligned exactly when LSHIFT + R + gx is even.
+__host__ __device__ constexpr bool pipe_pair_aligned(int gx) { return (CX % 2 == 0) && (((LSHIFT + R + gx) % 2 + 2) % 2 == 0); }
+
+template <class V>
+struct PairOf;
+template <>
+struct PairOf<double> {
+  typedef double2 type;
+};
+template <>
+struct PairOf<float> {
+  typedef float2 type;
+};
+
+// Shared-memory plane reader of one thread (origin `p`, row pitch PW).
+struct PipeRing {
+  const T* p;
+  __host__ __device__ static constexpr bool pair_aligned(int gx) { return pipe_pair_aligned(gx); }
+  template <int GX, int GY>
+  __device__ __forceinline__ T one() const {
+    return p[GY * PW + GX];
+  }
+  template <int GX, int GY>
+  __device__ __forceinline__ void two(T& a, T& b) const {
+    const typename PairOf<T>::type v = *reinterpret_cast<const typename PairOf<T>::type*>(p + GY * PW + GX);
+    a = v.x;
+    b = v.y;
+  }
+};
+}  // namespace tcs
+
+struct TcsPipeGeo {
+  tcs_u64 xdim, ydim, zdim;    // padded row pitch, rows, planes (1 in 2D)
+  tcs_u64 total;               // work items: tiles * m
+  tcs_u64 per_cta;             // work items per CTA
+  tcs_u32 x0, x_lim;           // interior x range
+  tcs_u32 y_lim, z_lim;        // interior upper bounds in y and z
+  tcs_u32 ntx;                 // tiles along x
+  tcs_u32 m;                   // output planes along the march axis
+  tcs_u32 nslot;               // ring slots
+  tcs_u32 loader;              // 0 = TMA, 1 = cp.async
+};
+
+extern "C" __global__ void __launch_bounds__(TCS_BX * ((TCS_DIM == 3) ? TCS_BY : 1))
+    tcs_pipe(const __grid_constant__ TcsTmaMap tmap, const T* __restrict__ in,
+             T* __restrict__ out, const TcsPipeGeo g) {
+  using namespace tcs;
+  extern __shared__ __align__(128) unsigned char tcs_smem[];
+  const tcs_u32 nslot = g.nslot;
+  const bool use_tma = (g.loader == 0);
+  constexpr tcs_u32 NTHREADS = BX * BY;
+  const tcs_u32 tid = threadIdx.x + BX * threadIdx.y;
+  const tcs_u32 bars = smem_addr(tcs_smem);
+  const tcs_u32 bar_bytes = ((nslot * 8u + 127u) / 128u) * 128u;
+  const tcs_u32 ring_s = (bars + bar_bytes + 127u) & ~127u;
+  T* ring = reinterpret_cast<T*>(tcs_smem + (ring_s - bars));
+  constexpr tcs_u32 CHUNK_BYTES = CHUNK * (tcs_u32)sizeof(T);
+
+  if (tid == 0) {
+    for (tcs_u32 i = 0; i < nslot; ++i) mbar_init(bars + 8u * i, use_tma ? 1u : NTHREADS);
+    fence_barrier_init();
+    if (use_tma) tma_prefetch_map(&tmap);
+  }
+  __syncthreads();
+
+  T acc[NP2][NEP];
+  tcs_u32 gc = 0;  // ring chunks consumed by this CTA so far (slot = gc % nslot)
+  // Output pairs are stored with one access only when every row keeps the parity of the first:
+  // an even row pitch and a pair-aligned base address.
+  const bool st_pair = (g.xdim % 2 == 0) &&
+                       (reinterpret_cast<tcs_u64>(out) % (2 * sizeof(T)) == 0);
+  const tcs_u64 w_begin = (tcs_u64)blockIdx.x * g.per_cta;
+  const tcs_u64 w_end = min(w_begin + g.per_cta, g.total);
+  tcs_u64 w = w_begin;
+  while (w < w_end) {
+    const tcs_u32 tile = (tcs_u32)(w / g.m);
+    const tcs_u32 zs = (tcs_u32)(w % g.m);
+    const tcs_u32 ze = (tcs_u32)min((tcs_u64)g.m, (tcs_u64)zs + (w_end - w));
+    w += ze - zs;
+    const tcs_u32 ms = R + zs;                 // first output plane of the piece
+    const tcs_u32 nout = ze - zs;              // output planes of the piece
+    const tcs_u32 np = nout + 2 * R;           // input planes streamed
+    const tcs_u32 nch = (np + CHP - 1) / CHP;  // chunks of the piece
+    const tcs_u32 X0 = g.x0 + (tile % g.ntx) * TXP;
+    const tcs_u32 xl = X0 - R - LSHIFT;        // TMA x start, a multiple of VEC
+    const tcs_u32 Y0 = (DIM == 3) ? R + (tile / g.ntx) * TYP : 0;
+
+    auto issue = [&](tcs_u32 j) {  // chunk j of the piece -> ring slot (gc + j) % nslot
+      const tcs_u32 slot = (gc + j) % nslot;
+      const tcs_u32 bar = bars + 8u * slot;
+      const tcs_u32 m0 = ms - R + j * CHP;   // first input plane of the chunk
+      if (use_tma) {
+        mbar_expect_tx(bar, CHUNK_BYTES);
+#if TCS_DIM == 2
+        tma_load_2d(ring_s + slot * CHUNK_BYTES, &tmap, bar, (int)xl, (int)m0);
+#else
+        tma_load_3d(ring_s + slot * CHUNK_BYTES, &tmap, bar, (int)xl, (int)(Y0 - R), (int)m0);
+#endif
+      } else {
+        const tcs_u32 dst0 = ring_s + slot * CHUNK_BYTES;
+        for (tcs_u32 q = tid; q < (tcs_u32)CHUNK; q += NTHREADS) {
+          const tcs_u32 xx = xl + q % PW;
+#if TCS_DIM == 2
+          const tcs_u64 yy = m0 + q / PW;
+          const bool inside = xx < g.xdim && yy < g.ydim;
+          const tcs_u64 gi = inside ? (tcs_u64)xx + yy * g.xdim : 0;
+#else
+          const tcs_u64 yy = (Y0 - R) + (q / PW) % ROWS;
+          const tcs_u64 zz = m0 + q / PLANE;
+          const bool inside = xx < g.xdim && yy < g.ydim && zz < g.zdim;
+          const tcs_u64 gi = inside ? (tcs_u64)xx + yy * g.xdim + zz * g.xdim * g.ydim : 0;
+#endif
+          cp_async_elem(dst0 + q * (tcs_u32)sizeof(T), in + gi, inside ? (tcs_u32)sizeof(T) : 0u);
+        }
+        cp_async_arrive(bar);
+      }
+    };
+    {
+      const tcs_u32 pro = min(nslot - 1, nch);
+      if (use_tma) {
+        if (tid == 0)
+          for (tcs_u32 j = 0; j < pro; ++j) issue(j);
+      } else {
+        for (tcs_u32 j = 0; j < pro; ++j) issue(j);
+      }
+    }
+
+    const tcs_u32 x = X0 + threadIdx.x * CX;
+    const tcs_u32 col0 = LSHIFT + R + threadIdx.x * CX;  // ring column of the thread's gx = 0
+#if TCS_DIM == 3
+    const tcs_u32 y = Y0 + threadIdx.y * CY;
+    const tcs_u32 lane_off = (R + threadIdx.y * CY) * PW + col0;
+    const bool lane_ok = (x + (CX - 1) < g.x_lim) && (y + (CY - 1) < g.y_lim);
+    const tcs_i64 plane_g = (tcs_i64)(g.xdim * g.ydim);
+    T* obase = out + (tcs_u64)x + (tcs_u64)y * g.xdim;
+#else
+    const tcs_u32 lane_off = col0;
+    const bool lane_ok = (x + (CX - 1) < g.x_lim);
+    const tcs_i64 plane_g = (tcs_i64)g.xdim;
+    T* obase = out + (tcs_u64)x;
+#endif
+    // Cursors advanced by additions only: ring slot and phase of the current chunk, the plane
+    // within it, and the output plane completed after the current input plane (pi - 2R).
+    tcs_u32 cur_slot = gc % nslot;
+    tcs_u32 cur_par = (gc / nslot) & 1u;
+    tcs_u32 in_chunk = 0;
+    tcs_u32 j = 0;  // chunk of the piece being consumed
+    const T* pt = ring + cur_slot * CHUNK + lane_off;
+    T* optr = obase + ((tcs_i64)ms - 2 * R) * plane_g;
+    bool aborted = false;
+    for (tcs_u32 s = 0; s * UNR < np && !aborted; ++s) {
+      static_for<0, UNR>([&](auto tt) {
+        constexpr int t = decltype(tt)::value;
+        const tcs_u32 pi = s * UNR + t;  // input plane index within the piece
+        if (pi < np && !aborted) {
+          if (in_chunk == 0) {
+            const bool expired = mbar_wait_bounded(bars + 8u * cur_slot, cur_par, TCS_WAIT_LIMIT);
+            if (__syncthreads_or(expired)) {
+              aborted = true;
+              if (use_tma) {
+                if (tid == 0) {
+                  atomicOr(&tcs_status, TCS_DEV_TIMEOUT);
+                  const tcs_u32 hi = min(j + nslot - 2, nch - 1);
+                  for (tcs_u32 jj = j; jj <= hi; ++jj)
+                    (void)mbar_wait_bounded(bars + 8u * ((gc + jj) % nslot), ((gc + jj) / nslot) & 1u,
+                                            TCS_WAIT_LIMIT);
+                }
+              } else {
+                if (tid == 0) atomicOr(&tcs_status, TCS_DEV_TIMEOUT);
+                cp_async_wait_all();
+              }
+            } else if (j + nslot - 1 < nch) {
+              if (!use_tma)
+                issue(j + nslot - 1);
+              else if (tid == 0)
+                issue(j + nslot - 1);
+            }
+          }
+          if (!aborted) {
+            const PipeRing ld{pt};
+            auto slot = [&](auto kk) -> T(&)[NEP] {
+              constexpr int k = decltype(kk)::value;
+              return acc[((t - k) % NP2 + NP2) % NP2];
+            };
+            pipe_plane(ld, slot);
+            // output pi - 2R received its last term (march-axis offset +R)
+            const int op = (int)pi - 2 * R;
+            if (lane_ok && op >= 0 && op < (int)nout) {
+              constexpr T c = T(1) / T(S);
+              T(&done)[NEP] = acc[((t - 2 * R) % NP2 + NP2) % NP2];
+              // Output x is R + leftOff + an even offset when CX is even: pairs are aligned when
+              // R + LSHIFT is even (the shared-memory pair rule at gx = 0).
+              static_for<0, (DIM == 3) ? CY : 1>([&](auto ey) {
+                static_for<0, CX>([&](auto ex) {
+                  constexpr int e = decltype(ex)::value + decltype(ey)::value * CX;
+                  constexpr bool pair = pipe_pair_aligned(0) && (decltype(ex)::value % 2 == 0);
+                  constexpr bool tail = pipe_pair_aligned(0) && (decltype(ex)::value % 2 == 1);
+                  T* o = optr + decltype(ex)::value + decltype(ey)::value * (tcs_i64)g.xdim;
+                  if constexpr (pair) {
+                    const T v0 = (COEFF == 0) ? done[e] * c : done[e];
+                    const T v1 = (COEFF == 0) ? done[e + 1] * c : done[e + 1];
+                    if (st_pair) {
+                      typename PairOf<T>::type v2;
+                      v2.x = v0;
+                      v2.y = v1;
+                      *reinterpret_cast<typename PairOf<T>::type*>(o) = v2;
+                    } else {
+                      o[0] = v0;
+                      o[1] = v1;
+                    }
+                  } else if constexpr (!tail) {
+                    *o = (COEFF == 0) ? done[e] * c : done[e];
+                  }
+                });
+              });
+            }
+            optr += plane_g;
+            pt += PLANE;
+            if (++in_chunk == (tcs_u32)CHP) {
+              in_chunk = 0;
+              ++j;
+              if (++cur_slot == nslot) {
+                cur_slot = 0;
+                cur_par ^= 1u;
+              }
+              pt = ring + cur_slot * CHUNK + lane_off;
+            }
+          }
+        }
+      });
+      // Re-align the register slots with the next body: slot m takes what slot (m + UNR) held.
+      if constexpr (UNR % NP2 != 0) {
+        T tmp[NP2][NEP];
+        static_for<0, NP2>([&](auto m) {
+          static_for<0, NEP>([&](auto e) { tmp[decltype(m)::value][decltype(e)::value] = acc[decltype(m)::value][decltype(e)::value]; });
+        });
+        static_for<0, NP2>([&](auto m) {
+          static_for<0, NEP>([&](auto e) {
+            acc[decltype(m)::value][decltype(e)::value] = tmp[(decltype(m)::value + UNR) % NP2][decltype(e)::value];
+          });
+        });
+      }
+    }
+    if (aborted) return;
+    gc += nch;
+  }
+}
+#endif  // TCS_PIPE

@@ -254,3 +254,164 @@ __device__ __forceinline__ void store(T* __restrict__ o, const T (&acc)[NE], tcs
 }
 
 }  // namespace tcs
+
+// ---- pipeline arithmetic (tcs_pipe) -------------------------------------------------------------
+// In the pipelined sweep a thread owns CX x CY (3D) or CX (2D) outputs per plane along the march
+// axis and keeps 2R+1 output planes in flight.  The term an input point contributes to the
+// output in pipeline slot DZ (the march-axis offset from that output) is (rx, ry, rz) =
+// (GX - ex, GY - ey, DZ) in 3D and (GX - ex, DZ, 0) in 2D (the march axis is y there).
+namespace tcs {
+constexpr int NEP = (DIM == 3) ? CX * CY : CX;  // outputs per thread and plane
+
+template <int GX, int GY, int DZ>
+__device__ __forceinline__ void apply_slot(T (&acc)[NEP], const T v) {
+  static_for<0, (DIM == 3) ? CY : 1>([&](auto ey) {
+    static_for<0, CX>([&](auto ex) {
+      constexpr int rx = GX - decltype(ex)::value;
+      constexpr int ry = (DIM == 3) ? GY - decltype(ey)::value : DZ;
+      constexpr int rz = (DIM == 3) ? DZ : 0;
+      constexpr int e = decltype(ex)::value + decltype(ey)::value * CX;
+      if constexpr (contributes(rx, ry, rz)) {
+        if constexpr (is_first(rx, ry, rz)) {
+          acc[e] = v;
+        } else if constexpr (COEFF == 0) {
+          acc[e] = acc[e] + v;
+        } else if constexpr (is_second(rx, ry, rz)) {
+          acc[e] = fmat(acc[e], tcs_mask[first_mask_index()], v * tcs_mask[mask_index(rx, ry, rz)]);
+        } else {
+          acc[e] = fmat(v, tcs_mask[mask_index(rx, ry, rz)], acc[e]);
+        }
+      }
+    });
+  });
+}
+
+// Load the row segment gx in [GX0, GX0 + N) of in-plane row GY into registers.  The loader says
+// which columns start a pair it can fetch with one 16-byte (8-byte for float) access
+// (`pair_aligned(gx)`, a compile-time property of the column parity) and provides `one<gx, gy>()`
+// and `two<gx, gy>(a, b)`.
+template <int GY, int GX0, int N, class LD>
+__device__ __forceinline__ void load_row(const LD& ld, T (&v)[N]) {
+  static_for<0, N>([&](auto ii) {
+    constexpr int i = decltype(ii)::value;
+    constexpr int gx = GX0 + i;
+    constexpr bool starts_pair = LD::pair_aligned(gx) && (i + 1 < N);
+    constexpr bool second_of_pair = (i > 0) && LD::pair_aligned(gx - 1);
+    if constexpr (starts_pair) {
+      ld.template two<gx, GY>(v[i], v[i + 1]);
+    } else if constexpr (!second_of_pair) {
+      v[i] = ld.template one<gx, GY>();
+    }
+  });
+}
+
+// Apply input plane (offset DZ relative to pending outputs) held in shared memory to the 2R+1
+// pipeline slots.  `ld` reads the plane at in-plane offsets from the thread origin (see load_row);
+// `slot(ic<k>)` returns the accumulators of the output at march-axis offset k - R.
+template <class LD, class SLOTS>
+__device__ __forceinline__ void pipe_plane(const LD& ld, SLOTS&& slot) {
+  if constexpr (SHAPE == 0) {
+    // Box: every in-plane footprint point feeds every slot, in the slice traversal order.
+    constexpr int NY = (DIM == 3) ? 2 * R + CY : 1;
+    constexpr int OY = (DIM == 3) ? R : 0;
+    if constexpr (ORIENT == 1 && DIM == 3) {
+      static_for<0, 2 * R + CX>([&](auto ix) {
+        static_for<0, NY>([&](auto iy) {
+          constexpr int gx = decltype(ix)::value - R, gy = decltype(iy)::value - OY;
+          const T v = ld.template one<gx, gy>();
+          static_for<0, 2 * R + 1>([&](auto k) { apply_slot<gx, gy, decltype(k)::value - R>(slot(k), v); });
+        });
+      });
+    } else {
+      static_for<0, NY>([&](auto iy) {
+        constexpr int gy = decltype(iy)::value - OY;
+        T row[2 * R + CX];
+        load_row<gy, -R, 2 * R + CX>(ld, row);
+        static_for<0, 2 * R + CX>([&](auto ix) {
+          constexpr int gx = decltype(ix)::value - R;
+          static_for<0, 2 * R + 1>([&](auto k) {
+            apply_slot<gx, gy, decltype(k)::value - R>(slot(k), row[decltype(ix)::value]);
+          });
+        });
+      });
+    }
+  } else {
+    // Star: the thread's own centre points feed the slots DZ != 0; the in-plane cross feeds DZ = 0.
+    constexpr int NY = (DIM == 3) ? CY : 1;
+    auto& s0 = slot(ic<R>{});
+    T cv[NEP];
+    if constexpr (ORIENT == 0 || DIM == 2) {
+      // Row order: the middle rows are contiguous segments that also hold the centre points.
+      if constexpr (DIM == 3) {
+        static_for<0, R>([&](auto i) {  // gy in [-R, 0): the thread's columns
+          constexpr int gy = decltype(i)::value - R;
+          T seg[CX];
+          load_row<gy, 0, CX>(ld, seg);
+          static_for<0, CX>([&](auto gx) { apply_slot<decltype(gx)::value, gy, 0>(s0, seg[decltype(gx)::value]); });
+        });
+      }
+      static_for<0, NY>([&](auto gyc) {  // middle rows: gx in [-R, R + CX)
+        constexpr int gy = decltype(gyc)::value;
+        T row[2 * R + CX];
+        load_row<gy, -R, 2 * R + CX>(ld, row);
+        static_for<0, CX>([&](auto ex) { cv[decltype(ex)::value + gy * CX] = row[R + decltype(ex)::value]; });
+        static_for<0, 2 * R + CX>([&](auto ix) {
+          apply_slot<decltype(ix)::value - R, gy, 0>(s0, row[decltype(ix)::value]);
+        });
+      });
+      if constexpr (DIM == 3) {
+        static_for<0, R>([&](auto i) {  // gy in [CY, CY + R)
+          constexpr int gy = CY + decltype(i)::value;
+          T seg[CX];
+          load_row<gy, 0, CX>(ld, seg);
+          static_for<0, CX>([&](auto gx) { apply_slot<decltype(gx)::value, gy, 0>(s0, seg[decltype(gx)::value]); });
+        });
+      }
+    } else {
+      // 3D Column order: columns of the cross, point by point.
+      static_for<0, NY>([&](auto ey) {
+        static_for<0, CX>([&](auto ex) {
+          cv[decltype(ex)::value + decltype(ey)::value * CX] = ld.template one<decltype(ex)::value, decltype(ey)::value>();
+        });
+      });
+      auto ldc = [&](auto gxc, auto gyc) -> T {
+        constexpr int gx = decltype(gxc)::value, gy = decltype(gyc)::value;
+        if constexpr (gx >= 0 && gx < CX && gy >= 0 && gy < NY)
+          return cv[gx + gy * CX];
+        else
+          return ld.template one<gx, gy>();
+      };
+      static_for<0, R>([&](auto i) {
+        static_for<0, CY>([&](auto gy) {
+          constexpr int gx = decltype(i)::value - R, y = decltype(gy)::value;
+          apply_slot<gx, y, 0>(s0, ldc(ic<gx>{}, ic<y>{}));
+        });
+      });
+      static_for<0, CX>([&](auto gx) {
+        static_for<0, 2 * R + CY>([&](auto i) {
+          constexpr int x = decltype(gx)::value, gy = decltype(i)::value - R;
+          apply_slot<x, gy, 0>(s0, ldc(ic<x>{}, ic<gy>{}));
+        });
+      });
+      static_for<0, R>([&](auto i) {
+        static_for<0, CY>([&](auto gy) {
+          constexpr int gx = CX + decltype(i)::value, y = decltype(gy)::value;
+          apply_slot<gx, y, 0>(s0, ldc(ic<gx>{}, ic<y>{}));
+        });
+      });
+    }
+    // centre points -> slots DZ != 0 (one term each)
+    static_for<0, 2 * R + 1>([&](auto k) {
+      constexpr int dz = decltype(k)::value - R;
+      if constexpr (dz != 0) {
+        static_for<0, NY>([&](auto ey) {
+          static_for<0, CX>([&](auto ex) {
+            apply_slot<decltype(ex)::value, decltype(ey)::value, dz>(
+                slot(k), cv[decltype(ex)::value + decltype(ey)::value * CX]);
+          });
+        });
+      }
+    });
+  }
+}
+}  // namespace tcs

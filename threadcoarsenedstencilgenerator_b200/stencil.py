@@ -37,18 +37,20 @@ class Launch:
     """Launch parameters of a sweep (see tcs_launch in include/tcs.h)."""
 
     block: tuple = (128, 1, 1)
-    variant: str = "auto"          # auto | direct | march
+    variant: str = "auto"          # auto | direct | march | pipe
     grid_blocks: tuple = (0, 0, 0)  # direct only; zeros: cover the interior
     segments: int = 0               # march: CTAs along the march axis per tile column (0 = auto)
-    depth: int = 0                  # march: chunks in flight (0 = auto)
+    depth: int = 0                  # march/pipe: chunks in flight (0 = auto)
+    chunk: int = 0                  # pipe: planes per ring chunk (0 = auto)
 
-    _VARIANTS = {"auto": _lib.VARIANT_AUTO, "direct": _lib.VARIANT_DIRECT, "march": _lib.VARIANT_MARCH}
+    _VARIANTS = {"auto": _lib.VARIANT_AUTO, "direct": _lib.VARIANT_DIRECT, "march": _lib.VARIANT_MARCH,
+                 "pipe": _lib.VARIANT_PIPE}
 
     def to_c(self) -> _lib.CLaunch:
         b = tuple(self.block) + (1,) * (3 - len(self.block))
         g = tuple(self.grid_blocks) + (0,) * (3 - len(self.grid_blocks))
         return _lib.CLaunch(_lib.U3(*b), _lib.U3(*g), self._VARIANTS[self.variant], int(self.segments),
-                            int(self.depth))
+                            int(self.depth), int(self.chunk))
 
 
 @dataclass
@@ -60,6 +62,7 @@ class Plan:
     seg_len: int
     nslot: int
     width: int
+    chunk: int
     depth: int
     loader: str
     ctas_per_sm: int
@@ -108,7 +111,7 @@ class Stencil:
                                              ctypes.byref(launch.to_c()), ctypes.byref(p)))
         names = {v: k for k, v in Launch._VARIANTS.items()}
         return Plan(names[p.variant], tuple(p.grid_blocks), tuple(p.block), p.dyn_smem, p.seg_len, p.nslot,
-                    p.width, p.depth, "tma" if p.loader == 0 else "cp.async", p.ctas_per_sm, p.num_sms)
+                    p.width, p.chunk, p.depth, "tma" if p.loader == 0 else "cp.async", p.ctas_per_sm, p.num_sms)
 
     def update_grid(self, geom: Geometry, src, dst, launch: Launch | None = None, stream=None) -> None:
         """One sweep dst = stencil(src) over the interior (asynchronous)."""
@@ -169,6 +172,14 @@ def precompile(spec: StencilSpec) -> str:
     """Instantiate the kernels of ``spec`` into the cubin cache (NVRTC only, no GPU needed)."""
     buf = ctypes.create_string_buffer(1024)
     _lib.check(_lib.load().tcs_precompile(ctypes.byref(spec.to_c()), buf, 1024))
+    return buf.value.decode()
+
+
+def precompile_pipe(spec: StencilSpec, block, chunk: int) -> str:
+    """Instantiate the pipelined sweep of ``spec`` for one launch shape into the cubin cache."""
+    buf = ctypes.create_string_buffer(1024)
+    b = tuple(block) + (1,) * (3 - len(block))
+    _lib.check(_lib.load().tcs_precompile_pipe(ctypes.byref(spec.to_c()), b[0], b[1], int(chunk), buf, 1024))
     return buf.value.decode()
 
 

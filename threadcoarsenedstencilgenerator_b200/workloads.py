@@ -59,7 +59,8 @@ class Workload:
             t = json.loads(TUNED_PATH.read_text()).get(self.name)
             if t:
                 return Launch(block=tuple(t["block"]), variant=t.get("variant", "auto"),
-                              segments=int(t.get("segments", 0)), depth=int(t.get("depth", 0)))
+                              segments=int(t.get("segments", 0)), depth=int(t.get("depth", 0)),
+                              chunk=int(t.get("chunk", 0)))
         return self.launch
 
     def tuned_spec(self) -> StencilSpec:
@@ -78,21 +79,21 @@ WORKLOADS = {
         name="2d_box_jacobi_r1_4096",
         spec=StencilSpec(dimension=2, neighbourhood="Box", orientation="Row", coefficients="Jacobi", range=1),
         grid=(4096, 4096, 1), sweeps=100, launch=Launch(block=(64, 4, 1), variant="march"),
-        reference=((1, 1, 1), (128, 1, 1))),
+        reference=((2, 2, 1), (128, 1, 1))),
     # 3D Star Variable r4 (25-point), FP64, 512^3, Read alignment to 16 points, 50 sweeps
     "3d_star_var_r4_512": Workload(
         name="3d_star_var_r4_512",
         spec=StencilSpec(dimension=3, neighbourhood="Star", orientation="Row", coefficients="Variable", range=4,
                          cx=1, cy=2, cz=2, alignment="Read", cl_size=16),
         grid=(512, 512, 512), sweeps=50, mask_kind="normal_sum1", launch=Launch(block=(32, 8, 1), variant="march"),
-        reference=((1, 1, 1), (32, 4, 1))),
+        reference=((1, 4, 2), (128, 2, 1))),
     # 2D Box Variable r6 (169-point), FP64, 16384x8192, mask N(0,1)/169, values U[-1,1], 200 sweeps
     "2d_box_var_r6_16384x8192": Workload(
         name="2d_box_var_r6_16384x8192",
         spec=StencilSpec(dimension=2, neighbourhood="Box", orientation="Row", coefficients="Variable", range=6,
                          cx=2, cy=4),
         grid=(16384, 8192, 1), sweeps=200, value_range=(-1.0, 1.0), mask_kind="normal_over_S",
-        launch=Launch(block=(32, 4, 1), variant="march"), reference=((2, 2, 1), (64, 2, 1))),
+        launch=Launch(block=(32, 4, 1), variant="march"), reference=((2, 4, 1), (32, 4, 1))),
 }
 
 DEFAULT_WORKLOAD = "3d_star_var_r4_512"
