@@ -92,6 +92,42 @@ def compile_one(cfg, shipped: bool = False) -> Path:
     return lib
 
 
+SHAPES = {"Box": 0, "Star": 1}
+ORIENTS = {"Row": 0, "Column": 1}
+COEFFS = {"Jacobi": 0, "Variable": 1}
+ALIGNS = {"None": 0, "Read": 1, "Write": 2}
+
+
+def build_shim_bench(cfg) -> Path:
+    """Link the reference's unmodified host program (cuda/main.cpp, cuda/benchmark.cpp,
+    cuda/primes.cpp) against the engine through launch_update_grid_shim.cpp: the reference's
+    `bench` binary for one parameter set, running on libtcs.so.  Output: oracle/_ref/<key>/bench_tcs."""
+    d, sh, o, c, r, cx, cy, cz, al, cl = cfg
+    dest = OUT / key(cfg)
+    dest.mkdir(parents=True, exist_ok=True)
+    pkg = HERE.parent / "threadcoarsenedstencilgenerator_b200"
+    exe = dest / "bench_tcs"
+    defs = ["-DTCS_SHIM_DIM=%d" % d, "-DTCS_SHIM_SHAPE=%d" % SHAPES[sh], "-DTCS_SHIM_ORIENT=%d" % ORIENTS[o],
+            "-DTCS_SHIM_COEFF=%d" % COEFFS[c], "-DTCS_SHIM_R=%d" % r, "-DTCS_SHIM_CX=%d" % cx,
+            "-DTCS_SHIM_CY=%d" % cy, "-DTCS_SHIM_CZ=%d" % (cz if d == 3 else 1), "-DTCS_SHIM_ALIGN=%d" % ALIGNS[al],
+            "-DTCS_SHIM_CL=%d" % cl]
+    rel = "$ORIGIN/../../../threadcoarsenedstencilgenerator_b200"
+    cmd = [NVCC, "-O2", *defs, "-I", str(HERE.parent / "include"), "-I", str(REF_CUDA),
+           str(REF_CUDA / "main.cpp"), str(REF_CUDA / "benchmark.cpp"), str(REF_CUDA / "primes.cpp"),
+           str(pkg / "csrc" / "launch_update_grid_shim.cpp"), "-L", str(pkg), "-ltcs",
+           "-Xlinker", "-rpath=" + rel, "-o", str(exe)]
+    proc = subprocess.run(cmd, capture_output=True, text=True)
+    if proc.returncode != 0:
+        raise RuntimeError("shim bench link failed for %s:\n%s" % (key(cfg), proc.stderr[-4000:]))
+    return exe
+
+
+SHIM_CONFIGS = [
+    (2, "Box", "Row", "Jacobi", 1, 1, 1, 1, "None", 0),
+    (3, "Star", "Row", "Variable", 4, 2, 2, 1, "Read", 16),
+]
+
+
 def build_ref(configs=None, shipped: bool = False, jobs: int = 8) -> list:
     if not reference_available():
         return []
@@ -112,4 +148,5 @@ if __name__ == "__main__":
     libs = build_ref(shipped=False, jobs=a.j)
     if a.shipped:
         libs += build_ref(shipped=True, jobs=a.j)
+    libs += [build_shim_bench(c) for c in SHIM_CONFIGS]
     print("built %d reference libraries under %s" % (len(libs), OUT))

@@ -88,7 +88,6 @@ def simulate(dim, shape, R, c, block, grid, left_offset, right_offset, aligned, 
         ch = 1
         while ch * 2 <= want:
             ch *= 2
-    assert ch & (ch - 1) == 0
     W = pipe_width(TX, R, lshift, vec, ch, rows, es)
     if W > 256 or rows > 256:
         return None
@@ -159,72 +158,66 @@ def simulate(dim, shape, R, c, block, grid, left_offset, right_offset, aligned, 
 
             for j in range(min(nslot - 1, nch)):
                 issue(j)
-            # the kernel's incremental cursors
-            cur_slot, cur_par, in_chunk, jc = gc % nslot, (gc // nslot) & 1, 0, 0
-            pt = cur_slot * CHUNK
-            for pi in range(np_):
-                if in_chunk == 0:
-                    j = pi // ch
-                    assert jc == j and cur_slot == (gc + j) % nslot and cur_par == ((gc + j) // nslot) & 1
-                    assert j in issued, "wait on a chunk never issued"
-                    assert slot_of[(gc + j) % nslot] == gc + j
-                    if j + nslot - 1 < nch:
-                        # the slot being refilled held chunk j-1, consumed before the barrier
-                        assert slot_of[(gc + j + nslot - 1) % nslot] in (None, gc + j - 1)
-                        issue(j + nslot - 1)
-                        assert slot_of[(gc + j) % nslot] == gc + j, "current chunk overwritten"
-                p = ms - R + pi
-                base = ((gc + pi // ch) % nslot) * CHUNK + (pi % ch) * plane
-                assert base == pt, "ring cursor drifted"
-                assert slot_of[(gc + pi // ch) % nslot] == gc + pi // ch
-                op = pi - 2 * R
-                for ty in range(by):
-                    for tx in range(bx):
-                        x = X0 + tx * cx
-                        col0 = lshift + R + tx * cx
-                        if dim == 3:
-                            y = Y0 + ty * cy
-                            lane_off = (R + ty * cy) * W + col0
-                            lane_ok = x + cx - 1 < x_lim and y + cy - 1 < y_lim
-                        else:
-                            y = 0
-                            lane_off = col0
-                            lane_ok = x + cx - 1 < x_lim
-                        for gx, gy in pts:
-                            idx = base + lane_off + gy * W + gx
-                            assert 0 <= idx < ring_elems, "shared-memory read out of bounds"
-                            if dim == 2:
-                                want = (x + gx) + p * xdim
+            # the kernel's chunk loop with its slot cursor
+            cur_slot, cur_par = gc % nslot, (gc // nslot) & 1
+            for j in range(nch):
+                assert cur_slot == (gc + j) % nslot and cur_par == ((gc + j) // nslot) & 1
+                assert j in issued, "wait on a chunk never issued"
+                assert slot_of[(gc + j) % nslot] == gc + j
+                if j + nslot - 1 < nch:
+                    # the slot being refilled held chunk j-1, consumed before the barrier
+                    assert slot_of[(gc + j + nslot - 1) % nslot] in (None, gc + j - 1)
+                    issue(j + nslot - 1)
+                    assert slot_of[(gc + j) % nslot] == gc + j, "current chunk overwritten"
+                for t in range(ch):
+                    pi = j * ch + t
+                    if pi >= np_:
+                        continue
+                    p = ms - R + pi
+                    base = cur_slot * CHUNK + t * plane
+                    op = pi - 2 * R
+                    for ty in range(by):
+                        for tx in range(bx):
+                            x = X0 + tx * cx
+                            col0 = lshift + R + tx * cx
+                            if dim == 3:
+                                y = Y0 + ty * cy
+                                lane_off = (R + ty * cy) * W + col0
+                                lane_ok = x + cx - 1 < x_lim and y + cy - 1 < y_lim
                             else:
-                                want = (x + gx) + (y + gy) * xdim + p * xdim * ydim
-                            if lane_ok:
-                                assert ring[idx] == want, "read %r want %r" % (ring[idx], want)
-                        for gx, gy in pairs:
-                            idx = base + lane_off + gy * W + gx
-                            assert idx % 2 == 0 and idx + 1 < ring_elems, "pair load not aligned"
-                        if lane_ok and 0 <= op < nout and pair_store and xdim % 2 == 0:
-                            # the kernel's st_pair rule (base pointers are pair-aligned in the model)
-                            for ey in range(cy):
-                                for ex_ in range(0, cx, 2):
-                                    o0 = x + ex_ + ((y + ey) * xdim if dim == 3 else 0) + \
-                                        (ms + op) * (xdim * ydim if dim == 3 else xdim)
-                                    assert o0 % 2 == 0, "pair store not aligned"
-                        if lane_ok and 0 <= op < nout:
-                            for ey in range(cy):
-                                for ex_ in range(cx):
-                                    if dim == 2:
-                                        o = (x + ex_) + (ms + op) * xdim
-                                    else:
-                                        o = (x + ex_) + (y + ey) * xdim + (ms + op) * xdim * ydim
-                                    written[o] = written.get(o, 0) + 1
-                pt += plane
-                in_chunk += 1
-                if in_chunk == ch:
-                    in_chunk, jc = 0, jc + 1
-                    cur_slot += 1
-                    if cur_slot == nslot:
-                        cur_slot, cur_par = 0, cur_par ^ 1
-                    pt = cur_slot * CHUNK
+                                y = 0
+                                lane_off = col0
+                                lane_ok = x + cx - 1 < x_lim
+                            for gx, gy in pts:
+                                idx = base + lane_off + gy * W + gx
+                                assert 0 <= idx < ring_elems, "shared-memory read out of bounds"
+                                if dim == 2:
+                                    want = (x + gx) + p * xdim
+                                else:
+                                    want = (x + gx) + (y + gy) * xdim + p * xdim * ydim
+                                if lane_ok:
+                                    assert ring[idx] == want, "read %r want %r" % (ring[idx], want)
+                            for gx, gy in pairs:
+                                idx = base + lane_off + gy * W + gx
+                                assert idx % 2 == 0 and idx + 1 < ring_elems, "pair load not aligned"
+                            if lane_ok and 0 <= op < nout and pair_store and xdim % 2 == 0:
+                                # the kernel's st_pair rule (base pointers are pair-aligned in the model)
+                                for ey in range(cy):
+                                    for ex_ in range(0, cx, 2):
+                                        o0 = x + ex_ + ((y + ey) * xdim if dim == 3 else 0) + \
+                                            (ms + op) * (xdim * ydim if dim == 3 else xdim)
+                                        assert o0 % 2 == 0, "pair store not aligned"
+                            if lane_ok and 0 <= op < nout:
+                                for ey in range(cy):
+                                    for ex_ in range(cx):
+                                        if dim == 2:
+                                            o = (x + ex_) + (ms + op) * xdim
+                                        else:
+                                            o = (x + ex_) + (y + ey) * xdim + (ms + op) * xdim * ydim
+                                        written[o] = written.get(o, 0) + 1
+                cur_slot += 1
+                if cur_slot == nslot:
+                    cur_slot, cur_par = 0, cur_par ^ 1
             gc += nch
     count = 0
     zr = range(R, z_lim) if dim == 3 else [0]

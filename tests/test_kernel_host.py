@@ -138,7 +138,7 @@ def test_pipe_addressing_model(case, es):
     spec = O.make_spec(d, sh, "Row", "Jacobi", r, c[0], c[1], c[2], al, cl)
     g = O.geometry(spec, *n)
     for nctas in (0, 1, 3, 7):
-        for chunk, depth in ((0, 0), (1, 1), (4, 2)):
+        for chunk, depth in ((0, 0), (1, 1), (3, 2), (5, 1)):
             cnt = pipe_model.simulate(d, sh, r, c, blk, g.grid, g.left_offset, g.right_offset, al != "None",
                                       es=es, num_sms=2, occ=2, chunk=chunk, depth=depth, nctas=nctas)
             assert cnt is None or cnt > 0

@@ -154,6 +154,27 @@ def test_benchmark_update_grid_dropin(tcs):
     assert lug.maxPotentialBlockSize() >= 32
 
 
+@pytest.mark.parametrize("block", [(128, 1, 1), (32, 4, 1), (64, 2, 1)])
+def test_benchmark_update_grid_dropin_each_variant(tcs, block):
+    """The drop-in with the engine's default choice for each block shape (pipe / march)."""
+    import torch
+
+    cfg = (2, "Box", "Row", "Jacobi", 1, 1, 1, 1, "None", 0)
+    spec = G.spec_of(cfg)
+    lug = tcs.LaunchUpdateGrid(spec)
+    geom = spec.geometry(1024, 1024)
+    a = np.random.default_rng(4).random(geom.shape)
+    d0 = torch.from_numpy(a).cuda()
+    d1 = d0.clone()
+    gb = tuple(-(-geom.threads[i] // block[i]) for i in range(3))
+    durations = lug.benchmarkUpdateGrid("Jacobi", "Box", 1, 2, "None", 0.0, geom.grid, block, gb, d0, d1, 0)
+    assert len(durations) == 1
+    want = O.sweep(O.make_spec(*cfg), a)
+    assert np.array_equal(d1.cpu().numpy(), want)
+    durations = lug.benchmarkUpdateGrid("Jacobi", "Box", 1, 2, "None", 0.02, geom.grid, block, gb, d0, d1, 0)
+    assert len(durations) >= 3
+
+
 def test_full_size_2d_box_jacobi_against_oracle(tcs):
     """The 4096^2 Box Jacobi r1 workload: 4 sweeps, bit-identical with the oracle."""
     import torch

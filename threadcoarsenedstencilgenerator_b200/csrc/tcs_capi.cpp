@@ -206,9 +206,9 @@ std::string cache_dir() {
 
 // Compile-time launch shape of a pipelined-sweep module (tcs_pipe).
 struct PipeKey {
-  unsigned bx, by, ch, lshift, unroll;
+  unsigned bx, by, ch, lshift;
   bool operator==(const PipeKey& o) const {
-    return bx == o.bx && by == o.by && ch == o.ch && lshift == o.lshift && unroll == o.unroll;
+    return bx == o.bx && by == o.by && ch == o.ch && lshift == o.lshift;
   }
 };
 
@@ -216,8 +216,7 @@ std::string instance_macros(const tcs_spec& s, const PipeKey* pk) {
   std::ostringstream m;
   if (pk)
     m << "#define TCS_PIPE 1\n#define TCS_BX " << pk->bx << "\n#define TCS_BY " << pk->by
-      << "\n#define TCS_CH " << pk->ch << "\n#define TCS_LSHIFT " << pk->lshift
-      << "\n#define TCS_UNROLL " << pk->unroll << "\n";
+      << "\n#define TCS_CH " << pk->ch << "\n#define TCS_LSHIFT " << pk->lshift << "\n";
   m << "#define TCS_T " << (s.precision == TCS_F64 ? "double" : "float") << "\n"
     << "#define TCS_DIM " << s.dimension << "\n"
     << "#define TCS_SHAPE " << s.neighbourhood << "\n"
@@ -591,24 +590,33 @@ int pipe_module(tcs_stencil* h, const PipeKey& key, PipeMod** out) {
   return TCS_OK;
 }
 
-// Default planes per ring chunk (a power of two): one plane in 3D, about 4 KB of rows in 2D.
-unsigned pipe_auto_chunk(const tcs_spec& s, unsigned tx) {
+// Default planes per ring chunk, which is also the unroll depth of the pipe kernel's loop body.
+// Limits: an instruction budget of about 2000 fused multiply-adds per body (one plane applies S
+// terms to each of the thread's NEP outputs) and a chunk small enough that two ring slots fit
+// in the shared memory left to each CTA at the occupancy the registers allow.  Among the
+// feasible depths, a divisor of 2R+1 (no register permutation at the loop back-edge) is
+// preferred unless it is less than half the largest feasible depth.
+unsigned pipe_auto_chunk(const tcs_spec& s, unsigned bx, unsigned by) {
   const unsigned es = (unsigned)elem_size(s), vec = 16u / es;
-  if (s.dimension == 3) return 1u;
-  const unsigned row_bytes = (tx + 2u * (unsigned)s.range + vec) * es;
-  const unsigned want = std::max(1u, std::min(16u, cdiv(4096, row_bytes)));
-  unsigned ch = 1;
-  while (ch * 2 <= want) ch *= 2;
-  return ch;
-}
-
-// Input planes per unrolled loop body: as many as fit an instruction budget of about 2000
-// fused multiply-adds (one plane applies S terms to each of the thread's outputs), at most 2R+1.
-unsigned pipe_auto_unroll(const tcs_spec& s) {
-  const unsigned S = stencil_size_of(s);
+  const unsigned R = (unsigned)s.range;
   const unsigned nep = (unsigned)s.cx * (s.dimension == 3 ? (unsigned)s.cy : 1u);
-  const unsigned n = 2u * (unsigned)s.range + 1u;
-  return std::max(1u, std::min(n, 2000u / std::max(1u, S * nep)));
+  const unsigned n = 2u * R + 1u;
+  const unsigned S = stencil_size_of(s);
+  const unsigned tx = bx * (unsigned)s.cx;
+  const unsigned rows = s.dimension == 3 ? by * (unsigned)s.cy + 2u * R : 1u;
+  const unsigned plane_bytes = ((tx + 2u * R + 2u * vec) / vec * vec) * rows * es;
+  const unsigned threads = bx * (s.dimension == 3 ? by : 1u);
+  const unsigned regs = std::min(255u, n * nep * (es / 4u) + 48u);
+  const unsigned occ = std::max(1u, 65536u / (((regs + 7u) / 8u * 8u) * threads));
+  const unsigned max_chunk = std::min(227u * 1024u, 228u * 1024u / std::min(occ, 8u)) / 2u;
+  const unsigned budget = std::max(1u, 2000u / std::max(1u, S * nep));
+  unsigned best = 1;
+  for (unsigned c = 1; c <= std::min(budget, 4u * n); ++c)
+    if (c * plane_bytes <= max_chunk) best = c;
+  unsigned div = 1;
+  for (unsigned c = 1; c <= best; ++c)
+    if (n % c == 0 || c % n == 0) div = c;
+  return (2 * div >= best) ? div : best;
 }
 
 // Compile-time row width of a pipe instantiation (tcs::pipe_width in tcs_kernels.cuh).
@@ -635,13 +643,12 @@ int resolve_pipe(tcs_stencil* h, const TcsGeo& g, const tcs_launch* L, Resolved&
   const unsigned TY = s.dimension == 3 ? L->block[1] * s.cy : 1;
   const unsigned rows = s.dimension == 3 ? TY + 2 * R : 1;
   const unsigned lshift = h->left_off % vec;
-  const unsigned ch = L->chunk ? L->chunk : pipe_auto_chunk(s, TX);
-  if ((ch & (ch - 1)) != 0) return fail(TCS_ERR_UNSUPPORTED, "pipe: planes per chunk must be a power of two");
+  const unsigned ch = L->chunk ? L->chunk : pipe_auto_chunk(s, L->block[0], L->block[1]);
   const unsigned W = pipe_width(TX, R, lshift, vec, ch, rows, es);
   if (W > 256 || rows > 256 || ch > 256)
     return fail(TCS_ERR_UNSUPPORTED, "pipe: tile exceeds the 256-element TMA box limit");
   const unsigned chunk_bytes = ch * rows * W * es;
-  PipeKey key{L->block[0], s.dimension == 3 ? L->block[1] : 1u, ch, lshift, pipe_auto_unroll(s)};
+  PipeKey key{L->block[0], s.dimension == 3 ? L->block[1] : 1u, ch, lshift};
   PipeMod* pm = nullptr;
   int rc = pipe_module(h, key, &pm);
   if (rc) return rc;
@@ -1210,9 +1217,8 @@ int tcs_precompile_pipe(const tcs_spec* spec, unsigned bx, unsigned by, unsigned
   const unsigned vec = 16u / (unsigned)elem_size(s);
   if (bx == 0 || (bx * (unsigned)s.cx) % vec != 0)
     return fail(TCS_ERR_UNSUPPORTED, "pipe: unsupported block");
-  if (chunk == 0) chunk = pipe_auto_chunk(s, bx * (unsigned)s.cx);
-  if ((chunk & (chunk - 1)) != 0) return fail(TCS_ERR_UNSUPPORTED, "pipe: chunk not a power of two");
-  PipeKey key{bx, s.dimension == 3 ? by : 1u, chunk, left_offset_of(s) % vec, pipe_auto_unroll(s)};
+  if (chunk == 0) chunk = pipe_auto_chunk(s, bx, by);
+  PipeKey key{bx, s.dimension == 3 ? by : 1u, chunk, left_offset_of(s) % vec};
   std::vector<char> cubin;
   std::string path;
   rc = instantiate(s, &key, cubin, &path);

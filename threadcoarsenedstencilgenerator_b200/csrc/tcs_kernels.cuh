@@ -406,10 +406,8 @@ constexpr int PW = pipe_width();     // shared-memory row width (elements)
 constexpr int PLANE = PW * ROWS;     // elements per plane
 constexpr int CHUNK = CHP * PLANE;   // elements per ring slot
 constexpr int NP2 = 2 * R + 1;       // pipeline depth (output planes in flight)
-constexpr int UNR = TCS_UNROLL;      // input planes per unrolled loop body (<= NP2)
 static_assert(!(DIM == 2 && ORIENT == 1), "2D Column orientation is not pipelined");
-static_assert(UNR >= 1 && UNR <= NP2, "unroll depth must be in [1, 2R+1]");
-static_assert((CHP & (CHP - 1)) == 0, "planes per chunk must be a power of two");
+static_assert(CHP >= 1, "planes per chunk");
 static_assert(TXP % VEC == 0, "tile width must be a multiple of the 16-byte granule");
 // Columns whose element index is even for every thread: the thread origin sits at ring column
 // LSHIFT + R + tx*CX and every row, plane and chunk starts on a 16-byte boundary, so with CX even
@@ -554,106 +552,101 @@ extern "C" __global__ void __launch_bounds__(TCS_BX * ((TCS_DIM == 3) ? TCS_BY :
     const tcs_i64 plane_g = (tcs_i64)g.xdim;
     T* obase = out + (tcs_u64)x;
 #endif
-    // Cursors advanced by additions only: ring slot and phase of the current chunk, the plane
-    // within it, and the output plane completed after the current input plane (pi - 2R).
+    // One loop iteration consumes one ring chunk: wait for it (bounded), release the slot of the
+    // previous chunk to the next copy, then run its CHP planes as straight-line code.  The slot
+    // cursor advances by additions only.  Output pi - 2R is complete after input plane pi.
     tcs_u32 cur_slot = gc % nslot;
     tcs_u32 cur_par = (gc / nslot) & 1u;
-    tcs_u32 in_chunk = 0;
-    tcs_u32 j = 0;  // chunk of the piece being consumed
-    const T* pt = ring + cur_slot * CHUNK + lane_off;
     T* optr = obase + ((tcs_i64)ms - 2 * R) * plane_g;
     bool aborted = false;
-    for (tcs_u32 s = 0; s * UNR < np && !aborted; ++s) {
-      static_for<0, UNR>([&](auto tt) {
-        constexpr int t = decltype(tt)::value;
-        const tcs_u32 pi = s * UNR + t;  // input plane index within the piece
-        if (pi < np && !aborted) {
-          if (in_chunk == 0) {
-            const bool expired = mbar_wait_bounded(bars + 8u * cur_slot, cur_par, TCS_WAIT_LIMIT);
-            if (__syncthreads_or(expired)) {
-              aborted = true;
-              if (use_tma) {
-                if (tid == 0) {
-                  atomicOr(&tcs_status, TCS_DEV_TIMEOUT);
-                  const tcs_u32 hi = min(j + nslot - 2, nch - 1);
-                  for (tcs_u32 jj = j; jj <= hi; ++jj)
-                    (void)mbar_wait_bounded(bars + 8u * ((gc + jj) % nslot), ((gc + jj) / nslot) & 1u,
-                                            TCS_WAIT_LIMIT);
-                }
-              } else {
-                if (tid == 0) atomicOr(&tcs_status, TCS_DEV_TIMEOUT);
-                cp_async_wait_all();
-              }
-            } else if (j + nslot - 1 < nch) {
-              if (!use_tma)
-                issue(j + nslot - 1);
-              else if (tid == 0)
-                issue(j + nslot - 1);
-            }
+    for (tcs_u32 j = 0; j < nch; ++j) {
+      const bool expired = mbar_wait_bounded(bars + 8u * cur_slot, cur_par, TCS_WAIT_LIMIT);
+      if (__syncthreads_or(expired)) {
+        aborted = true;
+        if (use_tma) {
+          if (tid == 0) {
+            atomicOr(&tcs_status, TCS_DEV_TIMEOUT);
+            const tcs_u32 hi = min(j + nslot - 2, nch - 1);
+            for (tcs_u32 jj = j; jj <= hi; ++jj)
+              (void)mbar_wait_bounded(bars + 8u * ((gc + jj) % nslot), ((gc + jj) / nslot) & 1u,
+                                      TCS_WAIT_LIMIT);
           }
-          if (!aborted) {
-            const PipeRing ld{pt};
-            auto slot = [&](auto kk) -> T(&)[NEP] {
-              constexpr int k = decltype(kk)::value;
-              return acc[((t - k) % NP2 + NP2) % NP2];
-            };
-            pipe_plane(ld, slot);
-            // output pi - 2R received its last term (march-axis offset +R)
-            const int op = (int)pi - 2 * R;
-            if (lane_ok && op >= 0 && op < (int)nout) {
-              constexpr T c = T(1) / T(S);
-              T(&done)[NEP] = acc[((t - 2 * R) % NP2 + NP2) % NP2];
-              // Output x is R + leftOff + an even offset when CX is even: pairs are aligned when
-              // R + LSHIFT is even (the shared-memory pair rule at gx = 0).
-              static_for<0, (DIM == 3) ? CY : 1>([&](auto ey) {
-                static_for<0, CX>([&](auto ex) {
-                  constexpr int e = decltype(ex)::value + decltype(ey)::value * CX;
-                  constexpr bool pair = pipe_pair_aligned(0) && (decltype(ex)::value % 2 == 0);
-                  constexpr bool tail = pipe_pair_aligned(0) && (decltype(ex)::value % 2 == 1);
-                  T* o = optr + decltype(ex)::value + decltype(ey)::value * (tcs_i64)g.xdim;
-                  if constexpr (pair) {
-                    const T v0 = (COEFF == 0) ? done[e] * c : done[e];
-                    const T v1 = (COEFF == 0) ? done[e + 1] * c : done[e + 1];
-                    if (st_pair) {
-                      typename PairOf<T>::type v2;
-                      v2.x = v0;
-                      v2.y = v1;
-                      *reinterpret_cast<typename PairOf<T>::type*>(o) = v2;
-                    } else {
-                      o[0] = v0;
-                      o[1] = v1;
-                    }
-                  } else if constexpr (!tail) {
-                    *o = (COEFF == 0) ? done[e] * c : done[e];
+        } else {
+          if (tid == 0) atomicOr(&tcs_status, TCS_DEV_TIMEOUT);
+          cp_async_wait_all();
+        }
+        break;
+      }
+      if (j + nslot - 1 < nch) {
+        if (!use_tma)
+          issue(j + nslot - 1);
+        else if (tid == 0)
+          issue(j + nslot - 1);
+      }
+      const T* pc = ring + cur_slot * CHUNK + lane_off;
+      const tcs_u32 pbase = j * CHP;  // input plane index (within the piece) of the chunk's first
+      static_for<0, CHP>([&](auto tt) {
+        constexpr int t = decltype(tt)::value;
+        const tcs_u32 pi = pbase + t;
+        if (pi < np) {
+          const PipeRing ld{pc + t * PLANE};
+          auto slot = [&](auto kk) -> T(&)[NEP] {
+            constexpr int k = decltype(kk)::value;
+            return acc[((t - k) % NP2 + NP2) % NP2];
+          };
+          pipe_plane(ld, slot);
+          const int op = (int)pi - 2 * R;
+          if (lane_ok && op >= 0 && op < (int)nout) {
+            constexpr T c = T(1) / T(S);
+            T(&done)[NEP] = acc[((t - 2 * R) % NP2 + NP2) % NP2];
+            T* orow = optr + (tcs_i64)t * plane_g;
+            // Output x is R + leftOff + an even offset when CX is even: pairs are aligned when
+            // R + LSHIFT is even (the shared-memory pair rule at gx = 0).
+            static_for<0, (DIM == 3) ? CY : 1>([&](auto ey) {
+              static_for<0, CX>([&](auto ex) {
+                constexpr int e = decltype(ex)::value + decltype(ey)::value * CX;
+                constexpr bool pair = pipe_pair_aligned(0) && (decltype(ex)::value % 2 == 0);
+                constexpr bool tail = pipe_pair_aligned(0) && (decltype(ex)::value % 2 == 1);
+                T* o = orow + decltype(ex)::value + decltype(ey)::value * (tcs_i64)g.xdim;
+                if constexpr (pair) {
+                  const T v0 = (COEFF == 0) ? done[e] * c : done[e];
+                  const T v1 = (COEFF == 0) ? done[e + 1] * c : done[e + 1];
+                  if (st_pair) {
+                    typename PairOf<T>::type v2;
+                    v2.x = v0;
+                    v2.y = v1;
+                    *reinterpret_cast<typename PairOf<T>::type*>(o) = v2;
+                  } else {
+                    o[0] = v0;
+                    o[1] = v1;
                   }
-                });
+                } else if constexpr (!tail) {
+                  *o = (COEFF == 0) ? done[e] * c : done[e];
+                }
               });
-            }
-            optr += plane_g;
-            pt += PLANE;
-            if (++in_chunk == (tcs_u32)CHP) {
-              in_chunk = 0;
-              ++j;
-              if (++cur_slot == nslot) {
-                cur_slot = 0;
-                cur_par ^= 1u;
-              }
-              pt = ring + cur_slot * CHUNK + lane_off;
-            }
+            });
           }
         }
       });
-      // Re-align the register slots with the next body: slot m takes what slot (m + UNR) held.
-      if constexpr (UNR % NP2 != 0) {
+      // Re-align the register slots with the next chunk: slot m takes what slot (m + CHP) held.
+      if constexpr (CHP % NP2 != 0) {
         T tmp[NP2][NEP];
         static_for<0, NP2>([&](auto m) {
-          static_for<0, NEP>([&](auto e) { tmp[decltype(m)::value][decltype(e)::value] = acc[decltype(m)::value][decltype(e)::value]; });
+          static_for<0, NEP>([&](auto e) {
+            tmp[decltype(m)::value][decltype(e)::value] = acc[decltype(m)::value][decltype(e)::value];
+          });
         });
         static_for<0, NP2>([&](auto m) {
           static_for<0, NEP>([&](auto e) {
-            acc[decltype(m)::value][decltype(e)::value] = tmp[(decltype(m)::value + UNR) % NP2][decltype(e)::value];
+            acc[decltype(m)::value][decltype(e)::value] =
+                tmp[(decltype(m)::value + CHP) % NP2][decltype(e)::value];
           });
         });
+      }
+      optr += (tcs_i64)CHP * plane_g;
+      if (++cur_slot == nslot) {
+        cur_slot = 0;
+        cur_par ^= 1u;
       }
     }
     if (aborted) return;
