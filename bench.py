@@ -43,60 +43,105 @@ def _peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+    """SM clock and clock-event (throttle) reasons sampled during the timed region.
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NVML is polled every ~5 ms from a thread (the device is matched by UUID); when NVML is not
+    usable, `nvidia-smi --query-gpu ... -lms 200` is read instead."""
+
+    REASONS = {0x8: "hw_slowdown", 0x40: "hw_thermal_slowdown", 0x20: "sw_thermal_slowdown",
+               0x4: "sw_power_cap", 0x80: "hw_power_brake_slowdown"}
 
     def __init__(self, index: int):
         self.index = index
-        self.proc = None
-        self.lines = []
+        self.sm, self.smax, self.reasons = [], [], set()
+        self.stop_flag = threading.Event()
         self.thread = None
+        self.proc = None
+        self.nvml = None
+
+    def _nvml_handle(self):
+        import pynvml
+        import torch
+
+        pynvml.nvmlInit()
+        uuid = str(torch.cuda.get_device_properties(self.index).uuid)
+        for cand in (uuid, "GPU-" + uuid):
+            try:
+                return pynvml, pynvml.nvmlDeviceGetHandleByUUID(cand)
+            except Exception:
+                continue
+        return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.index)
 
     def start(self):
         try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            nv, h = self._nvml_handle()
+            self.nvml = (nv, h)
+            self.smax.append(float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)))
+            getr = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+                nv.nvmlDeviceGetCurrentClocksThrottleReasons
+
+            def poll():
+                while not self.stop_flag.is_set():
+                    try:
+                        self.sm.append(float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)))
+                        bits = int(getr(h))
+                        for bit, name in self.REASONS.items():
+                            if bits & bit:
+                                self.reasons.add(name)
+                    except Exception:
+                        pass
+                    time.sleep(0.005)
+
+            self.thread = threading.Thread(target=poll, daemon=True)
+            self.thread.start()
+            return
+        except Exception:
+            self.nvml = None
+        fields = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                  "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                  "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + fields,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except OSError:
             self.proc = None
             return
-        self.thread = threading.Thread(target=self._read, daemon=True)
+
+        def read():
+            names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+            for line in self.proc.stdout:
+                parts = [q.strip() for q in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    self.sm.append(float(parts[1]))
+                    self.smax.append(float(parts[2]))
+                except ValueError:
+                    continue
+                for name, val in zip(names, parts[5:9]):
+                    if val.lower().startswith("active"):
+                        self.reasons.add(name)
+
+        self.thread = threading.Thread(target=read, daemon=True)
         self.thread.start()
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
-
     def stop(self) -> dict:
-        if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        time.sleep(0.25)
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except subprocess.TimeoutExpired:
-            self.proc.kill()
+        self.stop_flag.set()
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
         if self.thread:
             self.thread.join(timeout=2)
-        sm, smax, reasons = [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
-            parts = [p.strip() for p in ln.split(",")]
-            if len(parts) < 9:
-                continue
-            try:
-                sm.append(float(parts[1]))
-                smax.append(float(parts[2]))
-            except ValueError:
-                continue
-            for name, val in zip(names, parts[5:9]):
-                if val.lower().startswith("active"):
-                    reasons.add(name)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+        if not self.sm:
+            return {"sm_mhz": None, "sm_max_mhz": max(self.smax) if self.smax else None,
+                    "reasons": sorted(self.reasons), "samples": 0}
+        return {"sm_mhz": statistics.median(self.sm), "sm_max_mhz": max(self.smax) if self.smax else None,
+                "reasons": sorted(self.reasons), "samples": len(self.sm),
+                "source": "nvml" if self.nvml else "nvidia-smi"}
 
 
 def _dist():
@@ -208,7 +253,6 @@ def run_ours(args) -> dict | None:
     torch.cuda.synchronize()
     sampler = ClockSampler(local)
     sampler.start()
-    time.sleep(0.3)
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
@@ -305,6 +349,90 @@ def run_ours(args) -> dict | None:
     return line
 
 
+def run_precision(args) -> dict | None:
+    """FP64 vs FP32 vs FP32 with FP64 defect correction on one workload (single GPU): each runs the
+    workload's full sweep count from the same input; errors are measured on the GPU against the
+    FP64 result (the engine's FP64 sweep is bit-identical to the reference kernel)."""
+    import numpy as np
+    import torch
+
+    import threadcoarsenedstencilgenerator_b200 as tcs
+    from threadcoarsenedstencilgenerator_b200.mixed import DefectCorrectedSweeps
+    from threadcoarsenedstencilgenerator_b200.workloads import WORKLOADS
+
+    torch.cuda.set_device(0)
+    w = WORKLOADS[args.workload]
+    spec = w.tuned_spec()
+    launch = w.tuned_launch()
+    geom = spec.geometry(*w.grid)
+    mask = w.make_mask()
+    n = args.sweeps or w.sweeps
+    a = w.make_input(geom)
+    points = geom.interior_points
+    stream = torch.cuda.current_stream()
+    ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
+
+    dc = DefectCorrectedSweeps(spec, launch, mask=mask)
+    # FP64
+    x = torch.from_numpy(a).cuda()
+    y = x.clone()
+    dc.s64.sweeps(geom, x, y, 3, launch)
+    x.copy_(torch.from_numpy(a))
+    y.copy_(x)
+    e0, e1 = ev(), ev()
+    e0.record(stream)
+    ref = dc.s64.sweeps(geom, x, y, n, launch, stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t64 = e0.elapsed_time(e1)
+    # plain FP32
+    x32 = torch.from_numpy(a.astype(np.float32)).cuda()
+    y32 = x32.clone()
+    dc.s32.sweeps(geom, x32, y32, 3, launch)
+    x32.copy_(torch.from_numpy(a.astype(np.float32)))
+    y32.copy_(x32)
+    e0, e1 = ev(), ev()
+    e0.record(stream)
+    r32 = dc.s32.sweeps(geom, x32, y32, n, launch, stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t32 = e0.elapsed_time(e1)
+    s32 = dc.s64.compare(geom, r32, ref, "f32")
+    del x32, y32
+    # FP32 + FP64 defect correction
+    xm = torch.from_numpy(a).cuda()
+    work = {"sx": xm.clone(), "r": torch.zeros(geom.shape, dtype=torch.float32, device="cuda"),
+            "e0": torch.zeros(geom.shape, dtype=torch.float32, device="cuda"),
+            "e1": torch.zeros(geom.shape, dtype=torch.float32, device="cuda")}
+    e0, e1 = ev(), ev()
+    e0.record(stream)
+    xm, res = dc.run(geom, xm, n, args.period, stream, work)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    tmix = e0.elapsed_time(e1)
+    smix = dc.s64.compare(geom, xm, ref, "f64")
+    glups = lambda ms: points * n / (ms / 1e3) / 1e9  # noqa: E731
+    return {
+        "metric": "GLup/s (%s, %d sweeps, FP32 sweeps with FP64 defect correction every %d)" % (w.name, n, args.period),
+        "value": glups(tmix), "unit": "GLup/s", "n_gpus": 1, "steps": n, "warmup": 3,
+        "ms_per_step": tmix / n, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32+f64", "data": "synthetic (numpy default_rng seed %d)" % w.seed,
+        "config": {"workload": w.name, "grid": list(w.grid[:spec.dimension]), "coarsening": list(spec.coarsening),
+                   "block": list(launch.block), "variant": launch.variant, "period": args.period},
+        "precision": {
+            "f64": {"glups": glups(t64), "ms": t64},
+            "f32": {"glups": glups(t32), "ms": t32, "max_rel": s32["max_rel"], "rms_rel": s32["rms_rel"]},
+            "f32_defect_corrected": {"glups": glups(tmix), "ms": tmix, "max_rel": smix["max_rel"],
+                                     "rms_rel": smix["rms_rel"], "fp64_sweeps": res.fp64_sweeps,
+                                     "fp32_sweeps": res.fp32_sweeps,
+                                     "final_residual_max": res.residual_history[-1][0]},
+            "speedup_vs_f64": t64 / tmix,
+            "error_definition": "max_rel = max|a-b| / max|b|, rms_rel = ||a-b||_2 / ||b||_2 over the interior, "
+                                "b = FP64 result after the same sweeps",
+        },
+    }
+
+
 def run_reference(args) -> dict | None:
     """The reference's own stencil arithmetic on the host cores (oracle OpenMP restatement)."""
     import numpy as np
@@ -354,9 +482,18 @@ def main() -> int:
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--precision", default="f64", choices=["f64", "mixed"],
+                    help="mixed: FP64 vs FP32 vs FP32 with FP64 defect correction on the workload")
+    ap.add_argument("--sweeps", type=int, default=0, help="precision mode: sweeps (default: the workload's)")
+    ap.add_argument("--period", type=int, default=20, help="precision mode: FP32 sweeps per FP64 defect")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
-    line = run_reference(args) if args.impl == "reference" else run_ours(args)
+    if args.impl == "reference":
+        line = run_reference(args)
+    elif args.precision == "mixed":
+        line = run_precision(args)
+    else:
+        line = run_ours(args)
     if line is not None:
         print(json.dumps(line))
     return 0

@@ -189,6 +189,31 @@ int tcs_precompile(const tcs_spec* spec, char* cubin_path, unsigned path_cap);
 int tcs_precompile_pipe(const tcs_spec* spec, unsigned bx, unsigned by, unsigned chunk,
                         char* cubin_path, unsigned path_cap);
 
+/* ---- Mixed-precision helpers (FP64 defect correction of FP32 sweeps) ----
+ * All act on the interior of buffers laid out like the sweep buffers (gridSize, rightOffset).
+ * They are additions of this engine; the reference computes in FP64 only. */
+
+/* One sweep out = stencil(in) + src (src: same layout and precision).  With src == NULL this is
+ * tcs_update_grid. */
+int tcs_update_grid_source(tcs_stencil* h, const unsigned grid[3], unsigned right_offset,
+                           const tcs_launch* launch, const void* in, const void* src, void* out,
+                           void* stream);
+
+/* FP64 defect r = fl32(sx - x) (sx = one FP64 sweep of x) and, when norms != NULL, the global
+ * residual norms {max |sx - x|, ||sx - x||_2} computed on the GPU in FP64 (synchronises
+ * `stream`).  Uses library-allocated scratch memory for the per-block partial sums. */
+int tcs_residual(tcs_stencil* h, const unsigned grid[3], unsigned right_offset, const double* x,
+                 const double* sx, float* r, double norms[2], void* stream);
+
+/* x += e (FP64 state, FP32 correction). */
+int tcs_accumulate(tcs_stencil* h, const unsigned grid[3], unsigned right_offset, double* x,
+                   const float* e, void* stream);
+
+/* Error statistics of a (TCS_F32 or TCS_F64) against b (FP64): {max |a-b|, ||a-b||_2, max |b|,
+ * ||b||_2} over the interior, computed on the GPU (synchronises `stream`). */
+int tcs_compare(tcs_stencil* h, const unsigned grid[3], unsigned right_offset, const void* a,
+                int a_precision, const double* b, double stats[4], void* stream);
+
 /* Number of SMs of the current device. */
 int tcs_device_sm_count(int* out);
 

@@ -27,7 +27,7 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 HOST_SOURCES = ["tcs_capi.cpp"]
-CUDA_SOURCES: list[str] = []  # AOT device code compiled straight into libtcs.so
+CUDA_SOURCES: list[str] = ["tcs_field.cu"]  # AOT device code compiled straight into libtcs.so
 
 
 def _run(cmd: list[str]) -> None:
@@ -58,7 +58,7 @@ def _embed_kernel_source() -> Path:
 
 def _inputs_digest() -> str:
     h = hashlib.sha256()
-    files = [CSRC / f for f, _ in DEVICE_HEADERS] + [INCLUDE / "tcs.h", Path(__file__)]
+    files = [CSRC / f for f, _ in DEVICE_HEADERS] + [INCLUDE / "tcs.h", Path(__file__), CSRC / "tcs_field.h"]
     files += [CSRC / f for f in HOST_SOURCES + CUDA_SOURCES]
     for f in sorted(files):
         h.update(f.name.encode())

@@ -25,6 +25,7 @@
 #include <unistd.h>
 
 #include <algorithm>
+#include <cmath>
 #include <chrono>
 #include <cstdint>
 #include <cstdio>
@@ -36,6 +37,7 @@
 #include <string>
 #include <vector>
 
+#include "tcs_field.h"
 #include "tcs_kernels_src.inc"  // tcs_kernels_src[], tcs_tile_src[]: the device headers
 
 namespace {
@@ -342,6 +344,8 @@ struct tcs_stencil {
   int dropin_variant = TCS_VARIANT_AUTO;  // variant used by tcs_benchmark_update_grid
   unsigned dropin_segments = 0, dropin_depth = 0;
   std::vector<double> mask_host;          // last mask uploaded (copied into new pipe modules)
+  double* scratch = nullptr;              // per-block partials of the field reductions
+  size_t scratch_len = 0;                 // in doubles
   std::vector<PipeMod*> pipes;            // pipelined-sweep modules, one per launch shape
   std::mutex mu;
   std::vector<MapEntry> maps;
@@ -812,13 +816,16 @@ int tensor_map(tcs_stencil* h, const void* ptr, const Resolved& r, CUtensorMap**
   return TCS_OK;
 }
 
-int launch_resolved(tcs_stencil* h, const Resolved& r, const void* in, void* out, CUstream st) {
+int launch_resolved(tcs_stencil* h, const Resolved& r, const void* in, void* out, CUstream st,
+                    const void* src = nullptr) {
   if (!in || !out) return fail(TCS_ERR_INVALID_VALUE, "NULL device buffer");
   if (in == out) return fail(TCS_ERR_INVALID_VALUE, "input and output must be distinct buffers");
+  if (src == out) return fail(TCS_ERR_INVALID_VALUE, "source and output must be distinct buffers");
+  CUdeviceptr psrc = (CUdeviceptr)src;
   TcsGeo geo = r.geo;
   if (r.variant == TCS_VARIANT_DIRECT) {
     CUdeviceptr pin = (CUdeviceptr)in, pout = (CUdeviceptr)out;
-    void* args[] = {&pin, &pout, &geo};
+    void* args[] = {&pin, &pout, &psrc, &geo};
     TCS_CU(g_drv.LaunchKernel(h->f_direct, r.grid[0], r.grid[1], r.grid[2], r.block[0],
                               r.block[1], r.block[2], 0, st, args, nullptr));
     return TCS_OK;
@@ -835,7 +842,7 @@ int launch_resolved(tcs_stencil* h, const Resolved& r, const void* in, void* out
       pmap = *map;
     }
     CUdeviceptr pin = (CUdeviceptr)in, pout = (CUdeviceptr)out;
-    void* args[] = {&pmap, &pin, &pout, &pg};
+    void* args[] = {&pmap, &pin, &pout, &psrc, &pg};
     TCS_CU(g_drv.LaunchKernel(r.pipe->f, r.grid[0], 1, 1, r.block[0], r.block[1], 1, r.smem, st,
                               args, nullptr));
     return TCS_OK;
@@ -851,7 +858,7 @@ int launch_resolved(tcs_stencil* h, const Resolved& r, const void* in, void* out
     mcopy = *map;
   }
   CUdeviceptr pin = (CUdeviceptr)in, pout = (CUdeviceptr)out;
-  void* args[] = {&mcopy, &pin, &pout, &geo};
+  void* args[] = {&mcopy, &pin, &pout, &psrc, &geo};
   TCS_CU(g_drv.LaunchKernel(h->f_march, r.grid[0], r.grid[1], r.grid[2], r.block[0], r.block[1],
                             r.block[2], r.smem, st, args, nullptr));
   return TCS_OK;
@@ -975,6 +982,7 @@ int tcs_create(const tcs_spec* spec, tcs_stencil** out) {
 
 int tcs_destroy(tcs_stencil* h) {
   if (!h) return TCS_OK;
+  if (h->scratch) cudaFree(h->scratch);
   for (PipeMod* p : h->pipes) {
     if (p->mod && g_drv.ModuleUnload) g_drv.ModuleUnload(p->mod);
     delete p;
@@ -1047,6 +1055,16 @@ int tcs_update_grid(tcs_stencil* h, const unsigned grid[3], unsigned right_offse
   int rc = resolve(h, grid, right_offset, launch, r);
   if (rc) return rc;
   return launch_resolved(h, r, in, out, (CUstream)stream);
+}
+
+int tcs_update_grid_source(tcs_stencil* h, const unsigned grid[3], unsigned right_offset,
+                           const tcs_launch* launch, const void* in, const void* src, void* out,
+                           void* stream) {
+  Resolved r;
+  int rc = resolve(h, grid, right_offset, launch, r);
+  if (rc) return rc;
+  if (!src) return fail(TCS_ERR_INVALID_VALUE, "NULL source buffer");
+  return launch_resolved(h, r, in, out, (CUstream)stream, src);
 }
 
 int tcs_sweeps(tcs_stencil* h, const unsigned grid[3], unsigned right_offset,
@@ -1227,6 +1245,99 @@ int tcs_precompile_pipe(const tcs_spec* spec, unsigned bx, unsigned by, unsigned
     std::strncpy(cubin_path, path.c_str(), path_cap - 1);
     cubin_path[path_cap - 1] = '\0';
   }
+  return TCS_OK;
+}
+
+namespace {
+
+// Interior box of a buffer with the reference geometry (gridSize, rightOffset).
+int field_geo(const tcs_stencil* h, const unsigned grid[3], unsigned right_offset, TcsFieldGeo& f) {
+  TcsGeo g;
+  int rc = make_geo(h, grid, right_offset, g);
+  if (rc) return rc;
+  const unsigned R = (unsigned)h->spec.range;
+  f.xdim = g.xdim;
+  f.ydim = g.ydim;
+  f.x0 = g.x0;
+  f.x_lim = g.x_lim;
+  f.y0 = R;
+  f.y_lim = g.y_lim;
+  f.z0 = h->spec.dimension == 3 ? R : 0;
+  f.z_lim = g.z_lim;
+  return TCS_OK;
+}
+
+int field_blocks(const tcs_stencil* h) { return 2 * std::max(1, h->num_sms); }
+
+// Scratch of the two-pass reductions: nblocks*4 partials + 8 result slots, allocated once.
+int ensure_scratch(tcs_stencil* h, size_t need) {
+  std::lock_guard<std::mutex> lock(h->mu);
+  if (h->scratch_len >= need) return TCS_OK;
+  if (h->scratch) cudaFree(h->scratch);
+  h->scratch = nullptr;
+  h->scratch_len = 0;
+  TCS_RT(cudaMalloc(&h->scratch, need * sizeof(double)));
+  h->scratch_len = need;
+  return TCS_OK;
+}
+
+}  // namespace
+
+int tcs_residual(tcs_stencil* h, const unsigned grid[3], unsigned right_offset, const double* x,
+                 const double* sx, float* r, double norms[2], void* stream) {
+  if (!h || !x || !sx || !r) return fail(TCS_ERR_INVALID_VALUE, "NULL argument");
+  TcsFieldGeo f;
+  int rc = field_geo(h, grid, right_offset, f);
+  if (rc) return rc;
+  const int nb = field_blocks(h);
+  rc = ensure_scratch(h, (size_t)nb * 4 + 8);
+  if (rc) return rc;
+  double* res = h->scratch + (size_t)nb * 4;
+  const int e = tcs_field_launch_defect(x, sx, r, f, h->scratch, nb, res, (cudaStream_t)stream);
+  if (e != 0) return fail(TCS_ERR_CUDA, std::string("defect kernel: ") + cudaGetErrorString((cudaError_t)e));
+  if (norms) {
+    double host[2];
+    TCS_RT(cudaMemcpyAsync(host, res, sizeof(host), cudaMemcpyDeviceToHost, (cudaStream_t)stream));
+    TCS_RT(cudaStreamSynchronize((cudaStream_t)stream));
+    norms[0] = host[0];
+    norms[1] = std::sqrt(host[1]);
+  }
+  return TCS_OK;
+}
+
+int tcs_accumulate(tcs_stencil* h, const unsigned grid[3], unsigned right_offset, double* x,
+                   const float* e, void* stream) {
+  if (!h || !x || !e) return fail(TCS_ERR_INVALID_VALUE, "NULL argument");
+  TcsFieldGeo f;
+  int rc = field_geo(h, grid, right_offset, f);
+  if (rc) return rc;
+  const int err = tcs_field_launch_add(x, e, f, field_blocks(h), (cudaStream_t)stream);
+  if (err != 0) return fail(TCS_ERR_CUDA, std::string("add kernel: ") + cudaGetErrorString((cudaError_t)err));
+  return TCS_OK;
+}
+
+int tcs_compare(tcs_stencil* h, const unsigned grid[3], unsigned right_offset, const void* a,
+                int a_precision, const double* b, double stats[4], void* stream) {
+  if (!h || !a || !b || !stats) return fail(TCS_ERR_INVALID_VALUE, "NULL argument");
+  if (a_precision != TCS_F64 && a_precision != TCS_F32)
+    return fail(TCS_ERR_INVALID_VALUE, "unknown precision");
+  TcsFieldGeo f;
+  int rc = field_geo(h, grid, right_offset, f);
+  if (rc) return rc;
+  const int nb = field_blocks(h);
+  rc = ensure_scratch(h, (size_t)nb * 4 + 8);
+  if (rc) return rc;
+  double* res = h->scratch + (size_t)nb * 4;
+  const int e = tcs_field_launch_compare(a, a_precision == TCS_F32 ? 1 : 0, b, f, h->scratch, nb, res,
+                                         (cudaStream_t)stream);
+  if (e != 0) return fail(TCS_ERR_CUDA, std::string("compare kernel: ") + cudaGetErrorString((cudaError_t)e));
+  double host[4];
+  TCS_RT(cudaMemcpyAsync(host, res, sizeof(host), cudaMemcpyDeviceToHost, (cudaStream_t)stream));
+  TCS_RT(cudaStreamSynchronize((cudaStream_t)stream));
+  stats[0] = host[0];
+  stats[1] = std::sqrt(host[1]);
+  stats[2] = host[2];
+  stats[3] = std::sqrt(host[3]);
   return TCS_OK;
 }
 

@@ -157,7 +157,8 @@ __device__ __forceinline__ void cp_async_wait_all() {
 // ---- tcs_direct: the reference's launch geometry, operands through L1 -------------------------
 // Thread origin and tile guard as in cuda/generate2DStencil_cuda.py:78-104 and
 // cuda/generate3DStencil_cuda.py:81-114 (x0 already includes the Write left offset).
-extern "C" __global__ void tcs_direct(const T* __restrict__ in, T* __restrict__ out, const TcsGeo g) {
+extern "C" __global__ void tcs_direct(const T* __restrict__ in, T* __restrict__ out,
+                                      const T* __restrict__ src, const TcsGeo g) {
   using namespace tcs;
   const tcs_u64 x = (tcs_u64)(blockIdx.x * blockDim.x + threadIdx.x) * CX + g.x0;
   const tcs_u64 y = (tcs_u64)(blockIdx.y * blockDim.y + threadIdx.y) * CY + R;
@@ -173,7 +174,7 @@ extern "C" __global__ void tcs_direct(const T* __restrict__ in, T* __restrict__ 
     };
     T acc[NE];
     traverse(ld, acc);
-    store(out + base, acc, g.xdim, (tcs_u64)plane);
+    store(out + base, acc, g.xdim, (tcs_u64)plane, src ? src + base : nullptr);
   }
 }
 
@@ -188,7 +189,7 @@ extern "C" __global__ void tcs_direct(const T* __restrict__ in, T* __restrict__ 
 // elements with cp.async and signal the same mbarrier through cp.async.mbarrier.arrive.
 extern "C" __global__ void tcs_march(const __grid_constant__ TcsTmaMap tmap,
                                      const T* __restrict__ in, T* __restrict__ out,
-                                     const TcsGeo g) {
+                                     const T* __restrict__ src, const TcsGeo g) {
   using namespace tcs;
   extern __shared__ __align__(128) unsigned char tcs_smem[];
   const tcs_u32 nslot = g.nslot;
@@ -337,7 +338,8 @@ extern "C" __global__ void tcs_march(const __grid_constant__ TcsTmaMap tmap,
         return ring[rr * W + col + gx];
       };
       traverse(ld, acc);
-      store(out + (tcs_u64)x + (tcs_u64)m * g.xdim, acc, g.xdim, plane_g);
+      const tcs_u64 ob = (tcs_u64)x + (tcs_u64)m * g.xdim;
+      store(out + ob, acc, g.xdim, plane_g, src ? src + ob : nullptr);
 #else
       auto ld = [&](int gx, int gy, int gz) {
         tcs_u32 pp = pb + (tcs_u32)(gz + R);
@@ -345,7 +347,8 @@ extern "C" __global__ void tcs_march(const __grid_constant__ TcsTmaMap tmap,
         return ring[pp * plane_elems + (row0 + gy) * W + col + gx];
       };
       traverse(ld, acc);
-      store(out + (tcs_u64)x + (tcs_u64)y * g.xdim + (tcs_u64)m * plane_g, acc, g.xdim, plane_g);
+      const tcs_u64 ob = (tcs_u64)x + (tcs_u64)y * g.xdim + (tcs_u64)m * plane_g;
+      store(out + ob, acc, g.xdim, plane_g, src ? src + ob : nullptr);
 #endif
     }
     ring_base += STEP;
@@ -456,7 +459,7 @@ struct TcsPipeGeo {
 
 extern "C" __global__ void __launch_bounds__(TCS_BX * ((TCS_DIM == 3) ? TCS_BY : 1))
     tcs_pipe(const __grid_constant__ TcsTmaMap tmap, const T* __restrict__ in,
-             T* __restrict__ out, const TcsPipeGeo g) {
+             T* __restrict__ out, const T* __restrict__ src, const TcsPipeGeo g) {
   using namespace tcs;
   extern __shared__ __align__(128) unsigned char tcs_smem[];
   const tcs_u32 nslot = g.nslot;
@@ -608,9 +611,14 @@ extern "C" __global__ void __launch_bounds__(TCS_BX * ((TCS_DIM == 3) ? TCS_BY :
                 constexpr bool pair = pipe_pair_aligned(0) && (decltype(ex)::value % 2 == 0);
                 constexpr bool tail = pipe_pair_aligned(0) && (decltype(ex)::value % 2 == 1);
                 T* o = orow + decltype(ex)::value + decltype(ey)::value * (tcs_i64)g.xdim;
+                const T* so = src ? src + (o - out) : nullptr;
                 if constexpr (pair) {
-                  const T v0 = (COEFF == 0) ? done[e] * c : done[e];
-                  const T v1 = (COEFF == 0) ? done[e + 1] * c : done[e + 1];
+                  T v0 = (COEFF == 0) ? done[e] * c : done[e];
+                  T v1 = (COEFF == 0) ? done[e + 1] * c : done[e + 1];
+                  if (so) {
+                    v0 = v0 + so[0];
+                    v1 = v1 + so[1];
+                  }
                   if (st_pair) {
                     typename PairOf<T>::type v2;
                     v2.x = v0;
@@ -621,7 +629,9 @@ extern "C" __global__ void __launch_bounds__(TCS_BX * ((TCS_DIM == 3) ? TCS_BY :
                     o[1] = v1;
                   }
                 } else if constexpr (!tail) {
-                  *o = (COEFF == 0) ? done[e] * c : done[e];
+                  T v = (COEFF == 0) ? done[e] * c : done[e];
+                  if (so) v = v + so[0];
+                  *o = v;
                 }
               });
             });

@@ -238,8 +238,11 @@ __device__ __forceinline__ void traverse(const LD& ld, T (&acc)[NE]) {
 }
 
 // Write the tile back; Jacobi scales by c = fl(1/S) (cuda/generate2DStencil_cuda.py:300-315).
+// An optional source array `src` (same layout, positioned like `o`) is added after the stencil
+// value: out = stencil(in) + src.  Sweeps without a source (src == nullptr, every drop-in sweep)
+// store the reference's value unchanged.
 __device__ __forceinline__ void store(T* __restrict__ o, const T (&acc)[NE], tcs_u64 xdim,
-                                      tcs_u64 plane) {
+                                      tcs_u64 plane, const T* __restrict__ src = nullptr) {
   constexpr T c = T(1) / T(S);
 #pragma unroll
   for (int ez = 0; ez < CZ; ++ez)
@@ -248,8 +251,10 @@ __device__ __forceinline__ void store(T* __restrict__ o, const T (&acc)[NE], tcs
 #pragma unroll
       for (int ex = 0; ex < CX; ++ex) {
         const int e = ex + ey * CX + ez * CX * CY;
-        const T v = (COEFF == 0) ? acc[e] * c : acc[e];
-        o[(tcs_i64)ex + (tcs_i64)ey * (tcs_i64)xdim + (tcs_i64)ez * (tcs_i64)plane] = v;
+        const tcs_i64 off = (tcs_i64)ex + (tcs_i64)ey * (tcs_i64)xdim + (tcs_i64)ez * (tcs_i64)plane;
+        T v = (COEFF == 0) ? acc[e] * c : acc[e];
+        if (src) v = v + src[off];
+        o[off] = v;
       }
 }
 

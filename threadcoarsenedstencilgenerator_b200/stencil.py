@@ -137,6 +137,35 @@ class Stencil:
                                              _stream(stream), ctypes.byref(ms)))
         return ms.value
 
+    def update_grid_source(self, geom: Geometry, src, source, dst, launch: Launch | None = None,
+                           stream=None) -> None:
+        """One sweep dst = stencil(src) + source (asynchronous)."""
+        launch = launch or Launch()
+        _lib.check(self._lib.tcs_update_grid_source(self._h, _lib.U3(*geom.grid), geom.right_offset,
+                                                    ctypes.byref(launch.to_c()), _ptr(src), _ptr(source),
+                                                    _ptr(dst), _stream(stream)))
+
+    def residual(self, geom: Geometry, x, sx, r, stream=None, norms: bool = True):
+        """r = fl32(sx - x) on the interior; returns (max |sx - x|, ||sx - x||_2) when norms."""
+        out = (ctypes.c_double * 2)()
+        _lib.check(self._lib.tcs_residual(self._h, _lib.U3(*geom.grid), geom.right_offset, _ptr(x), _ptr(sx),
+                                          _ptr(r), out if norms else None, _stream(stream)))
+        return (out[0], out[1]) if norms else None
+
+    def accumulate(self, geom: Geometry, x, e, stream=None) -> None:
+        """x += e on the interior (x FP64, e FP32)."""
+        _lib.check(self._lib.tcs_accumulate(self._h, _lib.U3(*geom.grid), geom.right_offset, _ptr(x), _ptr(e),
+                                            _stream(stream)))
+
+    def compare(self, geom: Geometry, a, b, a_precision: str = "f64", stream=None) -> dict:
+        """Error statistics of a against the FP64 field b over the interior."""
+        out = (ctypes.c_double * 4)()
+        _lib.check(self._lib.tcs_compare(self._h, _lib.U3(*geom.grid), geom.right_offset, _ptr(a),
+                                         0 if a_precision == "f64" else 1, _ptr(b), out, _stream(stream)))
+        max_abs, l2, max_ref, l2_ref = out[0], out[1], out[2], out[3]
+        return {"max_abs": max_abs, "l2": l2, "max_ref": max_ref, "l2_ref": l2_ref,
+                "max_rel": max_abs / max_ref if max_ref else 0.0, "rms_rel": l2 / l2_ref if l2_ref else 0.0}
+
     def device_status(self, clear: bool = True) -> int:
         v = ctypes.c_uint()
         _lib.check(self._lib.tcs_device_status(self._h, ctypes.byref(v), 1 if clear else 0))
