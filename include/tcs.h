@@ -205,6 +205,23 @@ int tcs_update_grid_source(tcs_stencil* h, const unsigned grid[3], unsigned righ
 int tcs_residual(tcs_stencil* h, const unsigned grid[3], unsigned right_offset, const double* x,
                  const double* sx, float* r, double norms[2], void* stream);
 
+/* tcs_residual without any allocation.  No counterpart in the reference.
+ * For callers that cannot allocate device memory where they need the residual norm: code whose
+ * device memory is owned by another allocator (a framework's caching allocator), solver loops
+ * that cannot afford the implicit device synchronisation of cudaMalloc/cudaFree, or processes
+ * held to a fixed memory budget.  It calls no cudaMalloc, cudaFree or other allocating routine:
+ * the per-block partial sums live in a static 32 KiB device array of libtcs.so (4096 doubles),
+ * which every GPU that loads the library holds until the process exits.  `nblocks` partial
+ * blocks (0 = 2 per SM) need 2*nblocks + 2 doubles, so at most 2047 blocks; larger requests
+ * return TCS_ERR_INVALID_VALUE with the limit in the message.  The first call on a device looks
+ * up the array's device address (cudaGetSymbolAddress, with that device current), so make that
+ * first call before any stream capture.  All calls share the array and it keeps the last call's
+ * contents (nothing in it needs to start at zero); calls that overlap on the GPU race on it, so
+ * serialise them (one stream, or events).  Outputs and norms are those of tcs_residual. */
+int tcs_residual_static(tcs_stencil* h, const unsigned grid[3], unsigned right_offset,
+                        const double* x, const double* sx, float* r, double norms[2],
+                        unsigned nblocks, void* stream);
+
 /* x += e (FP64 state, FP32 correction). */
 int tcs_accumulate(tcs_stencil* h, const unsigned grid[3], unsigned right_offset, double* x,
                    const float* e, void* stream);

@@ -129,6 +129,7 @@ SIGNATURES = {
     "tcs_precompile_pipe": [_P(CSpec), _u, _u, _u, ctypes.c_char_p, _u],
     "tcs_update_grid_source": [_vp, U3, _u, _P(CLaunch), _vp, _vp, _vp, _vp],
     "tcs_residual": [_vp, U3, _u, _vp, _vp, _vp, _P(ctypes.c_double), _vp],
+    "tcs_residual_static": [_vp, U3, _u, _vp, _vp, _vp, _P(ctypes.c_double), _u, _vp],
     "tcs_accumulate": [_vp, U3, _u, _vp, _vp, _vp],
     "tcs_compare": [_vp, U3, _u, _vp, _i, _vp, _P(ctypes.c_double), _vp],
     "tcs_device_sm_count": [_P(_i)],

@@ -1305,6 +1305,38 @@ int tcs_residual(tcs_stencil* h, const unsigned grid[3], unsigned right_offset, 
   return TCS_OK;
 }
 
+int tcs_residual_static(tcs_stencil* h, const unsigned grid[3], unsigned right_offset,
+                        const double* x, const double* sx, float* r, double norms[2],
+                        unsigned nblocks, void* stream) {
+  if (!h || !x || !sx || !r) return fail(TCS_ERR_INVALID_VALUE, "NULL argument");
+  TcsFieldGeo f;
+  int rc = field_geo(h, grid, right_offset, f);
+  if (rc) return rc;
+  const unsigned nb = nblocks ? nblocks : (unsigned)field_blocks(h);
+  const unsigned long long need = 2ull * nb + 2ull;  // two partials per block + two results
+  if (need > TCS_STATIC_SCRATCH_DOUBLES)
+    return fail(TCS_ERR_INVALID_VALUE,
+                "tcs_residual_static: " + std::to_string(nb) + " blocks need " + std::to_string(need) +
+                    " doubles of scratch; the static array holds " +
+                    std::to_string(TCS_STATIC_SCRATCH_DOUBLES) + " (at most " +
+                    std::to_string((TCS_STATIC_SCRATCH_DOUBLES - 2) / 2) + " blocks)");
+  double* scratch = nullptr;
+  const int se = tcs_field_static_scratch(&scratch);
+  if (se != 0)
+    return fail(TCS_ERR_CUDA, std::string("static scratch address: ") + cudaGetErrorString((cudaError_t)se));
+  double* res = scratch + 2ull * nb;
+  const int e = tcs_field_launch_defect(x, sx, r, f, scratch, (int)nb, res, (cudaStream_t)stream);
+  if (e != 0) return fail(TCS_ERR_CUDA, std::string("defect kernel: ") + cudaGetErrorString((cudaError_t)e));
+  if (norms) {
+    double host[2];
+    TCS_RT(cudaMemcpyAsync(host, res, sizeof(host), cudaMemcpyDeviceToHost, (cudaStream_t)stream));
+    TCS_RT(cudaStreamSynchronize((cudaStream_t)stream));
+    norms[0] = host[0];
+    norms[1] = std::sqrt(host[1]);
+  }
+  return TCS_OK;
+}
+
 int tcs_accumulate(tcs_stencil* h, const unsigned grid[3], unsigned right_offset, double* x,
                    const float* e, void* stream) {
   if (!h || !x || !e) return fail(TCS_ERR_INVALID_VALUE, "NULL argument");

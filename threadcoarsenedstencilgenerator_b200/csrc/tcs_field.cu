@@ -143,3 +143,36 @@ extern "C" int tcs_field_launch_add(double* x, const float* e, TcsFieldGeo g, in
   tcs_k_add<<<nblocks, kThreads, 0, st>>>(x, e, g);
   return (int)cudaGetLastError();
 }
+
+// ---- allocation-free residual: scratch in a static device array ------------------------------
+// Some callers cannot allocate device memory at the point where they need the residual norm: a
+// framework whose caching allocator owns the device memory, a solver loop that must not pay the
+// implicit device synchronisation of cudaMalloc/cudaFree, or a process with a fixed memory
+// budget.  For them the partial sums live in this array, part of the library image: every GPU
+// that loads the library holds it until the process exits.  It is shared by all calls, keeps the
+// last call's contents, and calls that overlap on the GPU race on it.  Nothing in it has to start
+// at zero: each call writes every partial it later reads.
+static __device__ __align__(256) double tcs_static_scratch[TCS_STATIC_SCRATCH_DOUBLES];
+
+#include <mutex>
+
+// Device address of tcs_static_scratch on the current device.  In host code the array's name is
+// only a host-side stand-in, so the address is looked up with cudaGetSymbolAddress, once per
+// device, with that device current (the first call on a device does it).
+extern "C" int tcs_field_static_scratch(double** out) {
+  static std::mutex mu;
+  static double* addr[TCS_STATIC_SCRATCH_MAX_DEVICES] = {};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return (int)e;
+  if (dev < 0 || dev >= TCS_STATIC_SCRATCH_MAX_DEVICES) return (int)cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lock(mu);
+  if (!addr[dev]) {
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, tcs_static_scratch);
+    if (e != cudaSuccess) return (int)e;
+    addr[dev] = static_cast<double*>(p);
+  }
+  *out = addr[dev];
+  return 0;
+}

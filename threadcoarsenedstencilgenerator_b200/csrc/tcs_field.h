@@ -3,6 +3,11 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+// Size of the static scratch array of the allocation-free residual (doubles: 32 KiB), and the
+// number of devices whose address of it is cached.
+#define TCS_STATIC_SCRATCH_DOUBLES 4096
+#define TCS_STATIC_SCRATCH_MAX_DEVICES 64
+
 // Interior box of a grid buffer (units: grid points; xdim is the padded row pitch).
 struct TcsFieldGeo {
   uint64_t xdim, ydim;
@@ -20,6 +25,8 @@ int tcs_field_launch_defect(const double* x, const double* sx, float* r, TcsFiel
 int tcs_field_launch_compare(const void* a, int a_f32, const double* b, TcsFieldGeo g,
                              double* scratch, int nblocks, double* result4, cudaStream_t st);
 int tcs_field_launch_add(double* x, const float* e, TcsFieldGeo g, int nblocks, cudaStream_t st);
+// Device address of the static scratch array on the current device (cudaError_t value).
+int tcs_field_static_scratch(double** out);
 #ifdef __cplusplus
 }
 #endif
