@@ -433,6 +433,202 @@ def run_precision(args) -> dict | None:
     }
 
 
+def _batch_cpu(w, spec, geoms, arrs, budget_s: float, threads: int):
+    """The oracle's OpenMP loop over the batch's grids, one after another, until the budget is
+    spent (whole batch sweeps); returns (GLup/s, batch sweeps done, seconds)."""
+    import numpy as np
+
+    import oracle as O
+
+    ospec = O.make_spec(spec.dimension, spec.neighbourhood, spec.orientation, spec.coefficients, spec.range,
+                        spec.cx, spec.cy, spec.cz, spec.alignment, spec.cl_size)
+    outs = [np.array(a, copy=True) for a in arrs]
+    points = sum(g.interior_points for g in geoms)
+    t0 = time.perf_counter()
+    n = 0
+    while True:
+        for g, a, o in zip(geoms, arrs, outs):
+            O.cpu_sweep(ospec, a, o, g.right_offset, None, threads=threads)
+        n += 1
+        if time.perf_counter() - t0 > budget_s or n >= 200:
+            break
+    dt = time.perf_counter() - t0
+    return points * n / dt / 1e9, n, dt
+
+
+def run_batch(args) -> dict | None:
+    """Batched uneven grids: all grids swept by one persistent launch per sweep, the workload's
+    sweeps captured in one CUDA graph; a step is one replay of that graph.  Beside it: the same
+    sweeps as one launch per grid (plain stream launches, and captured in a graph too), and the
+    batched launches without a graph.  FP64 is the headline; FP32 is measured the same way."""
+    import numpy as np
+    import torch
+
+    import threadcoarsenedstencilgenerator_b200 as tcs
+    from threadcoarsenedstencilgenerator_b200.batch import BatchedSweeps
+    from threadcoarsenedstencilgenerator_b200.workloads import BATCH_WORKLOADS
+
+    world, rank, local = _dist()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    w = BATCH_WORKLOADS[args.workload]
+    stream = torch.cuda.current_stream()
+    ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
+
+    def timed(fn, reps):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = ev(), ev()
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    results = {}
+    line_parts = {}
+    for prec in ("f64", "f32"):
+        spec = w.spec.replace(precision=prec)
+        st = tcs.Stencil(spec)
+        geoms = w.geometries(spec)
+        arrs = w.make_inputs(geoms, np.float64 if prec == "f64" else np.float32)
+        hosts = [torch.from_numpy(a).pin_memory() for a in arrs]
+        xs = [h.to("cuda") for h in hosts]
+        ys = [x.clone() for x in xs]
+        launch = w.tuned_launch(prec)
+        bt = BatchedSweeps(st, geoms, xs, ys, launch)
+        plan = bt.plan()
+        points = sum(g.interior_points for g in geoms)
+        n = w.sweeps
+        bt.capture(n)
+        for _ in range(args.warmup):
+            bt.replay(stream)
+        torch.cuda.synchronize()
+        main = prec == "f64"
+        if main:
+            sampler = ClockSampler(local)
+            sampler.start()
+            if dist:
+                dist.barrier()
+        torch.cuda.synchronize()
+        e0, e1 = ev(), ev()
+        e0.record(stream)
+        for _ in range(args.steps):
+            bt.replay(stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        if main:
+            if dist:
+                dist.barrier()
+            clocks = sampler.stop()
+        if st.device_status() != 0:
+            raise RuntimeError("device status word set during the timed sweeps")
+        # comparisons (per batch sweep)
+        reps = max(1, min(10, args.steps // 5))
+        ms_batched_nograph = timed(lambda: bt.sweeps(n, stream), reps) / n
+        ms_separate = timed(lambda: bt.sweeps(n, stream, separate=True), reps) / n
+        bt.capture(n, separate=True)
+        ms_separate_graph = timed(lambda: bt.replay(stream), reps) / n
+        bt.capture(n)
+        per_sweep = ms / args.steps / n
+        glups = lambda t: points / (t / 1e3) / 1e9  # noqa: E731
+        results[prec] = {
+            "glups": world * glups(per_sweep), "ms_per_sweep": per_sweep,
+            "batched_graph_glups": glups(per_sweep), "batched_launches_glups": glups(ms_batched_nograph),
+            "separate_launches_glups": glups(ms_separate), "separate_launches_graph_glups": glups(ms_separate_graph),
+            "speedup_vs_separate_launches": ms_separate / per_sweep,
+            "speedup_vs_separate_launches_graph": ms_separate_graph / per_sweep,
+            "block": list(plan.block), "ctas": plan.grid_blocks[0], "loader": plan.loader, "chunk": plan.chunk,
+            "depth": plan.depth,
+        }
+        if main:
+            t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+            if dist:
+                dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms_max = float(t.item())
+            # e2e: every step uploads all grids from pinned memory, replays the graph, downloads
+            outs = [torch.empty_like(h).pin_memory() for h in hosts]
+            e2e_steps = max(1, args.e2e_steps)
+            torch.cuda.synchronize()
+            f0, f1 = ev(), ev()
+            f0.record(stream)
+            for _ in range(e2e_steps):
+                for h, x, y in zip(hosts, xs, ys):
+                    x.copy_(h, non_blocking=True)
+                    y.copy_(x)
+                res = bt.replay(stream)
+                for o, r in zip(outs, res):
+                    o.copy_(r, non_blocking=True)
+            f1.record(stream)
+            torch.cuda.synchronize()
+            te = torch.tensor([f0.elapsed_time(f1)], dtype=torch.float64, device="cuda")
+            if dist:
+                dist.all_reduce(te, op=dist.ReduceOp.MAX)
+            nbytes = sum(h.numel() * h.element_size() for h in hosts)
+            line_parts = {
+                "ms_max": ms_max, "points": points, "nbytes": nbytes, "plan": plan, "clocks": clocks,
+                "e2e": {"value": world * points * n * e2e_steps / (float(te.item()) / 1e3) / 1e9, "unit": "GLup/s",
+                        "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
+                        "job": "upload %d grids, %d batched sweeps (graph), download results" % (len(geoms), n),
+                        "steps": e2e_steps},
+                "itemsize": spec.itemsize, "geoms": geoms, "arrs": arrs, "spec": spec,
+            }
+        bt.close()
+        del xs, ys, hosts
+        torch.cuda.empty_cache()
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        import oracle as O
+
+        threads = O.max_threads()
+        v, nsw, dt = _batch_cpu(w, line_parts["spec"], line_parts["geoms"], line_parts["arrs"], 12.0, threads)
+        cpu = {"value": v, "unit": "GLup/s", "cores": threads, "kind": "port",
+               "sample": "%d sweeps of all %d grids (%.1f s, OpenMP restatement, grid after grid)" % (
+                   nsw, w.n_grids, dt)}
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return None
+    peak, peak_kind = _peaks()
+    n = w.sweeps
+    points = line_parts["points"]
+    ms_max = line_parts["ms_max"]
+    per_launch_ms = results["f64"]["ms_per_sweep"]
+    bytes_per_launch = 2 * line_parts["itemsize"] * points
+    achieved = bytes_per_launch / (per_launch_ms / 1e3) / 1e9
+    plan = line_parts["plan"]
+    return {
+        "metric": "GLup/s (FP64 batched sweeps, %s)" % w.name,
+        "value": world * points * n * args.steps / (ms_max / 1e3) / 1e9,
+        "unit": "GLup/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (numpy default_rng seed %d)" % w.seed,
+        "config": {"workload": w.name, "grids": w.n_grids, "sides": "log-uniform [%d, %d], multiples of %d" % (
+                   w.side_range[0], w.side_range[1], w.multiple), "neighbourhood": w.spec.neighbourhood,
+                   "coefficients": w.spec.coefficients, "range": w.spec.range,
+                   "coarsening": list(w.spec.coarsening), "block": list(plan.block), "ctas": plan.grid_blocks[0],
+                   "step": "one CUDA-graph replay of %d batched sweeps (one persistent launch per sweep)" % n,
+                   "parallelism": "replicas" if world > 1 else "single-gpu",
+                   "l2": "inputs larger than L2 (2 x %.2f GiB over all grids)" % (line_parts["nbytes"] / 2**30)},
+        "gpu_launches": args.steps * n,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": _traffic(w.name), "peak_source": "%s (MEASURED_PEAKS.json hbm_gbs)" % peak_kind
+                     if peak_kind == "measured" else "fallback 6.65 TB/s",
+                     "algorithmic_bytes_per_launch": bytes_per_launch},
+        "e2e": line_parts["e2e"],
+        "clocks": line_parts["clocks"],
+        "cpu_baseline": cpu,
+        "batch": results,
+    }
+
+
 def run_reference(args) -> dict | None:
     """The reference's own stencil arithmetic on the host cores (oracle OpenMP restatement)."""
     import numpy as np
@@ -443,6 +639,26 @@ def run_reference(args) -> dict | None:
     world, rank, local = _dist()
     if rank != 0:
         return None
+    from threadcoarsenedstencilgenerator_b200.workloads import BATCH_WORKLOADS
+
+    if args.workload in BATCH_WORKLOADS:
+        w = BATCH_WORKLOADS[args.workload]
+        geoms = w.geometries()
+        arrs = w.make_inputs(geoms)
+        threads = O.max_threads()
+        _batch_cpu(w, w.spec, geoms, arrs, 1.0, threads)  # warm-up
+        value, nsw, dt = _batch_cpu(w, w.spec, geoms, arrs, 20.0, threads)
+        return {
+            "metric": "GLup/s (FP64 batched sweeps, %s)" % w.name, "value": value, "unit": "GLup/s",
+            "n_gpus": world, "steps": nsw, "warmup": args.warmup, "ms_per_step": dt * 1e3 / nsw,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (numpy default_rng seed %d)" % w.seed,
+            "config": {"workload": w.name, "grids": w.n_grids}, "impl": "reference",
+            "cpu_baseline": {"value": value, "unit": "GLup/s", "cores": threads, "kind": "port",
+                             "sample": "%d sweeps of all %d grids, OpenMP restatement of the reference kernel, "
+                                       "grid after grid" % (nsw, w.n_grids)},
+            "e2e": {"value": value, "unit": "GLup/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }
     w = WORKLOADS[args.workload]
     spec = w.spec
     geom = spec.geometry(*w.grid)
@@ -472,13 +688,13 @@ def run_reference(args) -> dict | None:
 
 
 def main() -> int:
-    from threadcoarsenedstencilgenerator_b200.workloads import DEFAULT_WORKLOAD, WORKLOADS
+    from threadcoarsenedstencilgenerator_b200.workloads import BATCH_WORKLOADS, DEFAULT_WORKLOAD, WORKLOADS
 
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
-    ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS) + sorted(BATCH_WORKLOADS))
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -490,6 +706,8 @@ def main() -> int:
     args.warmup = max(3, args.warmup)
     if args.impl == "reference":
         line = run_reference(args)
+    elif args.workload in BATCH_WORKLOADS:
+        line = run_batch(args)
     elif args.precision == "mixed":
         line = run_precision(args)
     else:

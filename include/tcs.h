@@ -234,6 +234,37 @@ int tcs_compare(tcs_stencil* h, const unsigned grid[3], unsigned right_offset, c
 /* Number of SMs of the current device. */
 int tcs_device_sm_count(int* out);
 
+/* ---- Batched sweeps over many grids (no counterpart in the reference, which sweeps one grid
+ * per launch: cuda/generateLaunchUpdateGrid.py:103-147) ----
+ * A batch is a list of grids of ONE parameter set, each with its own extents and its own two
+ * buffers (a, b), swept together by ONE persistent launch of the pipelined kernel: the CTAs take
+ * equal shares of all grids' (tile, plane) work, so small grids leave no SM idle and there is no
+ * per-grid launch or tail.  Each grid's result is bit-identical to tcs_update_grid on that grid.
+ * Grids are described like tcs_update_grid's (gridSize x,y,z and rightOffset per grid, or NULL for
+ * zeros); `launch` gives the pipe block (bx, by, 1), chunk, depth and, in `segments`, an explicit
+ * CTA count (0 = every SM at full occupancy).  Buffers belong to the caller and must outlive the
+ * batch; the batch must be destroyed before its stencil handle.  tcs_batch_create allocates the
+ * two device grid tables (a->b and b->a; one tensor map per grid and direction). */
+typedef struct tcs_batch tcs_batch;
+int tcs_batch_create(tcs_stencil* h, unsigned ngrids, const unsigned* grids /* 3 per grid */,
+                     const unsigned* right_offsets, const tcs_launch* launch, void* const* a,
+                     void* const* b, tcs_batch** out);
+/* Launch shape of the batched kernel (grid_blocks[0] CTAs, seg_len work items each). */
+int tcs_batch_plan(const tcs_batch* b, tcs_plan* out);
+/* One sweep of every grid: a -> b (from_b = 0) or b -> a (from_b = 1), one launch. */
+int tcs_batch_sweep(tcs_batch* b, int from_b, void* stream);
+/* The same sweep as one single-grid pipe launch per grid (the unbatched comparison). */
+int tcs_batch_sweep_separate(tcs_batch* b, int from_b, void* stream);
+/* Capture n ping-pong sweeps starting from a (batched, or with separate != 0 one launch per grid
+ * per sweep) into a CUDA graph held by the batch, replacing any earlier one. */
+int tcs_batch_graph(tcs_batch* b, unsigned n, int separate);
+/* Launch the captured graph on `stream`. */
+int tcs_batch_graph_launch(tcs_batch* b, void* stream);
+int tcs_batch_destroy(tcs_batch* b);
+/* Instantiate the batched kernel of a launch shape into the cubin cache (NVRTC only). */
+int tcs_precompile_batch(const tcs_spec* spec, unsigned bx, unsigned by, unsigned chunk,
+                         char* cubin_path, unsigned path_cap);
+
 #ifdef __cplusplus
 }
 #endif

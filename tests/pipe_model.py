@@ -229,3 +229,36 @@ def simulate(dim, shape, R, c, block, grid, left_offset, right_offset, aligned, 
                 count += 1
     assert len(written) == count, "a point outside the interior was written"
     return count
+
+
+def batch_pieces(grids, total, per_cta):
+    """Pieces of tcs_pipe_batch: grids = [(first, n_tiles, m)] ascending by first.
+
+    Mirrors the kernel: a CTA's range [b*per, min((b+1)*per, total)) starts at the last grid
+    whose first item is <= the range start (binary search), then walks pieces, each inside one
+    tile of one grid.  Returns [(cta, grid, tile, zs, ze)]."""
+    out = []
+    ng = len(grids)
+    nctas = max(1, -(-total // per_cta))
+    for b in range(nctas):
+        w0 = b * per_cta
+        w1 = min(w0 + per_cta, total)
+        lo, hi = 0, ng
+        while hi - lo > 1:
+            mid = (lo + hi) // 2
+            if grids[mid][0] <= w0:
+                lo = mid
+            else:
+                hi = mid
+        gi = lo
+        w = w0
+        while w < w1:
+            while gi + 1 < ng and grids[gi + 1][0] <= w:
+                gi += 1
+            first, _, m = grids[gi]
+            local = w - first
+            tile, zs = divmod(local, m)
+            ze = min(m, zs + (w1 - w))
+            w += ze - zs
+            out.append((b, gi, tile, zs, ze))
+    return out

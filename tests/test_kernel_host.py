@@ -142,3 +142,34 @@ def test_pipe_addressing_model(case, es):
             cnt = pipe_model.simulate(d, sh, r, c, blk, g.grid, g.left_offset, g.right_offset, al != "None",
                                       es=es, num_sms=2, occ=2, chunk=chunk, depth=depth, nctas=nctas)
             assert cnt is None or cnt > 0
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_batch_work_split_covers_every_plane_once(seed):
+    """The batched kernel's split of the concatenated (grid, tile, plane) list over CTAs: every
+    output plane of every tile of every grid is swept exactly once, by pieces that stay inside one
+    tile of one grid (grids with no planes included)."""
+    from pipe_model import batch_pieces
+
+    rng = np.random.default_rng(seed)
+    ng = int(rng.integers(1, 40))
+    grids, first = [], 0
+    for _ in range(ng):
+        tiles = int(rng.integers(1, 9))
+        m = int(rng.integers(0, 30)) if rng.random() < 0.2 else int(rng.integers(1, 30))
+        grids.append((first, tiles, m))
+        first += tiles * m
+    total = first
+    if total == 0:
+        return
+    for nctas in (1, 2, 7, 148, 296, total, total + 5):
+        per = max(1, -(-total // nctas))
+        seen = {}
+        for b, gi, tile, zs, ze in batch_pieces(grids, total, per):
+            f, tiles, m = grids[gi]
+            assert m > 0 and 0 <= tile < tiles and 0 <= zs < ze <= m
+            for z in range(zs, ze):
+                key = (gi, tile, z)
+                assert key not in seen
+                seen[key] = b
+        assert len(seen) == total

@@ -133,6 +133,14 @@ SIGNATURES = {
     "tcs_accumulate": [_vp, U3, _u, _vp, _vp, _vp],
     "tcs_compare": [_vp, U3, _u, _vp, _i, _vp, _P(ctypes.c_double), _vp],
     "tcs_device_sm_count": [_P(_i)],
+    "tcs_batch_create": [_vp, _u, _P(_u), _P(_u), _P(CLaunch), _P(_vp), _P(_vp), _P(_vp)],
+    "tcs_batch_plan": [_vp, _P(CPlan)],
+    "tcs_batch_sweep": [_vp, _i, _vp],
+    "tcs_batch_sweep_separate": [_vp, _i, _vp],
+    "tcs_batch_graph": [_vp, _u, _i],
+    "tcs_batch_graph_launch": [_vp, _vp],
+    "tcs_batch_destroy": [_vp],
+    "tcs_precompile_batch": [_P(CSpec), _u, _u, _u, ctypes.c_char_p, _u],
 }
 _RESTYPE = {"tcs_last_error": ctypes.c_char_p}
 

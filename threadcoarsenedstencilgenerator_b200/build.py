@@ -79,6 +79,19 @@ def check_kernel_header() -> None:
         [NVCC, *ARCH, "-std=c++17", "-O3", "-lineinfo", "-fmad=false", "-I", str(CSRC), "-c",
          str(probe), "-o", str(BUILD / "tcs_kernels_check.o")]
     )
+    # the pipelined sweep and its batched form (3D Star Jacobi r2, 2x2 coarsening, block 16x4)
+    for name, extra in (("pipe", ""), ("batch", "#define TCS_BATCH 1\n")):
+        probe = BUILD / ("tcs_kernels_check_%s.cu" % name)
+        probe.write_text(
+            "#define TCS_T double\n#define TCS_DIM 3\n#define TCS_SHAPE 1\n#define TCS_ORIENT 0\n"
+            "#define TCS_COEFF 0\n#define TCS_R 2\n#define TCS_CX 2\n#define TCS_CY 2\n#define TCS_CZ 2\n"
+            "#define TCS_PIPE 1\n#define TCS_BX 16\n#define TCS_BY 4\n#define TCS_CH 5\n#define TCS_LSHIFT 0\n"
+            + extra + '#include "tcs_kernels.cuh"\n'
+        )
+        _run(
+            [NVCC, *ARCH, "-std=c++17", "-O3", "-lineinfo", "-fmad=false", "-I", str(CSRC), "-c",
+             str(probe), "-o", str(BUILD / ("tcs_kernels_check_%s.o" % name))]
+        )
 
 
 def build(force: bool = False, verbose: bool = False) -> Path:

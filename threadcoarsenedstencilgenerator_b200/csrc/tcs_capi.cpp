@@ -27,6 +27,7 @@
 #include <algorithm>
 #include <cmath>
 #include <chrono>
+#include <cstddef>
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
@@ -206,11 +207,13 @@ std::string cache_dir() {
   return d;
 }
 
-// Compile-time launch shape of a pipelined-sweep module (tcs_pipe).
+// Compile-time launch shape of a pipelined-sweep module: tcs_pipe (one grid), or tcs_pipe_batch
+// (a table of grids) when `batch` is set.
 struct PipeKey {
   unsigned bx, by, ch, lshift;
+  unsigned batch = 0;
   bool operator==(const PipeKey& o) const {
-    return bx == o.bx && by == o.by && ch == o.ch && lshift == o.lshift;
+    return bx == o.bx && by == o.by && ch == o.ch && lshift == o.lshift && batch == o.batch;
   }
 };
 
@@ -219,6 +222,7 @@ std::string instance_macros(const tcs_spec& s, const PipeKey* pk) {
   if (pk)
     m << "#define TCS_PIPE 1\n#define TCS_BX " << pk->bx << "\n#define TCS_BY " << pk->by
       << "\n#define TCS_CH " << pk->ch << "\n#define TCS_LSHIFT " << pk->lshift << "\n";
+  if (pk && pk->batch) m << "#define TCS_BATCH 1\n";
   m << "#define TCS_T " << (s.precision == TCS_F64 ? "double" : "float") << "\n"
     << "#define TCS_DIM " << s.dimension << "\n"
     << "#define TCS_SHAPE " << s.neighbourhood << "\n"
@@ -575,7 +579,8 @@ int pipe_module(tcs_stencil* h, const PipeKey& key, PipeMod** out) {
     return fail(TCS_ERR_CUDA, "cuModuleLoadData (pipe): " + cu_msg(cr));
   }
   size_t bytes = 0;
-  if ((cr = g_drv.ModuleGetFunction(&pm->f, pm->mod, "tcs_pipe")) != CUDA_SUCCESS ||
+  if ((cr = g_drv.ModuleGetFunction(&pm->f, pm->mod, key.batch ? "tcs_pipe_batch" : "tcs_pipe")) !=
+          CUDA_SUCCESS ||
       (cr = g_drv.ModuleGetGlobal(&pm->mask_ptr, &pm->mask_bytes, pm->mod, "tcs_mask")) != CUDA_SUCCESS ||
       (cr = g_drv.ModuleGetGlobal(&pm->status_ptr, &bytes, pm->mod, "tcs_status")) != CUDA_SUCCESS) {
     g_drv.ModuleUnload(pm->mod);
@@ -631,7 +636,8 @@ unsigned pipe_width(unsigned tx, unsigned R, unsigned lshift, unsigned vec, unsi
   return w;
 }
 
-int resolve_pipe(tcs_stencil* h, const TcsGeo& g, const tcs_launch* L, Resolved& out) {
+int resolve_pipe(tcs_stencil* h, const TcsGeo& g, const tcs_launch* L, Resolved& out,
+                 bool batch = false) {
   const tcs_spec& s = h->spec;
   const unsigned R = (unsigned)s.range;
   const unsigned es = (unsigned)elem_size(s);
@@ -652,7 +658,7 @@ int resolve_pipe(tcs_stencil* h, const TcsGeo& g, const tcs_launch* L, Resolved&
   if (W > 256 || rows > 256 || ch > 256)
     return fail(TCS_ERR_UNSUPPORTED, "pipe: tile exceeds the 256-element TMA box limit");
   const unsigned chunk_bytes = ch * rows * W * es;
-  PipeKey key{L->block[0], s.dimension == 3 ? L->block[1] : 1u, ch, lshift};
+  PipeKey key{L->block[0], s.dimension == 3 ? L->block[1] : 1u, ch, lshift, batch ? 1u : 0u};
   PipeMod* pm = nullptr;
   int rc = pipe_module(h, key, &pm);
   if (rc) return rc;
@@ -781,6 +787,26 @@ int resolve(tcs_stencil* h, const unsigned grid[3], unsigned right_offset, const
   return resolve_direct(h, g, L, out);
 }
 
+// Tiled tensor map of a grid buffer (rank = dimension, x innermost) with the given box.
+int encode_map(const tcs_spec& s, const void* ptr, const unsigned long long dims[3],
+               const unsigned box_in[3], CUtensorMap* map) {
+  if (reinterpret_cast<uintptr_t>(ptr) % 16 != 0)
+    return fail(TCS_ERR_INVALID_VALUE, "input buffer is not 16-byte aligned (TMA rule)");
+  const unsigned es = (unsigned)elem_size(s);
+  const cuuint32_t rank = (cuuint32_t)s.dimension;
+  cuuint64_t gdim[3] = {dims[0], dims[1], dims[2]};
+  cuuint64_t gstride[2] = {dims[0] * es, dims[0] * dims[1] * es};
+  cuuint32_t box[3] = {box_in[0], box_in[1], box_in[2]};
+  cuuint32_t estride[3] = {1, 1, 1};
+  CUresult cr = g_drv.TensorMapEncodeTiled(
+      map, s.precision == TCS_F64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
+      rank, const_cast<void*>(ptr), gdim, gstride, box, estride, CU_TENSOR_MAP_INTERLEAVE_NONE,
+      CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (cr != CUDA_SUCCESS) return fail(TCS_ERR_CUDA, "cuTensorMapEncodeTiled: " + cu_msg(cr));
+  return TCS_OK;
+}
+
 int tensor_map(tcs_stencil* h, const void* ptr, const Resolved& r, CUtensorMap** out) {
   std::lock_guard<std::mutex> lock(h->mu);
   const unsigned long long dims[3] = {r.geo.xdim, r.geo.ydim, r.geo.zdim};
@@ -791,33 +817,21 @@ int tensor_map(tcs_stencil* h, const void* ptr, const Resolved& r, CUtensorMap**
       return TCS_OK;
     }
   }
-  if (reinterpret_cast<uintptr_t>(ptr) % 16 != 0)
-    return fail(TCS_ERR_INVALID_VALUE, "input buffer is not 16-byte aligned (TMA rule)");
-  const tcs_spec& s = h->spec;
-  const unsigned es = (unsigned)elem_size(s);
   MapEntry e;
   e.ptr = ptr;
   std::memcpy(e.dims, dims, sizeof(dims));
   std::memcpy(e.box, r.box, sizeof(r.box));
-  const cuuint32_t rank = (cuuint32_t)s.dimension;
-  cuuint64_t gdim[3] = {dims[0], dims[1], dims[2]};
-  cuuint64_t gstride[2] = {dims[0] * es, dims[0] * dims[1] * es};
-  cuuint32_t box[3] = {r.box[0], r.box[1], r.box[2]};
-  cuuint32_t estride[3] = {1, 1, 1};
-  CUresult cr = g_drv.TensorMapEncodeTiled(
-      &e.map, s.precision == TCS_F64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
-      rank, const_cast<void*>(ptr), gdim, gstride, box, estride, CU_TENSOR_MAP_INTERLEAVE_NONE,
-      CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-  if (cr != CUDA_SUCCESS) return fail(TCS_ERR_CUDA, "cuTensorMapEncodeTiled: " + cu_msg(cr));
+  int rc = encode_map(h->spec, ptr, dims, r.box, &e.map);
+  if (rc) return rc;
   if (h->maps.size() > 64) h->maps.erase(h->maps.begin());
   h->maps.push_back(e);
   *out = &h->maps.back().map;
   return TCS_OK;
 }
 
+// `pre`: an already encoded tensor map of `in` for the pipe kernel (skips the map cache).
 int launch_resolved(tcs_stencil* h, const Resolved& r, const void* in, void* out, CUstream st,
-                    const void* src = nullptr) {
+                    const void* src = nullptr, const CUtensorMap* pre = nullptr) {
   if (!in || !out) return fail(TCS_ERR_INVALID_VALUE, "NULL device buffer");
   if (in == out) return fail(TCS_ERR_INVALID_VALUE, "input and output must be distinct buffers");
   if (src == out) return fail(TCS_ERR_INVALID_VALUE, "source and output must be distinct buffers");
@@ -835,7 +849,9 @@ int launch_resolved(tcs_stencil* h, const Resolved& r, const void* in, void* out
     if (pg.loader == 0 && reinterpret_cast<uintptr_t>(in) % 16 != 0) pg.loader = 1;
     alignas(64) CUtensorMap pmap;
     std::memset(&pmap, 0, sizeof(pmap));
-    if (pg.loader == 0) {
+    if (pg.loader == 0 && pre) {
+      pmap = *pre;
+    } else if (pg.loader == 0) {
       CUtensorMap* map = nullptr;
       int rc = tensor_map(h, in, r, &map);
       if (rc) return rc;
@@ -1224,8 +1240,12 @@ int tcs_precompile(const tcs_spec* spec, char* cubin_path, unsigned path_cap) {
   return TCS_OK;
 }
 
-int tcs_precompile_pipe(const tcs_spec* spec, unsigned bx, unsigned by, unsigned chunk,
-                        char* cubin_path, unsigned path_cap) {
+}  // extern "C"
+
+namespace {
+
+int precompile_pipe(const tcs_spec* spec, unsigned bx, unsigned by, unsigned chunk, bool batch,
+                    char* cubin_path, unsigned path_cap) {
   int rc = validate(spec);
   if (rc) return rc;
   tcs_spec s = *spec;
@@ -1236,7 +1256,7 @@ int tcs_precompile_pipe(const tcs_spec* spec, unsigned bx, unsigned by, unsigned
   if (bx == 0 || (bx * (unsigned)s.cx) % vec != 0)
     return fail(TCS_ERR_UNSUPPORTED, "pipe: unsupported block");
   if (chunk == 0) chunk = pipe_auto_chunk(s, bx, by);
-  PipeKey key{bx, s.dimension == 3 ? by : 1u, chunk, left_offset_of(s) % vec};
+  PipeKey key{bx, s.dimension == 3 ? by : 1u, chunk, left_offset_of(s) % vec, batch ? 1u : 0u};
   std::vector<char> cubin;
   std::string path;
   rc = instantiate(s, &key, cubin, &path);
@@ -1247,8 +1267,6 @@ int tcs_precompile_pipe(const tcs_spec* spec, unsigned bx, unsigned by, unsigned
   }
   return TCS_OK;
 }
-
-namespace {
 
 // Interior box of a buffer with the reference geometry (gridSize, rightOffset).
 int field_geo(const tcs_stencil* h, const unsigned grid[3], unsigned right_offset, TcsFieldGeo& f) {
@@ -1282,6 +1300,18 @@ int ensure_scratch(tcs_stencil* h, size_t need) {
 }
 
 }  // namespace
+
+extern "C" {
+
+int tcs_precompile_pipe(const tcs_spec* spec, unsigned bx, unsigned by, unsigned chunk,
+                        char* cubin_path, unsigned path_cap) {
+  return precompile_pipe(spec, bx, by, chunk, false, cubin_path, path_cap);
+}
+
+int tcs_precompile_batch(const tcs_spec* spec, unsigned bx, unsigned by, unsigned chunk,
+                         char* cubin_path, unsigned path_cap) {
+  return precompile_pipe(spec, bx, by, chunk, true, cubin_path, path_cap);
+}
 
 int tcs_residual(tcs_stencil* h, const unsigned grid[3], unsigned right_offset, const double* x,
                  const double* sx, float* r, double norms[2], void* stream) {
@@ -1379,6 +1409,289 @@ int tcs_device_sm_count(int* out) {
   int dev = 0;
   TCS_RT(cudaGetDevice(&dev));
   TCS_RT(cudaDeviceGetAttribute(out, cudaDevAttrMultiProcessorCount, dev));
+  return TCS_OK;
+}
+
+}  // extern "C"
+
+// =============================================================================================
+// Batched sweeps: many grids of one parameter set in one persistent launch (tcs_pipe_batch).
+
+// Host mirror of the device TcsBatchGrid (same layout: tensor map, then pointers and geometry).
+struct alignas(64) TcsBatchGrid {
+  CUtensorMap map;
+  const void* in;
+  void* out;
+  const void* src;
+  unsigned long long xdim, ydim, zdim;
+  unsigned long long first;
+  unsigned x0, x_lim, y_lim, z_lim;
+  unsigned ntx, m;
+  unsigned loader;
+  unsigned pad_;
+};
+static_assert(sizeof(TcsBatchGrid) == 256, "TcsBatchGrid layout");
+static_assert(offsetof(TcsBatchGrid, in) == 128 && offsetof(TcsBatchGrid, first) == 176 &&
+                  offsetof(TcsBatchGrid, loader) == 208,
+              "TcsBatchGrid layout");
+
+struct tcs_batch {
+  tcs_stencil* h = nullptr;
+  tcs_launch launch{};
+  unsigned n = 0;
+  std::vector<unsigned> dims;           // 3 per grid
+  std::vector<unsigned> right_offsets;  // 1 per grid
+  std::vector<void*> a, b;              // the two buffers of each grid
+  PipeMod* pm = nullptr;
+  unsigned smem = 0, nslot = 0, depth = 0, chunk = 0, width = 0, occ = 0, block[2] = {1, 1};
+  unsigned nctas = 0;
+  unsigned long long total = 0, per = 0;
+  unsigned tma_grids[2] = {0, 0};       // grids loaded by TMA in each direction
+  CUdeviceptr table[2] = {0, 0};        // grid tables: a -> b, b -> a
+  std::vector<Resolved> single;         // per-grid single-grid launches (filled on first use)
+  std::vector<CUtensorMap> maps[2];     // per-grid tensor maps of the input, per direction
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+};
+
+namespace {
+
+void batch_free(tcs_batch* b) {
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  for (CUdeviceptr t : b->table)
+    if (t) cudaFree((void*)t);
+  delete b;
+}
+
+int batch_launch(tcs_batch* b, int from_b, CUstream st) {
+  CUdeviceptr table = b->table[from_b ? 1 : 0];
+  unsigned ngrids = b->n, nslot = b->nslot;
+  unsigned long long total = b->total, per = b->per;
+  void* args[] = {&table, &ngrids, &total, &per, &nslot};
+  TCS_CU(g_drv.LaunchKernel(b->pm->f, b->nctas, 1, 1, b->block[0], b->block[1], 1, b->smem, st, args,
+                            nullptr));
+  return TCS_OK;
+}
+
+int batch_single(tcs_batch* b) {
+  if (!b->single.empty()) return TCS_OK;
+  std::vector<Resolved> rs(b->n);
+  for (unsigned i = 0; i < b->n; ++i) {
+    TcsGeo g;
+    int rc = make_geo(b->h, &b->dims[3 * i], b->right_offsets[i], g);
+    if (rc) return rc;
+    tcs_launch L = b->launch;
+    L.segments = 0;  // each grid spreads over the whole device
+    rc = resolve_pipe(b->h, g, &L, rs[i], false);
+    if (rc) return rc;
+  }
+  b->single.swap(rs);
+  return TCS_OK;
+}
+
+int batch_launch_separate(tcs_batch* b, int from_b, CUstream st) {
+  int rc = batch_single(b);
+  if (rc) return rc;
+  for (unsigned i = 0; i < b->n; ++i) {
+    const void* in = from_b ? b->b[i] : b->a[i];
+    void* out = from_b ? b->a[i] : b->b[i];
+    rc = launch_resolved(b->h, b->single[i], in, out, st, nullptr, &b->maps[from_b ? 1 : 0][i]);
+    if (rc) return rc;
+  }
+  return TCS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int tcs_batch_create(tcs_stencil* h, unsigned ngrids, const unsigned* grids,
+                     const unsigned* right_offsets, const tcs_launch* launch, void* const* a,
+                     void* const* b, tcs_batch** out) {
+  if (!h || !grids || !launch || !a || !b || !out)
+    return fail(TCS_ERR_INVALID_VALUE, "NULL argument");
+  *out = nullptr;
+  if (ngrids == 0) return fail(TCS_ERR_INVALID_VALUE, "a batch needs at least one grid");
+  if (launch->variant != TCS_VARIANT_AUTO && launch->variant != TCS_VARIANT_PIPE)
+    return fail(TCS_ERR_UNSUPPORTED, "batched sweeps run the pipe kernel only");
+  int rc = check_block(h, launch->block);
+  if (rc) return rc;
+  const tcs_spec& s = h->spec;
+  tcs_batch* B = new tcs_batch();
+  B->h = h;
+  B->launch = *launch;
+  B->launch.variant = TCS_VARIANT_PIPE;
+  B->n = ngrids;
+  B->dims.assign(grids, grids + 3 * (size_t)ngrids);
+  B->right_offsets.assign(ngrids, 0u);
+  if (right_offsets) B->right_offsets.assign(right_offsets, right_offsets + ngrids);
+  B->a.assign(a, a + ngrids);
+  B->b.assign(b, b + ngrids);
+  std::vector<TcsBatchGrid> tab[2];
+  tab[0].resize(ngrids);
+  tab[1].resize(ngrids);
+  B->maps[0].resize(ngrids);
+  B->maps[1].resize(ngrids);
+  unsigned long long first = 0;
+  for (unsigned i = 0; i < ngrids; ++i) {
+    if (!a[i] || !b[i] || a[i] == b[i]) {
+      batch_free(B);
+      return fail(TCS_ERR_INVALID_VALUE, "grid " + std::to_string(i) + ": NULL or shared buffers");
+    }
+    TcsGeo g;
+    Resolved r;
+    if ((rc = make_geo(h, &B->dims[3 * i], B->right_offsets[i], g)) ||
+        (rc = resolve_pipe(h, g, &B->launch, r, true))) {
+      batch_free(B);
+      g_err = "grid " + std::to_string(i) + ": " + g_err;
+      return rc;
+    }
+    if (i == 0) {
+      B->pm = r.pipe;
+      B->smem = r.smem;
+      B->nslot = r.pgeo.nslot;
+      B->depth = r.depth;
+      B->chunk = r.chunk;
+      B->width = r.geo.width;
+      B->occ = r.occ;
+      B->block[0] = r.block[0];
+      B->block[1] = r.block[1];
+    }
+    const TcsPipeGeo& pg = r.pgeo;
+    for (int d = 0; d < 2; ++d) {
+      TcsBatchGrid& e = tab[d][i];
+      std::memset(&e, 0, sizeof(e));
+      e.in = d ? b[i] : a[i];
+      e.out = d ? a[i] : b[i];
+      e.src = nullptr;
+      e.xdim = pg.xdim;
+      e.ydim = pg.ydim;
+      e.zdim = pg.zdim;
+      e.first = first;
+      e.x0 = pg.x0;
+      e.x_lim = pg.x_lim;
+      e.y_lim = pg.y_lim;
+      e.z_lim = pg.z_lim;
+      e.ntx = pg.ntx;
+      e.m = pg.m;
+      // TMA needs a 16-byte row pitch and base; other grids stream through cp.async.
+      e.loader = (pg.loader == 0 && reinterpret_cast<uintptr_t>(e.in) % 16 == 0) ? 0u : 1u;
+      if (e.loader == 0) {
+        const unsigned long long dims[3] = {pg.xdim, pg.ydim, pg.zdim};
+        if ((rc = encode_map(s, e.in, dims, r.box, &e.map))) {
+          batch_free(B);
+          return rc;
+        }
+        ++B->tma_grids[d];
+      }
+      B->maps[d][i] = e.map;
+    }
+    first += pg.total;
+  }
+  B->total = first;
+  unsigned long long nctas = (unsigned long long)h->num_sms * B->occ;
+  if (launch->segments) nctas = launch->segments;
+  B->per = std::max<unsigned long long>(1, (B->total + nctas - 1) / nctas);
+  const unsigned long long grid = std::max<unsigned long long>(1, (B->total + B->per - 1) / B->per);
+  if (grid > 0x7fffffffull) {
+    batch_free(B);
+    return fail(TCS_ERR_UNSUPPORTED, "batch grid too large");
+  }
+  B->nctas = (unsigned)grid;
+  for (int d = 0; d < 2; ++d) {
+    cudaError_t e = cudaMalloc((void**)&B->table[d], sizeof(TcsBatchGrid) * ngrids);
+    if (e == cudaSuccess)
+      e = cudaMemcpy((void*)B->table[d], tab[d].data(), sizeof(TcsBatchGrid) * ngrids,
+                     cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+      batch_free(B);
+      return fail(TCS_ERR_CUDA, std::string("batch table: ") + cudaGetErrorString(e));
+    }
+  }
+  *out = B;
+  return TCS_OK;
+}
+
+int tcs_batch_plan(const tcs_batch* b, tcs_plan* out) {
+  if (!b || !out) return fail(TCS_ERR_INVALID_VALUE, "NULL argument");
+  tcs_plan p{};
+  p.variant = TCS_VARIANT_PIPE;
+  p.grid_blocks[0] = b->nctas;
+  p.grid_blocks[1] = p.grid_blocks[2] = 1;
+  p.block[0] = b->block[0];
+  p.block[1] = b->block[1];
+  p.block[2] = 1;
+  p.dyn_smem = b->smem;
+  p.seg_len = (unsigned)std::min<unsigned long long>(b->per, 0xffffffffull);
+  p.nslot = b->nslot;
+  p.width = b->width;
+  p.chunk = b->chunk;
+  p.depth = b->depth;
+  p.loader = (b->tma_grids[0] == b->n) ? 0u : 1u;
+  p.ctas_per_sm = b->occ;
+  p.num_sms = b->h->num_sms;
+  *out = p;
+  return TCS_OK;
+}
+
+int tcs_batch_sweep(tcs_batch* b, int from_b, void* stream) {
+  if (!b) return fail(TCS_ERR_INVALID_VALUE, "NULL batch");
+  return batch_launch(b, from_b, (CUstream)stream);
+}
+
+int tcs_batch_sweep_separate(tcs_batch* b, int from_b, void* stream) {
+  if (!b) return fail(TCS_ERR_INVALID_VALUE, "NULL batch");
+  return batch_launch_separate(b, from_b, (CUstream)stream);
+}
+
+int tcs_batch_graph(tcs_batch* b, unsigned n, int separate) {
+  if (!b) return fail(TCS_ERR_INVALID_VALUE, "NULL batch");
+  if (n == 0) return fail(TCS_ERR_INVALID_VALUE, "a graph needs at least one sweep");
+  int rc = separate ? batch_single(b) : TCS_OK;  // module loads and uploads happen before capture
+  if (rc) return rc;
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  b->exec = nullptr;
+  b->graph = nullptr;
+  cudaStream_t cs;
+  TCS_RT(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+  cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) {
+    cudaStreamDestroy(cs);
+    return fail(TCS_ERR_CUDA, std::string("cudaStreamBeginCapture: ") + cudaGetErrorString(e));
+  }
+  for (unsigned i = 0; i < n && rc == TCS_OK; ++i)
+    rc = separate ? batch_launch_separate(b, (int)(i & 1u), (CUstream)cs)
+                  : batch_launch(b, (int)(i & 1u), (CUstream)cs);
+  cudaGraph_t graph = nullptr;
+  e = cudaStreamEndCapture(cs, &graph);
+  cudaStreamDestroy(cs);
+  if (rc) {
+    if (graph) cudaGraphDestroy(graph);
+    return rc;
+  }
+  if (e != cudaSuccess)
+    return fail(TCS_ERR_CUDA, std::string("cudaStreamEndCapture: ") + cudaGetErrorString(e));
+  e = cudaGraphInstantiate(&b->exec, graph, 0);
+  if (e != cudaSuccess) {
+    cudaGraphDestroy(graph);
+    b->exec = nullptr;
+    return fail(TCS_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+  }
+  b->graph = graph;
+  return TCS_OK;
+}
+
+int tcs_batch_graph_launch(tcs_batch* b, void* stream) {
+  if (!b) return fail(TCS_ERR_INVALID_VALUE, "NULL batch");
+  if (!b->exec) return fail(TCS_ERR_INVALID_VALUE, "no graph captured (tcs_batch_graph)");
+  TCS_RT(cudaGraphLaunch(b->exec, (cudaStream_t)stream));
+  return TCS_OK;
+}
+
+int tcs_batch_destroy(tcs_batch* b) {
+  if (b) batch_free(b);
   return TCS_OK;
 }
 

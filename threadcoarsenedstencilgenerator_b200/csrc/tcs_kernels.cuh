@@ -86,6 +86,10 @@ __device__ __forceinline__ void mbar_expect_tx(tcs_u32 bar, tcs_u32 bytes) {
                : "memory");
 }
 
+__device__ __forceinline__ void mbar_arrive(tcs_u32 bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+
 __device__ __forceinline__ bool mbar_try_wait(tcs_u32 bar, tcs_u32 parity) {
   tcs_u32 done;
   asm volatile(
@@ -457,210 +461,335 @@ struct TcsPipeGeo {
   tcs_u32 loader;              // 0 = TMA, 1 = cp.async
 };
 
+// One grid of a batched sweep: an entry of the device-resident grid table (256 bytes).
+struct __align__(64) TcsBatchGrid {
+  TcsTmaMap map;               // tensor map of `in` (unused with the cp.async loader)
+  const T* in;
+  T* out;
+  const T* src;                // optional source term (nullptr: none)
+  tcs_u64 xdim, ydim, zdim;
+  tcs_u64 first;               // index of the grid's first work item in the batch
+  tcs_u32 x0, x_lim, y_lim, z_lim;
+  tcs_u32 ntx, m;
+  tcs_u32 loader;
+  tcs_u32 pad_;
+};
+
+namespace tcs {
+
+// What the pipe body needs to know about the grid a piece belongs to.
+struct PipeGridView {
+  const TcsTmaMap* map;
+  const T* in;
+  T* out;
+  const T* src;
+  tcs_u64 xdim, ydim, zdim;
+  tcs_u32 x0, x_lim, y_lim, z_lim, ntx;
+  bool use_tma;
+  bool st_pair;  // output pairs stored with one access (even pitch, pair-aligned base)
+};
+
+// Per-CTA streaming state that survives from piece to piece.
+struct PipeState {
+  tcs_u32 bars, ring_s, nslot, tid, gc;
+  T* ring;
+};
+
+// Sweep one piece: tile `tile` of grid `G`, output planes [R + zs, R + ze) along the march axis.
+// Returns false when a bounded wait expired (the CTA must stop).  With MIXED, every barrier
+// counts all threads of the CTA, so that pieces loaded by TMA and by cp.async can share the ring:
+// for a TMA chunk thread 0 arrives with the byte count and the other threads arrive plainly.
+// Every piece consumes all chunks it issues, so the loader may change from piece to piece.
+template <bool MIXED>
+__device__ __forceinline__ bool pipe_piece(const PipeGridView& G, tcs_u32 tile, tcs_u32 zs,
+                                           tcs_u32 ze, PipeState& st, T (&acc)[NP2][NEP]) {
+  constexpr tcs_u32 NTHREADS = BX * BY;
+  constexpr tcs_u32 CHUNK_BYTES = CHUNK * (tcs_u32)sizeof(T);
+  const tcs_u32 nslot = st.nslot, tid = st.tid, bars = st.bars, gc = st.gc;
+  const bool use_tma = G.use_tma;
+  const tcs_u32 ms = R + zs;                 // first output plane of the piece
+  const tcs_u32 nout = ze - zs;              // output planes of the piece
+  const tcs_u32 np = nout + 2 * R;           // input planes streamed
+  const tcs_u32 nch = (np + CHP - 1) / CHP;  // chunks of the piece
+  const tcs_u32 X0 = G.x0 + (tile % G.ntx) * TXP;
+  const tcs_u32 xl = X0 - R - LSHIFT;        // TMA x start, a multiple of VEC
+  const tcs_u32 Y0 = (DIM == 3) ? R + (tile / G.ntx) * TYP : 0;
+
+  auto issue = [&](tcs_u32 j) {  // chunk j of the piece -> ring slot (gc + j) % nslot
+    const tcs_u32 slot = (gc + j) % nslot;
+    const tcs_u32 bar = bars + 8u * slot;
+    const tcs_u32 m0 = ms - R + j * CHP;   // first input plane of the chunk
+    if (use_tma) {
+      if (MIXED && tid != 0) {
+        mbar_arrive(bar);
+        return;
+      }
+      mbar_expect_tx(bar, CHUNK_BYTES);
+#if TCS_DIM == 2
+      tma_load_2d(st.ring_s + slot * CHUNK_BYTES, G.map, bar, (int)xl, (int)m0);
+#else
+      tma_load_3d(st.ring_s + slot * CHUNK_BYTES, G.map, bar, (int)xl, (int)(Y0 - R), (int)m0);
+#endif
+    } else {
+      const tcs_u32 dst0 = st.ring_s + slot * CHUNK_BYTES;
+      for (tcs_u32 q = tid; q < (tcs_u32)CHUNK; q += NTHREADS) {
+        const tcs_u32 xx = xl + q % PW;
+#if TCS_DIM == 2
+        const tcs_u64 yy = m0 + q / PW;
+        const bool inside = xx < G.xdim && yy < G.ydim;
+        const tcs_u64 gi = inside ? (tcs_u64)xx + yy * G.xdim : 0;
+#else
+        const tcs_u64 yy = (Y0 - R) + (q / PW) % ROWS;
+        const tcs_u64 zz = m0 + q / PLANE;
+        const bool inside = xx < G.xdim && yy < G.ydim && zz < G.zdim;
+        const tcs_u64 gi = inside ? (tcs_u64)xx + yy * G.xdim + zz * G.xdim * G.ydim : 0;
+#endif
+        cp_async_elem(dst0 + q * (tcs_u32)sizeof(T), G.in + gi, inside ? (tcs_u32)sizeof(T) : 0u);
+      }
+      cp_async_arrive(bar);
+    }
+  };
+  {
+    const tcs_u32 pro = min(nslot - 1, nch);
+    if (use_tma && !MIXED) {
+      if (tid == 0)
+        for (tcs_u32 j = 0; j < pro; ++j) issue(j);
+    } else {
+      for (tcs_u32 j = 0; j < pro; ++j) issue(j);
+    }
+  }
+
+  const tcs_u32 x = X0 + threadIdx.x * CX;
+  const tcs_u32 col0 = LSHIFT + R + threadIdx.x * CX;  // ring column of the thread's gx = 0
+#if TCS_DIM == 3
+  const tcs_u32 y = Y0 + threadIdx.y * CY;
+  const tcs_u32 lane_off = (R + threadIdx.y * CY) * PW + col0;
+  const bool lane_ok = (x + (CX - 1) < G.x_lim) && (y + (CY - 1) < G.y_lim);
+  const tcs_i64 plane_g = (tcs_i64)(G.xdim * G.ydim);
+  T* obase = G.out + (tcs_u64)x + (tcs_u64)y * G.xdim;
+#else
+  const tcs_u32 lane_off = col0;
+  const bool lane_ok = (x + (CX - 1) < G.x_lim);
+  const tcs_i64 plane_g = (tcs_i64)G.xdim;
+  T* obase = G.out + (tcs_u64)x;
+#endif
+  // One loop iteration consumes one ring chunk: wait for it (bounded), release the slot of the
+  // previous chunk to the next copy, then run its CHP planes as straight-line code.  The slot
+  // cursor advances by additions only.  Output pi - 2R is complete after input plane pi.
+  tcs_u32 cur_slot = gc % nslot;
+  tcs_u32 cur_par = (gc / nslot) & 1u;
+  T* optr = obase + ((tcs_i64)ms - 2 * R) * plane_g;
+  // A return from inside this loop costs registers across the whole body: leave it by break.
+  bool aborted = false;
+  for (tcs_u32 j = 0; j < nch; ++j) {
+    const bool expired = mbar_wait_bounded(bars + 8u * cur_slot, cur_par, TCS_WAIT_LIMIT);
+    if (__syncthreads_or(expired)) {
+      if (use_tma) {
+        if (tid == 0) {
+          atomicOr(&tcs_status, TCS_DEV_TIMEOUT);
+          const tcs_u32 hi = min(j + nslot - 2, nch - 1);
+          for (tcs_u32 jj = j; jj <= hi; ++jj)
+            (void)mbar_wait_bounded(bars + 8u * ((gc + jj) % nslot), ((gc + jj) / nslot) & 1u,
+                                    TCS_WAIT_LIMIT);
+        }
+      } else {
+        if (tid == 0) atomicOr(&tcs_status, TCS_DEV_TIMEOUT);
+        cp_async_wait_all();
+      }
+      aborted = true;
+      break;
+    }
+    if (j + nslot - 1 < nch) {
+      if (!use_tma || MIXED)
+        issue(j + nslot - 1);
+      else if (tid == 0)
+        issue(j + nslot - 1);
+    }
+    const T* pc = st.ring + cur_slot * CHUNK + lane_off;
+    const tcs_u32 pbase = j * CHP;  // input plane index (within the piece) of the chunk's first
+    static_for<0, CHP>([&](auto tt) {
+      constexpr int t = decltype(tt)::value;
+      const tcs_u32 pi = pbase + t;
+      if (pi < np) {
+        const PipeRing ld{pc + t * PLANE};
+        auto slot = [&](auto kk) -> T(&)[NEP] {
+          constexpr int k = decltype(kk)::value;
+          return acc[((t - k) % NP2 + NP2) % NP2];
+        };
+        pipe_plane(ld, slot);
+        const int op = (int)pi - 2 * R;
+        if (lane_ok && op >= 0 && op < (int)nout) {
+          constexpr T c = T(1) / T(S);
+          T(&done)[NEP] = acc[((t - 2 * R) % NP2 + NP2) % NP2];
+          T* orow = optr + (tcs_i64)t * plane_g;
+          // Output x is R + leftOff + an even offset when CX is even: pairs are aligned when
+          // R + LSHIFT is even (the shared-memory pair rule at gx = 0).
+          static_for<0, (DIM == 3) ? CY : 1>([&](auto ey) {
+            static_for<0, CX>([&](auto ex) {
+              constexpr int e = decltype(ex)::value + decltype(ey)::value * CX;
+              constexpr bool pair = pipe_pair_aligned(0) && (decltype(ex)::value % 2 == 0);
+              constexpr bool tail = pipe_pair_aligned(0) && (decltype(ex)::value % 2 == 1);
+              T* o = orow + decltype(ex)::value + decltype(ey)::value * (tcs_i64)G.xdim;
+              const T* so = G.src ? G.src + (o - G.out) : nullptr;
+              if constexpr (pair) {
+                T v0 = (COEFF == 0) ? done[e] * c : done[e];
+                T v1 = (COEFF == 0) ? done[e + 1] * c : done[e + 1];
+                if (so) {
+                  v0 = v0 + so[0];
+                  v1 = v1 + so[1];
+                }
+                if (G.st_pair) {
+                  typename PairOf<T>::type v2;
+                  v2.x = v0;
+                  v2.y = v1;
+                  *reinterpret_cast<typename PairOf<T>::type*>(o) = v2;
+                } else {
+                  o[0] = v0;
+                  o[1] = v1;
+                }
+              } else if constexpr (!tail) {
+                T v = (COEFF == 0) ? done[e] * c : done[e];
+                if (so) v = v + so[0];
+                *o = v;
+              }
+            });
+          });
+        }
+      }
+    });
+    // Re-align the register slots with the next chunk: slot m takes what slot (m + CHP) held.
+    if constexpr (CHP % NP2 != 0) {
+      T tmp[NP2][NEP];
+      static_for<0, NP2>([&](auto m) {
+        static_for<0, NEP>([&](auto e) {
+          tmp[decltype(m)::value][decltype(e)::value] = acc[decltype(m)::value][decltype(e)::value];
+        });
+      });
+      static_for<0, NP2>([&](auto m) {
+        static_for<0, NEP>([&](auto e) {
+          acc[decltype(m)::value][decltype(e)::value] =
+              tmp[(decltype(m)::value + CHP) % NP2][decltype(e)::value];
+        });
+      });
+    }
+    optr += (tcs_i64)CHP * plane_g;
+    if (++cur_slot == nslot) {
+      cur_slot = 0;
+      cur_par ^= 1u;
+    }
+  }
+  st.gc = gc + nch;
+  return !aborted;
+}
+
+// Shared-memory layout of both pipe kernels: nslot mbarriers, then the ring on a 128-byte
+// boundary.  Thread 0 initialises the barriers (arrival count 1 when only thread 0 arrives, for
+// TMA; all threads otherwise).
+__device__ __forceinline__ PipeState pipe_setup(tcs_u32 nslot, bool single_arrival) {
+  extern __shared__ __align__(128) unsigned char tcs_smem[];
+  PipeState st;
+  st.nslot = nslot;
+  st.tid = threadIdx.x + BX * threadIdx.y;
+  st.bars = smem_addr(tcs_smem);
+  const tcs_u32 bar_bytes = ((nslot * 8u + 127u) / 128u) * 128u;
+  st.ring_s = (st.bars + bar_bytes + 127u) & ~127u;
+  st.ring = reinterpret_cast<T*>(tcs_smem + (st.ring_s - st.bars));
+  st.gc = 0;
+  if (st.tid == 0) {
+    for (tcs_u32 i = 0; i < nslot; ++i) mbar_init(st.bars + 8u * i, single_arrival ? 1u : BX * BY);
+    fence_barrier_init();
+  }
+  __syncthreads();
+  return st;
+}
+
+}  // namespace tcs
+
+#ifndef TCS_BATCH
 extern "C" __global__ void __launch_bounds__(TCS_BX * ((TCS_DIM == 3) ? TCS_BY : 1))
     tcs_pipe(const __grid_constant__ TcsTmaMap tmap, const T* __restrict__ in,
              T* __restrict__ out, const T* __restrict__ src, const TcsPipeGeo g) {
   using namespace tcs;
-  extern __shared__ __align__(128) unsigned char tcs_smem[];
-  const tcs_u32 nslot = g.nslot;
-  const bool use_tma = (g.loader == 0);
-  constexpr tcs_u32 NTHREADS = BX * BY;
-  const tcs_u32 tid = threadIdx.x + BX * threadIdx.y;
-  const tcs_u32 bars = smem_addr(tcs_smem);
-  const tcs_u32 bar_bytes = ((nslot * 8u + 127u) / 128u) * 128u;
-  const tcs_u32 ring_s = (bars + bar_bytes + 127u) & ~127u;
-  T* ring = reinterpret_cast<T*>(tcs_smem + (ring_s - bars));
-  constexpr tcs_u32 CHUNK_BYTES = CHUNK * (tcs_u32)sizeof(T);
-
-  if (tid == 0) {
-    for (tcs_u32 i = 0; i < nslot; ++i) mbar_init(bars + 8u * i, use_tma ? 1u : NTHREADS);
-    fence_barrier_init();
-    if (use_tma) tma_prefetch_map(&tmap);
-  }
-  __syncthreads();
-
-  T acc[NP2][NEP];
-  tcs_u32 gc = 0;  // ring chunks consumed by this CTA so far (slot = gc % nslot)
+  PipeGridView G;
+  G.map = &tmap;
+  G.in = in;
+  G.out = out;
+  G.src = src;
+  G.xdim = g.xdim;
+  G.ydim = g.ydim;
+  G.zdim = g.zdim;
+  G.x0 = g.x0;
+  G.x_lim = g.x_lim;
+  G.y_lim = g.y_lim;
+  G.z_lim = g.z_lim;
+  G.ntx = g.ntx;
+  G.use_tma = (g.loader == 0);
   // Output pairs are stored with one access only when every row keeps the parity of the first:
   // an even row pitch and a pair-aligned base address.
-  const bool st_pair = (g.xdim % 2 == 0) &&
-                       (reinterpret_cast<tcs_u64>(out) % (2 * sizeof(T)) == 0);
+  G.st_pair = (g.xdim % 2 == 0) && (reinterpret_cast<tcs_u64>(out) % (2 * sizeof(T)) == 0);
+  if (G.use_tma && threadIdx.x == 0 && threadIdx.y == 0) tma_prefetch_map(&tmap);
+  PipeState st = pipe_setup(g.nslot, G.use_tma);
+  T acc[NP2][NEP];
   const tcs_u64 w_begin = (tcs_u64)blockIdx.x * g.per_cta;
   const tcs_u64 w_end = min(w_begin + g.per_cta, g.total);
-  tcs_u64 w = w_begin;
-  while (w < w_end) {
+  for (tcs_u64 w = w_begin; w < w_end;) {
     const tcs_u32 tile = (tcs_u32)(w / g.m);
     const tcs_u32 zs = (tcs_u32)(w % g.m);
     const tcs_u32 ze = (tcs_u32)min((tcs_u64)g.m, (tcs_u64)zs + (w_end - w));
     w += ze - zs;
-    const tcs_u32 ms = R + zs;                 // first output plane of the piece
-    const tcs_u32 nout = ze - zs;              // output planes of the piece
-    const tcs_u32 np = nout + 2 * R;           // input planes streamed
-    const tcs_u32 nch = (np + CHP - 1) / CHP;  // chunks of the piece
-    const tcs_u32 X0 = g.x0 + (tile % g.ntx) * TXP;
-    const tcs_u32 xl = X0 - R - LSHIFT;        // TMA x start, a multiple of VEC
-    const tcs_u32 Y0 = (DIM == 3) ? R + (tile / g.ntx) * TYP : 0;
-
-    auto issue = [&](tcs_u32 j) {  // chunk j of the piece -> ring slot (gc + j) % nslot
-      const tcs_u32 slot = (gc + j) % nslot;
-      const tcs_u32 bar = bars + 8u * slot;
-      const tcs_u32 m0 = ms - R + j * CHP;   // first input plane of the chunk
-      if (use_tma) {
-        mbar_expect_tx(bar, CHUNK_BYTES);
-#if TCS_DIM == 2
-        tma_load_2d(ring_s + slot * CHUNK_BYTES, &tmap, bar, (int)xl, (int)m0);
-#else
-        tma_load_3d(ring_s + slot * CHUNK_BYTES, &tmap, bar, (int)xl, (int)(Y0 - R), (int)m0);
-#endif
-      } else {
-        const tcs_u32 dst0 = ring_s + slot * CHUNK_BYTES;
-        for (tcs_u32 q = tid; q < (tcs_u32)CHUNK; q += NTHREADS) {
-          const tcs_u32 xx = xl + q % PW;
-#if TCS_DIM == 2
-          const tcs_u64 yy = m0 + q / PW;
-          const bool inside = xx < g.xdim && yy < g.ydim;
-          const tcs_u64 gi = inside ? (tcs_u64)xx + yy * g.xdim : 0;
-#else
-          const tcs_u64 yy = (Y0 - R) + (q / PW) % ROWS;
-          const tcs_u64 zz = m0 + q / PLANE;
-          const bool inside = xx < g.xdim && yy < g.ydim && zz < g.zdim;
-          const tcs_u64 gi = inside ? (tcs_u64)xx + yy * g.xdim + zz * g.xdim * g.ydim : 0;
-#endif
-          cp_async_elem(dst0 + q * (tcs_u32)sizeof(T), in + gi, inside ? (tcs_u32)sizeof(T) : 0u);
-        }
-        cp_async_arrive(bar);
-      }
-    };
-    {
-      const tcs_u32 pro = min(nslot - 1, nch);
-      if (use_tma) {
-        if (tid == 0)
-          for (tcs_u32 j = 0; j < pro; ++j) issue(j);
-      } else {
-        for (tcs_u32 j = 0; j < pro; ++j) issue(j);
-      }
-    }
-
-    const tcs_u32 x = X0 + threadIdx.x * CX;
-    const tcs_u32 col0 = LSHIFT + R + threadIdx.x * CX;  // ring column of the thread's gx = 0
-#if TCS_DIM == 3
-    const tcs_u32 y = Y0 + threadIdx.y * CY;
-    const tcs_u32 lane_off = (R + threadIdx.y * CY) * PW + col0;
-    const bool lane_ok = (x + (CX - 1) < g.x_lim) && (y + (CY - 1) < g.y_lim);
-    const tcs_i64 plane_g = (tcs_i64)(g.xdim * g.ydim);
-    T* obase = out + (tcs_u64)x + (tcs_u64)y * g.xdim;
-#else
-    const tcs_u32 lane_off = col0;
-    const bool lane_ok = (x + (CX - 1) < g.x_lim);
-    const tcs_i64 plane_g = (tcs_i64)g.xdim;
-    T* obase = out + (tcs_u64)x;
-#endif
-    // One loop iteration consumes one ring chunk: wait for it (bounded), release the slot of the
-    // previous chunk to the next copy, then run its CHP planes as straight-line code.  The slot
-    // cursor advances by additions only.  Output pi - 2R is complete after input plane pi.
-    tcs_u32 cur_slot = gc % nslot;
-    tcs_u32 cur_par = (gc / nslot) & 1u;
-    T* optr = obase + ((tcs_i64)ms - 2 * R) * plane_g;
-    bool aborted = false;
-    for (tcs_u32 j = 0; j < nch; ++j) {
-      const bool expired = mbar_wait_bounded(bars + 8u * cur_slot, cur_par, TCS_WAIT_LIMIT);
-      if (__syncthreads_or(expired)) {
-        aborted = true;
-        if (use_tma) {
-          if (tid == 0) {
-            atomicOr(&tcs_status, TCS_DEV_TIMEOUT);
-            const tcs_u32 hi = min(j + nslot - 2, nch - 1);
-            for (tcs_u32 jj = j; jj <= hi; ++jj)
-              (void)mbar_wait_bounded(bars + 8u * ((gc + jj) % nslot), ((gc + jj) / nslot) & 1u,
-                                      TCS_WAIT_LIMIT);
-          }
-        } else {
-          if (tid == 0) atomicOr(&tcs_status, TCS_DEV_TIMEOUT);
-          cp_async_wait_all();
-        }
-        break;
-      }
-      if (j + nslot - 1 < nch) {
-        if (!use_tma)
-          issue(j + nslot - 1);
-        else if (tid == 0)
-          issue(j + nslot - 1);
-      }
-      const T* pc = ring + cur_slot * CHUNK + lane_off;
-      const tcs_u32 pbase = j * CHP;  // input plane index (within the piece) of the chunk's first
-      static_for<0, CHP>([&](auto tt) {
-        constexpr int t = decltype(tt)::value;
-        const tcs_u32 pi = pbase + t;
-        if (pi < np) {
-          const PipeRing ld{pc + t * PLANE};
-          auto slot = [&](auto kk) -> T(&)[NEP] {
-            constexpr int k = decltype(kk)::value;
-            return acc[((t - k) % NP2 + NP2) % NP2];
-          };
-          pipe_plane(ld, slot);
-          const int op = (int)pi - 2 * R;
-          if (lane_ok && op >= 0 && op < (int)nout) {
-            constexpr T c = T(1) / T(S);
-            T(&done)[NEP] = acc[((t - 2 * R) % NP2 + NP2) % NP2];
-            T* orow = optr + (tcs_i64)t * plane_g;
-            // Output x is R + leftOff + an even offset when CX is even: pairs are aligned when
-            // R + LSHIFT is even (the shared-memory pair rule at gx = 0).
-            static_for<0, (DIM == 3) ? CY : 1>([&](auto ey) {
-              static_for<0, CX>([&](auto ex) {
-                constexpr int e = decltype(ex)::value + decltype(ey)::value * CX;
-                constexpr bool pair = pipe_pair_aligned(0) && (decltype(ex)::value % 2 == 0);
-                constexpr bool tail = pipe_pair_aligned(0) && (decltype(ex)::value % 2 == 1);
-                T* o = orow + decltype(ex)::value + decltype(ey)::value * (tcs_i64)g.xdim;
-                const T* so = src ? src + (o - out) : nullptr;
-                if constexpr (pair) {
-                  T v0 = (COEFF == 0) ? done[e] * c : done[e];
-                  T v1 = (COEFF == 0) ? done[e + 1] * c : done[e + 1];
-                  if (so) {
-                    v0 = v0 + so[0];
-                    v1 = v1 + so[1];
-                  }
-                  if (st_pair) {
-                    typename PairOf<T>::type v2;
-                    v2.x = v0;
-                    v2.y = v1;
-                    *reinterpret_cast<typename PairOf<T>::type*>(o) = v2;
-                  } else {
-                    o[0] = v0;
-                    o[1] = v1;
-                  }
-                } else if constexpr (!tail) {
-                  T v = (COEFF == 0) ? done[e] * c : done[e];
-                  if (so) v = v + so[0];
-                  *o = v;
-                }
-              });
-            });
-          }
-        }
-      });
-      // Re-align the register slots with the next chunk: slot m takes what slot (m + CHP) held.
-      if constexpr (CHP % NP2 != 0) {
-        T tmp[NP2][NEP];
-        static_for<0, NP2>([&](auto m) {
-          static_for<0, NEP>([&](auto e) {
-            tmp[decltype(m)::value][decltype(e)::value] = acc[decltype(m)::value][decltype(e)::value];
-          });
-        });
-        static_for<0, NP2>([&](auto m) {
-          static_for<0, NEP>([&](auto e) {
-            acc[decltype(m)::value][decltype(e)::value] =
-                tmp[(decltype(m)::value + CHP) % NP2][decltype(e)::value];
-          });
-        });
-      }
-      optr += (tcs_i64)CHP * plane_g;
-      if (++cur_slot == nslot) {
-        cur_slot = 0;
-        cur_par ^= 1u;
-      }
-    }
-    if (aborted) return;
-    gc += nch;
+    if (!pipe_piece<false>(G, tile, zs, ze, st, acc)) return;
   }
 }
+#endif  // !TCS_BATCH
+
+#ifdef TCS_BATCH
+// ---- tcs_pipe_batch: one persistent launch over many grids of the same parameter set ---------
+// The work list is the concatenation of every grid's (tile, plane) items; each CTA takes an equal
+// contiguous share and sweeps it as pieces of one grid each, reusing its ring, barriers and
+// register pipeline from piece to piece.  Grid g's items start at grids[g].first (ascending);
+// each grid has its own loader (TMA where its rows and base allow, cp.async otherwise).
+extern "C" __global__ void __launch_bounds__(TCS_BX * ((TCS_DIM == 3) ? TCS_BY : 1))
+    tcs_pipe_batch(const TcsBatchGrid* __restrict__ grids, const tcs_u32 ngrids,
+                   const tcs_u64 total, const tcs_u64 per_cta, const tcs_u32 nslot) {
+  using namespace tcs;
+  PipeState st = pipe_setup(nslot, false);
+  T acc[NP2][NEP];
+  const tcs_u64 w_begin = (tcs_u64)blockIdx.x * per_cta;
+  const tcs_u64 w_end = min(w_begin + per_cta, total);
+  tcs_u32 gi = 0;
+  {  // last grid whose first item is <= w_begin (binary search)
+    tcs_u32 lo = 0, hi = ngrids;
+    while (hi - lo > 1) {
+      const tcs_u32 mid = (lo + hi) / 2;
+      if (grids[mid].first <= w_begin) lo = mid; else hi = mid;
+    }
+    gi = lo;
+  }
+  for (tcs_u64 w = w_begin; w < w_end;) {
+    while (gi + 1 < ngrids && grids[gi + 1].first <= w) ++gi;
+    const TcsBatchGrid& B = grids[gi];
+    PipeGridView G;
+    G.map = &B.map;
+    G.in = B.in;
+    G.out = B.out;
+    G.src = B.src;
+    G.xdim = B.xdim;
+    G.ydim = B.ydim;
+    G.zdim = B.zdim;
+    G.x0 = B.x0;
+    G.x_lim = B.x_lim;
+    G.y_lim = B.y_lim;
+    G.z_lim = B.z_lim;
+    G.ntx = B.ntx;
+    G.use_tma = (B.loader == 0);
+    G.st_pair = (B.xdim % 2 == 0) && (reinterpret_cast<tcs_u64>(B.out) % (2 * sizeof(T)) == 0);
+    const tcs_u64 local = w - B.first;
+    const tcs_u32 tile = (tcs_u32)(local / B.m);
+    const tcs_u32 zs = (tcs_u32)(local % B.m);
+    const tcs_u32 ze = (tcs_u32)min((tcs_u64)B.m, (tcs_u64)zs + (w_end - w));
+    w += ze - zs;
+    if (!pipe_piece<true>(G, tile, zs, ze, st, acc)) return;
+  }
+}
+#endif  // TCS_BATCH
 #endif  // TCS_PIPE

@@ -97,3 +97,55 @@ WORKLOADS = {
 }
 
 DEFAULT_WORKLOAD = "3d_star_var_r4_512"
+
+
+@dataclass(frozen=True)
+class BatchWorkload:
+    """Many independent grids of one parameter set with seeded uneven extents."""
+
+    name: str
+    spec: StencilSpec
+    n_grids: int
+    side_range: tuple            # each side log-uniform in [lo, hi]
+    multiple: int                # sides rounded to a multiple of this (the coarsening)
+    sweeps: int
+    seed: int = 2024
+    launch: Launch = field(default_factory=lambda: Launch(block=(32, 4, 1), variant="pipe"))
+
+    def sides(self) -> list:
+        """Grid extents (nx, ny, nz) per grid, drawn per axis from default_rng(seed)."""
+        rng = np.random.default_rng(self.seed)
+        lo, hi = self.side_range
+        u = rng.uniform(np.log(lo), np.log(hi), size=(self.n_grids, 3))
+        s = np.rint(np.exp(u) / self.multiple).astype(np.int64) * self.multiple
+        s = np.clip(s, lo, hi)
+        return [tuple(int(v) for v in row) for row in s]
+
+    def geometries(self, spec: StencilSpec | None = None) -> list:
+        spec = spec or self.spec
+        return [spec.geometry(*sd) for sd in self.sides()]
+
+    def make_inputs(self, geoms, dtype=np.float64) -> list:
+        """Values uniform [0, 1) per grid (one stream of draws, grid after grid)."""
+        rng = np.random.default_rng(self.seed + 1)
+        return [rng.random(g.shape, dtype=np.float64).astype(dtype, copy=False) for g in geoms]
+
+    def tuned_launch(self, precision: str = "f64") -> Launch:
+        """Launch chosen by the autotuner for this batch (per precision), else the default."""
+        if TUNED_PATH.exists():
+            t = json.loads(TUNED_PATH.read_text()).get(self.name + ("" if precision == "f64" else "_" + precision))
+            if t:
+                return Launch(block=tuple(t["block"]), variant="pipe", segments=int(t.get("segments", 0)),
+                              depth=int(t.get("depth", 0)), chunk=int(t.get("chunk", 0)))
+        return self.launch
+
+
+BATCH_WORKLOADS = {
+    # 64 independent 3D Star Jacobi r2 grids, sides log-uniform in [64, 256] (multiples of the
+    # coarsening 2x2x2), values U[0,1), 50 sweeps per run, FP64 and FP32
+    "batch_3d_star_jacobi_r2_64": BatchWorkload(
+        name="batch_3d_star_jacobi_r2_64",
+        spec=StencilSpec(dimension=3, neighbourhood="Star", orientation="Row", coefficients="Jacobi", range=2,
+                         cx=2, cy=2, cz=2),
+        n_grids=64, side_range=(64, 256), multiple=2, sweeps=50),
+}
