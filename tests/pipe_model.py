@@ -262,3 +262,30 @@ def batch_pieces(grids, total, per_cta):
             w += ze - zs
             out.append((b, gi, tile, zs, ze))
     return out
+
+
+def copy_chunk(dim, E, pw, rows, chp, xl, y0, m0, xdim, ydim, zdim):
+    """Ring chunk filled by pipe_copy_chunk<E> (tcs_kernels.cuh): element offset -> global linear
+    index, or -1 for a zero fill.  Asserts the alignment rules of the E-element copies."""
+    out = {}
+    nseg = pw // E
+    assert pw % E == 0
+    nrow = chp * rows if dim == 3 else chp
+    for q in range(nrow * nseg):
+        row = q // nseg
+        xx = xl + (q - row * nseg) * E
+        if dim == 2:
+            yy, zz = m0 + row, 0
+            inside = xx < xdim and yy < ydim
+        else:
+            t = row // rows
+            yy, zz = y0 + row - t * rows, m0 + t
+            inside = xx < xdim and yy < ydim and zz < zdim
+        gi = xx + (yy + zz * ydim) * xdim if inside else 0
+        if inside:
+            assert gi % E == 0  # source aligned to the copy size (base aligned to it too)
+            assert xx + E - 1 < xdim
+        d = q * E
+        for k in range(E):
+            out[d + k] = gi + k if inside else -1
+    return out

@@ -182,3 +182,37 @@ def test_batch_rejects_bad_arguments(tcs):
         BatchedSweeps(st, [g], [x], [x.clone()], tcs.Launch(block=(16, 4, 1), variant="direct"))
     with pytest.raises(ValueError):
         BatchedSweeps(st, [], [], [])
+
+
+@pytest.mark.parametrize("cx, sides, offset, loader", [
+    (2, (32, 20, 18), 0, "tma"),             # 128-byte rows: TMA
+    (2, (34, 20, 18), 0, "cp.async pairs"),  # 136-byte rows: two floats per copy
+    (2, (34, 20, 18), 1, "cp.async pairs"),  # same pitch, base 4 bytes off: single floats
+    (1, (33, 20, 18), 0, "cp.async"),        # odd pitch: single floats
+])
+def test_fp32_pipe_loaders_match_oracle(tcs, cx, sides, offset, loader):
+    """Each loader of the FP32 pipe kernel (TMA, cp.async pairs, cp.async elements) gives the
+    oracle's bits; the base offset forces the element loader on an even pitch.  (The plan names
+    the loader of the pitch; the base is only known at launch.)"""
+    import torch
+
+    cfg = (3, "Star", "Row", "Jacobi", 2, cx, 2, 2, "None", 0)
+    spec = G.spec_of(cfg, "f32")
+    st = tcs.Stencil(spec)
+    geom = spec.geometry(*sides)
+    assert geom.grid[0] == sides[0]
+    launch = tcs.Launch(block=(32 // cx, 4, 1), variant="pipe")
+    assert st.plan(geom, launch).loader == loader
+    a = np.random.default_rng(3).random(geom.shape).astype(np.float32)
+    n = int(np.prod(geom.shape))
+    bx = torch.zeros(n + 1, dtype=torch.float32, device="cuda")
+    by = torch.zeros(n + 1, dtype=torch.float32, device="cuda")
+    x = bx[offset:offset + n].view(geom.shape)
+    y = by[offset:offset + n].view(geom.shape)
+    x.copy_(torch.from_numpy(a))
+    y.copy_(x)
+    res = st.sweeps(geom, x, y, 3, launch)
+    torch.cuda.synchronize()
+    assert st.device_status() == 0
+    want = O.sweeps(O.make_spec(*cfg), a, 3, geom.right_offset)
+    assert np.array_equal(res.cpu().numpy(), want)

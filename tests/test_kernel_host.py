@@ -173,3 +173,26 @@ def test_batch_work_split_covers_every_plane_once(seed):
                 assert key not in seen
                 seen[key] = b
         assert len(seen) == total
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_pair_cp_async_fill_equals_element_fill(dim):
+    """The FP32 pair loader (two elements per cp.async, even pitch) fills every ring chunk exactly
+    like the element loader: same global point (or zero fill) at every ring offset."""
+    from pipe_model import copy_chunk
+
+    rng = np.random.default_rng(dim)
+    for _ in range(40):
+        vec = 4
+        pw = int(rng.integers(2, 20)) * vec
+        rows = int(rng.integers(1, 12)) if dim == 3 else 1
+        chp = int(rng.integers(1, 6))
+        xdim = int(rng.integers(1, 60)) * 2
+        ydim = int(rng.integers(3, 40))
+        zdim = int(rng.integers(3, 30)) if dim == 3 else 1
+        xl = int(rng.integers(0, max(1, xdim // vec + 2))) * vec
+        y0 = int(rng.integers(0, ydim + 3))
+        m0 = int(rng.integers(0, (zdim if dim == 3 else ydim) + 3))
+        one = copy_chunk(dim, 1, pw, rows, chp, xl, y0, m0, xdim, ydim, zdim)
+        two = copy_chunk(dim, 2, pw, rows, chp, xl, y0, m0, xdim, ydim, zdim)
+        assert one == two

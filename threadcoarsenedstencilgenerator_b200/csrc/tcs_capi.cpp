@@ -636,6 +636,17 @@ unsigned pipe_width(unsigned tx, unsigned R, unsigned lshift, unsigned vec, unsi
   return w;
 }
 
+// Loader of the pipe kernel for a row pitch (and input base, when known): 0 = TMA (pitch and
+// base on 16 bytes), 2 = cp.async of element pairs (FP32 with an even pitch and an 8-byte base),
+// 1 = cp.async of single elements.
+unsigned pipe_loader(const tcs_spec& s, unsigned long long xdim, const void* in) {
+  const unsigned es = (unsigned)elem_size(s);
+  const uintptr_t base = reinterpret_cast<uintptr_t>(in);
+  if ((xdim * es) % 16 == 0 && base % 16 == 0) return 0u;
+  if (es == 4 && xdim % 2 == 0 && base % 8 == 0) return 2u;
+  return 1u;
+}
+
 int resolve_pipe(tcs_stencil* h, const TcsGeo& g, const tcs_launch* L, Resolved& out,
                  bool batch = false) {
   const tcs_spec& s = h->spec;
@@ -740,7 +751,7 @@ int resolve_pipe(tcs_stencil* h, const TcsGeo& g, const tcs_launch* L, Resolved&
   pg.ntx = ntx;
   pg.m = (unsigned)M;
   pg.nslot = nslot;
-  pg.loader = ((g.xdim * es) % 16 == 0) ? 0u : 1u;
+  pg.loader = pipe_loader(s, g.xdim, nullptr);
   out.geo.loader = pg.loader;
   out.geo.seg = (unsigned)std::min<unsigned long long>(per, 0xffffffffull);
   out.grid[0] = (unsigned)grid;
@@ -846,7 +857,7 @@ int launch_resolved(tcs_stencil* h, const Resolved& r, const void* in, void* out
   }
   if (r.variant == TCS_VARIANT_PIPE) {
     TcsPipeGeo pg = r.pgeo;
-    if (pg.loader == 0 && reinterpret_cast<uintptr_t>(in) % 16 != 0) pg.loader = 1;
+    pg.loader = pipe_loader(h->spec, pg.xdim, in);
     alignas(64) CUtensorMap pmap;
     std::memset(&pmap, 0, sizeof(pmap));
     if (pg.loader == 0 && pre) {
@@ -1576,7 +1587,7 @@ int tcs_batch_create(tcs_stencil* h, unsigned ngrids, const unsigned* grids,
       e.ntx = pg.ntx;
       e.m = pg.m;
       // TMA needs a 16-byte row pitch and base; other grids stream through cp.async.
-      e.loader = (pg.loader == 0 && reinterpret_cast<uintptr_t>(e.in) % 16 == 0) ? 0u : 1u;
+      e.loader = pipe_loader(s, pg.xdim, e.in);
       if (e.loader == 0) {
         const unsigned long long dims[3] = {pg.xdim, pg.ydim, pg.zdim};
         if ((rc = encode_map(s, e.in, dims, r.box, &e.map))) {

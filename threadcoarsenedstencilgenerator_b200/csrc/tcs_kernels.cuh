@@ -146,6 +146,24 @@ __device__ __forceinline__ void cp_async_elem(tcs_u32 dst, const T* src, tcs_u32
   }
 }
 
+// Copy of E consecutive elements (E * sizeof(T) = 4, 8 or 16 bytes; both addresses aligned to
+// that size); src_bytes = 0 writes zeros.
+template <int E>
+__device__ __forceinline__ void cp_async_vec(tcs_u32 dst, const T* src, tcs_u32 src_bytes) {
+  constexpr int B = E * (int)sizeof(T);
+  static_assert(B == 4 || B == 8 || B == 16, "cp.async copies 4, 8 or 16 bytes");
+  if constexpr (B == 16) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(src_bytes)
+                 : "memory");
+  } else if constexpr (B == 8) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(dst), "l"(src), "r"(src_bytes)
+                 : "memory");
+  } else {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(dst), "l"(src), "r"(src_bytes)
+                 : "memory");
+  }
+}
+
 // The mbarrier receives one arrival once all of this thread's prior cp.async copies landed.
 __device__ __forceinline__ void cp_async_arrive(tcs_u32 bar) {
   asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(bar) : "memory");
@@ -458,7 +476,7 @@ struct TcsPipeGeo {
   tcs_u32 ntx;                 // tiles along x
   tcs_u32 m;                   // output planes along the march axis
   tcs_u32 nslot;               // ring slots
-  tcs_u32 loader;              // 0 = TMA, 1 = cp.async
+  tcs_u32 loader;              // 0 = TMA, 1 = cp.async by element, 2 = cp.async by pairs
 };
 
 // One grid of a batched sweep: an entry of the device-resident grid table (256 bytes).
@@ -486,8 +504,39 @@ struct PipeGridView {
   tcs_u64 xdim, ydim, zdim;
   tcs_u32 x0, x_lim, y_lim, z_lim, ntx;
   bool use_tma;
+  bool cp_pair;  // cp.async loader moves two elements per copy (FP32, even pitch, 8-byte base)
   bool st_pair;  // output pairs stored with one access (even pitch, pair-aligned base)
 };
+
+// cp.async fill of one ring chunk: CHP planes of ROWS rows (3D) or CHP rows (2D), PW elements
+// each, starting at grid column xl, row y0 (3D) and plane / row m0.  The copies walk the chunk
+// row-major in units of E elements, so the row and plane of a copy come from divisions by
+// compile-time constants.  Points outside the tensor are filled with zeros, as TMA does.
+template <int E>
+__device__ __forceinline__ void pipe_copy_chunk(const PipeGridView& G, tcs_u32 dst0, tcs_u32 xl,
+                                                tcs_u32 y0, tcs_u32 m0, tcs_u32 tid) {
+  constexpr tcs_u32 NTHREADS = BX * BY;
+  constexpr tcs_u32 NSEG = PW / E;
+  static_assert(PW % E == 0, "ring row width is a multiple of the copy width");
+  constexpr tcs_u32 NROW = (DIM == 3) ? CHP * ROWS : CHP;
+  for (tcs_u32 q = tid; q < NROW * NSEG; q += NTHREADS) {
+    const tcs_u32 row = q / NSEG;
+    const tcs_u32 xx = xl + (q - row * NSEG) * E;
+#if TCS_DIM == 2
+    const tcs_u64 yy = m0 + row;
+    const bool inside = xx < G.xdim && yy < G.ydim;
+    const tcs_u64 gi = inside ? (tcs_u64)xx + yy * G.xdim : 0;
+#else
+    const tcs_u32 t = row / ROWS;
+    const tcs_u64 yy = y0 + (row - t * ROWS);
+    const tcs_u64 zz = m0 + t;
+    const bool inside = xx < G.xdim && yy < G.ydim && zz < G.zdim;
+    const tcs_u64 gi = inside ? (tcs_u64)xx + (yy + zz * G.ydim) * G.xdim : 0;
+#endif
+    cp_async_vec<E>(dst0 + q * (tcs_u32)(E * sizeof(T)), G.in + gi,
+                    inside ? (tcs_u32)(E * sizeof(T)) : 0u);
+  }
+}
 
 // Per-CTA streaming state that survives from piece to piece.
 struct PipeState {
@@ -532,19 +581,14 @@ __device__ __forceinline__ bool pipe_piece(const PipeGridView& G, tcs_u32 tile, 
 #endif
     } else {
       const tcs_u32 dst0 = st.ring_s + slot * CHUNK_BYTES;
-      for (tcs_u32 q = tid; q < (tcs_u32)CHUNK; q += NTHREADS) {
-        const tcs_u32 xx = xl + q % PW;
-#if TCS_DIM == 2
-        const tcs_u64 yy = m0 + q / PW;
-        const bool inside = xx < G.xdim && yy < G.ydim;
-        const tcs_u64 gi = inside ? (tcs_u64)xx + yy * G.xdim : 0;
-#else
-        const tcs_u64 yy = (Y0 - R) + (q / PW) % ROWS;
-        const tcs_u64 zz = m0 + q / PLANE;
-        const bool inside = xx < G.xdim && yy < G.ydim && zz < G.zdim;
-        const tcs_u64 gi = inside ? (tcs_u64)xx + yy * G.xdim + zz * G.xdim * G.ydim : 0;
-#endif
-        cp_async_elem(dst0 + q * (tcs_u32)sizeof(T), G.in + gi, inside ? (tcs_u32)sizeof(T) : 0u);
+      const tcs_u32 y0 = (DIM == 3) ? Y0 - R : 0;
+      if constexpr (sizeof(T) == 4) {
+        if (G.cp_pair)
+          pipe_copy_chunk<2>(G, dst0, xl, y0, m0, tid);
+        else
+          pipe_copy_chunk<1>(G, dst0, xl, y0, m0, tid);
+      } else {
+        pipe_copy_chunk<1>(G, dst0, xl, y0, m0, tid);
       }
       cp_async_arrive(bar);
     }
@@ -724,6 +768,7 @@ extern "C" __global__ void __launch_bounds__(TCS_BX * ((TCS_DIM == 3) ? TCS_BY :
   G.z_lim = g.z_lim;
   G.ntx = g.ntx;
   G.use_tma = (g.loader == 0);
+  G.cp_pair = (g.loader == 2);
   // Output pairs are stored with one access only when every row keeps the parity of the first:
   // an even row pitch and a pair-aligned base address.
   G.st_pair = (g.xdim % 2 == 0) && (reinterpret_cast<tcs_u64>(out) % (2 * sizeof(T)) == 0);
@@ -782,6 +827,7 @@ extern "C" __global__ void __launch_bounds__(TCS_BX * ((TCS_DIM == 3) ? TCS_BY :
     G.z_lim = B.z_lim;
     G.ntx = B.ntx;
     G.use_tma = (B.loader == 0);
+    G.cp_pair = (B.loader == 2);
     G.st_pair = (B.xdim % 2 == 0) && (reinterpret_cast<tcs_u64>(B.out) % (2 * sizeof(T)) == 0);
     const tcs_u64 local = w - B.first;
     const tcs_u32 tile = (tcs_u32)(local / B.m);

@@ -3,9 +3,13 @@
     python -m threadcoarsenedstencilgenerator_b200.profile_case --workload 3d_star_var_r4_512 \
         --grid 256 256 256 --sweeps 3
 
+    python -m threadcoarsenedstencilgenerator_b200.profile_case --workload batch_3d_star_jacobi_r2_64 \
+        --grids 16 --sweeps 3 --precision f32
+
 The workload's tuned launch (tuned.json) and seeded data are used.  Keep the grid above the L2
 size (126 MB per buffer) so that DRAM counters stay meaningful, and small enough for an ncu
-capture to finish in a minute or two.
+capture to finish in a minute or two.  For a batch workload, `--grids K` keeps its first K grids
+and each sweep is one batched launch.
 """
 
 from __future__ import annotations
@@ -18,14 +22,19 @@ def main(argv=None) -> int:
     import torch
 
     import threadcoarsenedstencilgenerator_b200 as tcs
-    from threadcoarsenedstencilgenerator_b200.workloads import WORKLOADS
+    from threadcoarsenedstencilgenerator_b200.workloads import BATCH_WORKLOADS, WORKLOADS
 
     ap = argparse.ArgumentParser()
-    ap.add_argument("--workload", required=True, choices=sorted(WORKLOADS))
-    ap.add_argument("--grid", type=int, nargs="+", required=True)
+    ap.add_argument("--workload", required=True, choices=sorted(WORKLOADS) + sorted(BATCH_WORKLOADS))
+    ap.add_argument("--grid", type=int, nargs="+")
+    ap.add_argument("--grids", type=int, default=0, help="batch workloads: first K grids (0 = all)")
     ap.add_argument("--sweeps", type=int, default=3)
     ap.add_argument("--precision", default="f64", choices=["f64", "f32"])
     a = ap.parse_args(argv)
+    if a.workload in BATCH_WORKLOADS:
+        return _batch(a)
+    if not a.grid:
+        ap.error("--grid is required for single-grid workloads")
     w = WORKLOADS[a.workload]
     spec = w.tuned_spec().replace(precision=a.precision)
     launch = w.tuned_launch()
@@ -46,6 +55,34 @@ def main(argv=None) -> int:
         print("device status word set", file=sys.stderr)
         return 1
     print("ok", a.workload, grid, st.plan(geom, launch))
+    return 0
+
+
+def _batch(a) -> int:
+    import numpy as np
+    import torch
+
+    import threadcoarsenedstencilgenerator_b200 as tcs
+    from threadcoarsenedstencilgenerator_b200.batch import BatchedSweeps
+    from threadcoarsenedstencilgenerator_b200.workloads import BATCH_WORKLOADS
+
+    w = BATCH_WORKLOADS[a.workload]
+    spec = w.spec.replace(precision=a.precision)
+    geoms = w.geometries(spec)
+    arrs = w.make_inputs(geoms, np.float64 if a.precision == "f64" else np.float32)
+    if a.grids:
+        geoms, arrs = geoms[:a.grids], arrs[:a.grids]
+    st = tcs.Stencil(spec)
+    xs = [torch.from_numpy(v).cuda() for v in arrs]
+    ys = [x.clone() for x in xs]
+    bt = BatchedSweeps(st, geoms, xs, ys, w.tuned_launch(a.precision))
+    bt.sweeps(a.sweeps)
+    torch.cuda.synchronize()
+    if st.device_status() != 0:
+        print("device status word set", file=sys.stderr)
+        return 1
+    print("ok", a.workload, len(geoms), "grids", sum(g.interior_points for g in geoms), "points", bt.plan())
+    bt.close()
     return 0
 
 

@@ -111,7 +111,7 @@ class Stencil:
                                              ctypes.byref(launch.to_c()), ctypes.byref(p)))
         names = {v: k for k, v in Launch._VARIANTS.items()}
         return Plan(names[p.variant], tuple(p.grid_blocks), tuple(p.block), p.dyn_smem, p.seg_len, p.nslot,
-                    p.width, p.chunk, p.depth, "tma" if p.loader == 0 else "cp.async", p.ctas_per_sm, p.num_sms)
+                    p.width, p.chunk, p.depth, {0: "tma", 2: "cp.async pairs"}.get(p.loader, "cp.async"), p.ctas_per_sm, p.num_sms)
 
     def update_grid(self, geom: Geometry, src, dst, launch: Launch | None = None, stream=None) -> None:
         """One sweep dst = stencil(src) over the interior (asynchronous)."""
