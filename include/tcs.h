@@ -265,6 +265,32 @@ int tcs_batch_destroy(tcs_batch* b);
 int tcs_precompile_batch(const tcs_spec* spec, unsigned bx, unsigned by, unsigned chunk,
                          char* cubin_path, unsigned path_cap);
 
+/* ---- Autotuner cost model (no counterpart in the reference, whose block shape is chosen by an
+ * exhaustive timed sweep: cuda/benchmark.cpp:223-251, 287-318) ----
+ * A 3-layer perceptron n_in -> H -> H -> 1 with ReLU, FP32, trained with Adam on the mean squared
+ * error, all on the GPU by this library's own kernels.  Parameters are one packed vector:
+ * W1 [n_in x H], b1 [H], W2 [H x H], b2 [H], W3 [H], b3 (row-major, input index first).
+ * Inputs x are device arrays of n rows x n_in features; targets t and outputs y have n rows.
+ * Reductions run in a fixed order: results are deterministic. */
+typedef struct tcs_mlp tcs_mlp;
+/* Allocates parameters, Adam state and activation buffers for batches of up to max_batch rows
+ * (parameters start at zero: set them). */
+int tcs_mlp_create(unsigned n_in, unsigned n_hidden, unsigned max_batch, tcs_mlp** out);
+int tcs_mlp_param_count(const tcs_mlp* m, unsigned* count);
+/* Host -> model parameters (count values); also clears the Adam moments and step. */
+int tcs_mlp_set_params(tcs_mlp* m, const float* host, unsigned count);
+int tcs_mlp_get_params(const tcs_mlp* m, float* host, unsigned count);
+/* y = model(x) for n rows (any n; processed max_batch rows at a time). */
+int tcs_mlp_forward(tcs_mlp* m, const float* x, unsigned n, float* y, void* stream);
+/* Gradient of mean((model(x) - t)^2) over n <= max_batch rows into the device vector grad (count
+ * values, may be NULL); the loss goes to *loss (host; synchronises the stream) when loss != NULL. */
+int tcs_mlp_gradient(tcs_mlp* m, const float* x, const float* t, unsigned n, float* grad, float* loss,
+                     void* stream);
+/* One Adam step (bias-corrected) on the minibatch (x, t) of n <= max_batch rows. */
+int tcs_mlp_adam_step(tcs_mlp* m, const float* x, const float* t, unsigned n, float lr, float beta1,
+                      float beta2, float eps, float* loss, void* stream);
+int tcs_mlp_destroy(tcs_mlp* m);
+
 #ifdef __cplusplus
 }
 #endif

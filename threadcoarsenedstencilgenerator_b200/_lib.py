@@ -141,6 +141,15 @@ SIGNATURES = {
     "tcs_batch_graph_launch": [_vp, _vp],
     "tcs_batch_destroy": [_vp],
     "tcs_precompile_batch": [_P(CSpec), _u, _u, _u, ctypes.c_char_p, _u],
+    "tcs_mlp_create": [_u, _u, _u, _P(_vp)],
+    "tcs_mlp_param_count": [_vp, _P(_u)],
+    "tcs_mlp_set_params": [_vp, _P(ctypes.c_float), _u],
+    "tcs_mlp_get_params": [_vp, _P(ctypes.c_float), _u],
+    "tcs_mlp_forward": [_vp, _vp, _u, _vp, _vp],
+    "tcs_mlp_gradient": [_vp, _vp, _vp, _u, _vp, _P(ctypes.c_float), _vp],
+    "tcs_mlp_adam_step": [_vp, _vp, _vp, _u, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                          _P(ctypes.c_float), _vp],
+    "tcs_mlp_destroy": [_vp],
 }
 _RESTYPE = {"tcs_last_error": ctypes.c_char_p}
 

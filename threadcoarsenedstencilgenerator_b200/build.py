@@ -27,7 +27,13 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 HOST_SOURCES = ["tcs_capi.cpp"]
-CUDA_SOURCES: list[str] = ["tcs_field.cu"]  # AOT device code compiled straight into libtcs.so
+# NVRTC is linked statically (its symbols kept private): a process that already loaded another
+# libnvrtc.so.12 (PyTorch ships one) would otherwise hand the library that NVRTC, whose version
+# changes both the generated code and the cubin cache keys.
+CUDA_LIB = Path("/usr/local/cuda/lib64")
+NVRTC_STATIC = [str(CUDA_LIB / "libnvrtc_static.a"), str(CUDA_LIB / "libnvrtc-builtins_static.a"),
+                str(CUDA_LIB / "libnvptxcompiler_static.a")]
+CUDA_SOURCES: list[str] = ["tcs_field.cu", "tcs_mlp.cu"]  # AOT device code compiled straight into libtcs.so
 
 
 def _run(cmd: list[str]) -> None:
@@ -106,7 +112,7 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     cmd = [
         NVCC, *ARCH, "-std=c++17", "-O3", "-lineinfo", "-shared", "-Xcompiler", "-fPIC",
         "-Xcompiler", "-Wall", "-cudart", "static", "-I", str(INCLUDE), "-I", str(BUILD),
-        "-I", str(CSRC), *srcs, "-o", str(LIB) + ".tmp", "-lnvrtc", "-ldl", "-lpthread", "-lrt",
+        "-I", str(CSRC), *srcs, "-o", str(LIB) + ".tmp", *NVRTC_STATIC, "-Xlinker", "--exclude-libs,ALL", "-ldl", "-lpthread", "-lrt",
         "-Xlinker", "-rpath=/usr/local/cuda/lib64",
     ]
     if verbose:

@@ -25,6 +25,7 @@
 #include <unistd.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <chrono>
 #include <cstddef>
@@ -235,13 +236,15 @@ std::string instance_macros(const tcs_spec& s, const PipeKey* pk) {
   return m.str();
 }
 
-std::mutex g_compile_mu;
+std::atomic<unsigned long long> g_tmp_counter{0};
 
+// NVRTC programs are independent, so instantiations run concurrently (the build step compiles
+// many in parallel); a finished cubin is published into the cache by an atomic rename.
 int instantiate(const tcs_spec& s, const PipeKey* pk, std::vector<char>& cubin,
                 std::string* path_out) {
   const std::string src = instance_macros(s, pk) + "#include \"tcs_kernels.cuh\"\n";
   const char* opts[] = {"--gpu-architecture=sm_100a", "--std=c++17", "--fmad=false",
-                        "-lineinfo", "--device-as-default-execution-space"};
+                        "--device-as-default-execution-space"};
   const int nopts = sizeof(opts) / sizeof(opts[0]);
   int major = 0, minor = 0;
   nvrtcVersion(&major, &minor);
@@ -253,7 +256,6 @@ int instantiate(const tcs_spec& s, const PipeKey* pk, std::vector<char>& cubin,
   const std::string path = cache_dir() + "/tcs_" + key + ".cubin";
   if (path_out) *path_out = path;
 
-  std::lock_guard<std::mutex> lock(g_compile_mu);
   {
     std::ifstream f(path, std::ios::binary);
     if (f) {
@@ -281,7 +283,8 @@ int instantiate(const tcs_spec& s, const PipeKey* pk, std::vector<char>& cubin,
   nvrtcGetCUBIN(prog, cubin.data());
   nvrtcDestroyProgram(&prog);
   // atomic publish into the cache
-  const std::string tmp = path + ".tmp." + std::to_string((long long)getpid());
+  const std::string tmp = path + ".tmp." + std::to_string((long long)getpid()) + "." +
+                          std::to_string(g_tmp_counter.fetch_add(1));
   {
     std::ofstream f(tmp, std::ios::binary);
     f.write(cubin.data(), (std::streamsize)cubin.size());
@@ -897,6 +900,8 @@ int launch_resolved(tcs_stencil* h, const Resolved& r, const void* in, void* out
 extern "C" {
 
 int tcs_abi_version(void) { return TCS_ABI_VERSION; }
+
+void tcs_internal_set_error(const char* msg) { g_err = msg ? msg : ""; }
 
 const char* tcs_last_error(void) { return g_err.c_str(); }
 

@@ -27,6 +27,8 @@ int tcs_field_launch_compare(const void* a, int a_f32, const double* b, TcsField
 int tcs_field_launch_add(double* x, const float* e, TcsFieldGeo g, int nblocks, cudaStream_t st);
 // Device address of the static scratch array on the current device (cudaError_t value).
 int tcs_field_static_scratch(double** out);
+// Set the calling thread's message returned by tcs_last_error (for the other .cu files).
+void tcs_internal_set_error(const char* msg);
 #ifdef __cplusplus
 }
 #endif
