@@ -67,9 +67,14 @@ def test_features_and_sampler():
     spec = StencilSpec(dimension=3, neighbourhood="Star", coefficients="Variable", range=2, cx=2, cy=1, cz=4)
     geom = spec.geometry(*corpus_grid(spec))
     assert geom.n_points * 8 <= (512 << 20) * 1.05
-    f = features(spec, geom, (32, 4, 2), 256)
+    from types import SimpleNamespace
+
+    plan = SimpleNamespace(grid_blocks=(8, 8, 4), ctas_per_sm=2, num_sms=148)
+    f = features(spec, geom, (32, 4, 2), 256, plan)
     assert f.shape == (len(FEATURES),) and f.dtype == np.float32
     d = dict(zip(FEATURES, f))
     assert d["dim3"] == 1 and d["star"] == 1 and d["variable"] == 1 and d["f64"] == 1
     assert d["log_tile_x"] == 6 and d["log_tile_z"] == 3 and d["log_threads"] == 8
     assert d["log_S"] == pytest.approx(math.log2(13))
+    assert d["log_warps_per_sm"] == pytest.approx(math.log2(2 * 256 / 32))
+    assert d["tail_efficiency"] == pytest.approx(256 / 296)

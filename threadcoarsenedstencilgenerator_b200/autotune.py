@@ -7,12 +7,14 @@ cuda/generateLaunchUpdateGrid.py:103-147).  Here
 * ``exhaustive`` times every candidate block of the drop-in (direct) kernel with CUDA events over a
   few sweeps of the real grid (milliseconds per candidate instead of a second);
 * ``CostModel`` is a 3-layer perceptron (128 hidden units, FP32) that predicts log GLup/s of a
-  (parameter set, grid, block) triple from one-hot and numeric features.  It is trained and
-  evaluated on the GPU by libtcs.so's own kernels (``tcs_mlp_*``);
+  (parameter set, grid, block) triple from one-hot and numeric features, relative to the mean over
+  that parameter set's candidates (the targets are centred per parameter set: ranking the blocks
+  of one set needs only the differences).  It is trained and evaluated on the GPU by libtcs.so's
+  own kernels (``tcs_mlp_*``);
 * ``Autotuner.tune`` ranks all candidates with the model, times only the top k, and falls back to
   the exhaustive sweep when the model is missing, the parameter set lies outside the corpus the
-  model was trained on, or the timed candidates disagree with the predictions by more than a
-  tolerance (the sweep then also records the model's error).
+  model was trained on, or the measured differences between the timed candidates disagree with the
+  predicted ones by more than a tolerance (the sweep then also records the model's error).
 
 ``python -m threadcoarsenedstencilgenerator_b200.autotune corpus|train|evaluate`` builds the
 timing corpus on a GPU, trains the model on it and reports its held-out quality.
@@ -48,6 +50,7 @@ FEATURES = [
     "range", "log_cx", "log_cy", "log_cz", "log_S", "log_NE", "log_terms",
     "log_bx", "log_by", "log_bz", "log_threads", "log_tile_x", "log_tile_y", "log_tile_z",
     "log_potential_block", "log_nx", "log_ny", "log_nz",
+    "log_warps_per_sm", "log_waves", "tail_efficiency", "tile_efficiency",
 ]
 
 
@@ -73,8 +76,9 @@ def candidate_blocks(dimension: int, max_threads: int = 1024) -> list:
     return out
 
 
-def features(spec: StencilSpec, geom: Geometry, block, potential_block: int) -> np.ndarray:
-    """Feature vector of one candidate (order: FEATURES)."""
+def features(spec: StencilSpec, geom: Geometry, block, potential_block: int, plan) -> np.ndarray:
+    """Feature vector of one candidate (order: FEATURES); ``plan`` is the direct launch resolved for
+    it (CTA grid and resident CTAs per SM, from the driver's occupancy calculator)."""
     d3 = spec.dimension == 3
     cz = spec.cz if d3 else 1
     bz = block[2] if d3 else 1
@@ -89,7 +93,35 @@ def features(spec: StencilSpec, geom: Geometry, block, potential_block: int) -> 
         l2(block[0]), l2(block[1]), l2(bz), l2(block[0] * block[1] * bz),
         l2(block[0] * spec.cx), l2(block[1] * spec.cy), l2(bz * cz),
         l2(potential_block), l2(geom.grid[0]), l2(geom.grid[1]), l2(geom.grid[2] if d3 else 1),
+        *_launch_features(geom, block, plan, d3),
     ], dtype=np.float32)
+
+
+def _launch_features(geom: Geometry, block, plan, d3: bool) -> list:
+    threads = block[0] * block[1] * (block[2] if d3 else 1)
+    occ = max(1, plan.ctas_per_sm)
+    ctas = plan.grid_blocks[0] * plan.grid_blocks[1] * (plan.grid_blocks[2] if d3 else 1)
+    per_wave = plan.num_sms * occ
+    waves = ctas / per_wave
+    tile = 1.0
+    for i in range(3 if d3 else 2):
+        tile *= geom.threads[i] / float(plan.grid_blocks[i] * block[i])
+    return [math.log2(occ * threads / 32.0), math.log2(max(waves, 1e-3)), ctas / (math.ceil(waves) * per_wave),
+            tile]
+
+
+def candidate_features(st: Stencil, geom: Geometry, blocks) -> tuple:
+    """(runnable blocks, their feature matrix): blocks the direct kernel cannot launch are dropped."""
+    pot = st.max_potential_block_size()
+    keep, rows = [], []
+    for b in blocks:
+        try:
+            plan = st.plan(geom, Launch(block=tuple(b), variant="direct"))
+        except _lib.TcsError:
+            continue
+        keep.append(tuple(b))
+        rows.append(features(st.spec, geom, b, pot, plan))
+    return keep, (np.stack(rows) if rows else np.zeros((0, len(FEATURES)), np.float32))
 
 
 def corpus_grid(spec: StencilSpec) -> tuple:
@@ -214,14 +246,19 @@ class CostModel:
         return loss.value if want_loss else None
 
     # standardised interface
-    def fit(self, X: np.ndarray, y: np.ndarray, epochs: int = 150, batch: int = 1024, lr: float = 2e-3,
-            seed: int = 0, log=None) -> list:
-        """Train on features X [n x n_in] and targets y = log GLup/s [n]; returns the per-epoch
-        mean training loss (standardised units)."""
+    def fit(self, X: np.ndarray, y: np.ndarray, groups: np.ndarray | None = None, epochs: int = 150,
+            batch: int = 1024, lr: float = 2e-3, seed: int = 0, log=None) -> list:
+        """Train on features X [n x n_in] and targets y = log GLup/s [n] (centred per group when
+        ``groups`` gives each row's parameter set); returns the per-epoch mean training loss
+        (standardised units)."""
         import torch
 
         X = np.asarray(X, np.float32)
-        y = np.asarray(y, np.float32)
+        y = np.asarray(y, np.float32).copy()
+        if groups is not None:
+            for gid in np.unique(groups):
+                sel = groups == gid
+                y[sel] -= y[sel].mean()
         self.x_mean = X.mean(axis=0)
         self.x_std = np.where(X.std(axis=0) > 1e-6, X.std(axis=0), 1.0).astype(np.float32)
         self.y_mean, self.y_std = float(y.mean()), float(y.std() or 1.0)
@@ -260,9 +297,11 @@ class CostModel:
         torch.cuda.synchronize()
         return out.cpu().numpy() * self.y_std + self.y_mean
 
-    def in_domain(self, X: np.ndarray, slack: float = 0.0) -> bool:
+    def in_domain(self, X: np.ndarray, slack: float = 0.1) -> bool:
+        """Every feature within the training range widened by ``slack`` of its width."""
         X = np.asarray(X, np.float32)
-        return bool(np.all(X >= self.feature_lo - slack) and np.all(X <= self.feature_hi + slack))
+        w = (self.feature_hi - self.feature_lo) * slack + 1e-3
+        return bool(np.all(X >= self.feature_lo - w) and np.all(X <= self.feature_hi + w))
 
     def save(self, path: Path = MODEL_PATH, **meta) -> None:
         path.parent.mkdir(parents=True, exist_ok=True)
@@ -302,55 +341,60 @@ class TuneResult:
     fell_back: bool                 # exhaustive sweep ran
     seconds: float                  # wall time of the tuning
     reason: str = ""
-    predicted: dict = field(default_factory=dict)  # block -> predicted GLup/s of the timed ones
+    predicted: dict = field(default_factory=dict)  # block -> predicted relative log GLup/s (timed ones)
     measured: dict = field(default_factory=dict)   # block -> measured GLup/s
+    model_error: float | None = None               # largest gap between measured and predicted differences
 
 
 class Autotuner:
     """Picks the direct kernel's block for (stencil, grid): model-ranked top-k, exhaustive fallback."""
 
-    def __init__(self, model: CostModel | None = None, top_k: int = 3, tolerance: float = 0.5,
+    def __init__(self, model: CostModel | None = None, top_k: int = 3, tolerance: float = 0.25,
                  sweeps: int = 2):
         self.model = model
         self.top_k = top_k
-        self.tolerance = tolerance  # allowed |log(measured / predicted)| of the best timed candidate
+        # allowed gap between measured and predicted log-throughput differences of the timed blocks
+        self.tolerance = tolerance
         self.sweeps = sweeps
 
     def rank(self, st: Stencil, geom: Geometry, blocks: list) -> tuple:
-        pot = st.max_potential_block_size()
-        X = np.stack([features(st.spec, geom, b, pot) for b in blocks])
-        return X, self.model.predict(X)
+        """(runnable blocks, features, predicted relative log GLup/s)."""
+        keep, X = candidate_features(st, geom, blocks)
+        return keep, X, self.model.predict(X)
 
     def tune(self, st: Stencil, geom: Geometry, x, y) -> TuneResult:
         t0 = time.perf_counter()
         blocks = candidate_blocks(st.spec.dimension)
         if self.model is None:
             return self._exhaustive(st, geom, x, y, blocks, t0, "no model")
-        X, pred = self.rank(st, geom, blocks)
-        if not self.model.in_domain(X, slack=1e-3):
-            return self._exhaustive(st, geom, x, y, blocks, t0, "parameter set outside the training corpus")
+        keep, X, pred = self.rank(st, geom, blocks)
+        if not keep:
+            raise _lib.UnsupportedLaunch(_lib.TCS_ERR_UNSUPPORTED, "no candidate block runs this parameter set")
+        if not self.model.in_domain(X):
+            return self._exhaustive(st, geom, x, y, keep, t0, "parameter set outside the training corpus")
         order = np.argsort(-pred)
         timed, measured, predicted = 0, {}, {}
         for i in order:
             if timed >= self.top_k:
                 break
-            g = time_block(st, geom, x, y, blocks[i], self.sweeps)
+            g = time_block(st, geom, x, y, keep[i], self.sweeps)
             if g is None:
                 continue
             timed += 1
-            measured[blocks[i]] = g
-            predicted[blocks[i]] = float(math.exp(pred[i]))
+            measured[keep[i]] = g
+            predicted[keep[i]] = float(pred[i])
         if not measured:
-            return self._exhaustive(st, geom, x, y, blocks, t0, "no predicted candidate runs")
+            return self._exhaustive(st, geom, x, y, keep, t0, "no predicted candidate runs")
         best = max(measured, key=measured.get)
-        err = abs(math.log(measured[best] / predicted[best]))
+        err = max(abs((predicted[b] - predicted[best]) - math.log(measured[b] / measured[best])) for b in measured)
         if err > self.tolerance:
-            r = self._exhaustive(st, geom, x, y, blocks, t0, "prediction error %.2f (log) above %.2f" % (
+            r = self._exhaustive(st, geom, x, y, keep, t0, "prediction error %.2f (log) above %.2f" % (
                 err, self.tolerance))
             r.predicted = predicted
+            r.model_error = err
             return r
-        return TuneResult(best, measured[best], timed, len(blocks), False, time.perf_counter() - t0,
-                          "model top-%d" % self.top_k, predicted, measured)
+        return TuneResult(best, measured[best], timed, len(keep), False, time.perf_counter() - t0,
+                          "model top-%d" % self.top_k, predicted, measured, err)
 
     def _exhaustive(self, st, geom, x, y, blocks, t0, reason) -> TuneResult:
         res = exhaustive(st, geom, x, y, blocks, self.sweeps)
@@ -393,13 +437,14 @@ def build_corpus(n_configs: int, seed: int, out: Path, sweeps: int = 2, log=prin
         if spec.coefficients == "Variable":
             st.copy_mask(np.random.default_rng(ci).standard_normal(spec.stencil_size) / spec.stencil_size)
         x, y = _alloc(spec, geom, ci)
-        pot = st.max_potential_block_size()
+        blocks, F = candidate_features(st, geom, candidate_blocks(spec.dimension))
+        fmap = dict(zip(blocks, F))
         t0 = time.perf_counter()
-        res = exhaustive(st, geom, x, y, candidate_blocks(spec.dimension), sweeps)
+        res = exhaustive(st, geom, x, y, blocks, sweeps)
         if st.device_status() != 0:
             raise RuntimeError("device status word set during the corpus sweep")
         for b, g in res:
-            rows.append((ci, *features(spec, geom, b, pot), math.log(g)))
+            rows.append((ci, *fmap[b], math.log(g)))
         log("config %d/%d %s: %d blocks, best %.1f GLup/s (%.1fs)" % (
             ci + 1, len(specs), _spec_str(spec), len(res), max(g for _, g in res) if res else 0.0,
             time.perf_counter() - t0))
@@ -463,6 +508,41 @@ def evaluate(model: CostModel, cfg, X, y, ids, top_k: int = 3, seed: int = 3) ->
             "timed_fraction": top_k / float(np.mean([np.sum(cfg == c) for c in ids]))}
 
 
+def live(model: CostModel, ids, n_configs: int = 400, seed: int = 7, log=print) -> dict:
+    """Tune held-out parameter sets on the GPU twice -- the learned tuner (model top-3, fallback)
+    and the exhaustive sweep -- and compare the chosen blocks re-timed with 10 sweeps each, and the
+    wall time each method spent."""
+    import torch
+
+    specs = sample_configs(n_configs, seed)
+    tuner = Autotuner(model)
+    rows = []
+    for cid in ids:
+        spec = specs[int(cid)]
+        geom = spec.geometry(*corpus_grid(spec))
+        st = Stencil(spec)
+        if spec.coefficients == "Variable":
+            st.copy_mask(np.random.default_rng(int(cid)).standard_normal(spec.stencil_size) / spec.stencil_size)
+        x, y = _alloc(spec, geom, int(cid))
+        learned = tuner.tune(st, geom, x, y)
+        full = Autotuner(None).tune(st, geom, x, y)
+        g_l = time_block(st, geom, x, y, learned.block, 10)
+        g_f = time_block(st, geom, x, y, full.block, 10)
+        rows.append({"config": int(cid), "spec": _spec_str(spec), "learned_block": list(learned.block),
+                     "exhaustive_block": list(full.block), "ratio": g_l / g_f, "learned_s": learned.seconds,
+                     "exhaustive_s": full.seconds, "fell_back": learned.fell_back, "reason": learned.reason,
+                     "timed": learned.timed, "candidates": full.timed})
+        log(json.dumps(rows[-1]))
+        st.close()
+        del x, y
+        torch.cuda.empty_cache()
+    r = np.array([q["ratio"] for q in rows])
+    return {"configs": len(rows), "mean_ratio": float(r.mean()), "min_ratio": float(r.min()),
+            "within_5pct": float(np.mean(r >= 0.95)),
+            "time_fraction": float(sum(q["learned_s"] for q in rows) / sum(q["exhaustive_s"] for q in rows)),
+            "fallbacks": int(sum(q["fell_back"] for q in rows))}
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser(prog="python -m threadcoarsenedstencilgenerator_b200.autotune")
     sub = ap.add_subparsers(dest="cmd", required=True)
@@ -480,6 +560,7 @@ def main(argv=None) -> int:
     e = sub.add_parser("evaluate", help="held-out quality of the trained model (GPU)")
     e.add_argument("--corpus", type=Path, default=CORPUS_PATH)
     e.add_argument("--model", type=Path, default=MODEL_PATH)
+    e.add_argument("--live", type=int, default=0, help="also tune this many held-out sets live on the GPU")
     a = ap.parse_args(argv)
     if a.cmd == "corpus":
         if a.precompile:
@@ -501,13 +582,16 @@ def main(argv=None) -> int:
     if a.cmd == "train":
         m = CostModel()
         t0 = time.perf_counter()
-        hist = m.fit(X[train_mask], y[train_mask], epochs=a.epochs, log=print)
+        hist = m.fit(X[train_mask], y[train_mask], groups=cfg[train_mask], epochs=a.epochs, log=print)
         dt = time.perf_counter() - t0
         m.save(a.out, epochs=a.epochs, train_seconds=dt, final_loss=hist[-1], holdout=hold)
         print(json.dumps({"train_seconds": dt, "final_loss": hist[-1], **evaluate(m, cfg, X, y, hold)}))
         return 0
     m = CostModel.load(a.model)
-    print(json.dumps(evaluate(m, cfg, X, y, hold)))
+    out = {"corpus": evaluate(m, cfg, X, y, hold)}
+    if a.live:
+        out["live"] = live(m, hold[:a.live])
+    print(json.dumps(out))
     return 0
 
 
