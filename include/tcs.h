@@ -265,6 +265,19 @@ int tcs_batch_destroy(tcs_batch* b);
 int tcs_precompile_batch(const tcs_spec* spec, unsigned bx, unsigned by, unsigned chunk,
                          char* cubin_path, unsigned path_cap);
 
+/* ---- Tensor-core sweep of 2D Box stencils on FP32 grids (no counterpart in the reference, which
+ * runs the generated kernel on the FP64 pipe: cuda/generate2DStencil_cuda.py:146-198) ----
+ * out = stencil(in) (+ src when src != NULL) over the interior, as a banded dense contraction on the
+ * tcgen05 tensor cores: inputs and mask split into BF16 high and low parts, the products hi*hi,
+ * hi*lo and lo*hi accumulated in FP32.  Each output has a relative error of a few 1e-5 of
+ * sum |mask| |in| (not the reference's bits: this is a precision option, meant for the FP32
+ * correction sweeps of FP64 defect correction).  Supported: dimension 2, Box, TCS_F32, range 1..8
+ * (any orientation, alignment and coarsening; Jacobi uses the weight 1/S).  The first call after
+ * tcs_copy_mask uploads the mask's Toeplitz operands (synchronous). */
+int tcs_tc_supported(const tcs_spec* spec);
+int tcs_tc_update_grid(tcs_stencil* h, const unsigned grid[3], unsigned right_offset, const float* in,
+                       const float* src, float* out, void* stream);
+
 /* ---- Autotuner cost model (no counterpart in the reference, whose block shape is chosen by an
  * exhaustive timed sweep: cuda/benchmark.cpp:223-251, 287-318) ----
  * A 3-layer perceptron n_in -> H -> H -> 1 with ReLU, FP32, trained with Adam on the mean squared

@@ -196,3 +196,28 @@ def test_pair_cp_async_fill_equals_element_fill(dim):
         one = copy_chunk(dim, 1, pw, rows, chp, xl, y0, m0, xdim, ydim, zdim)
         two = copy_chunk(dim, 2, pw, rows, chp, xl, y0, m0, xdim, ydim, zdim)
         assert one == two
+
+
+@pytest.mark.parametrize("R, left", [(1, 0), (3, 0), (6, 0), (8, 0), (2, 5)])
+def test_tensor_core_operand_layouts_reproduce_the_stencil(R, left):
+    """The tensor-core sweep's banded contraction, with operands laid out as tcs_tc.cu writes them
+    and read as the tcgen05 K-major no-swizzle descriptors address them, equals the stencil on a
+    tile (values exact in BF16, so hi = value and the contraction is exact in float64)."""
+    from tc_model import TM, TN, tile_product
+
+    rng = np.random.default_rng(R)
+    D = 2 * R + 1
+    mask2d = rng.integers(-4, 5, size=(D, D)).astype(np.float64)
+    ydim, xdim = TM + 2 * R + 37, left + TN + 2 * R + 45
+    grid = rng.integers(-8, 9, size=(ydim, xdim)).astype(np.float64)
+    x0 = R + left
+    for ty, tx in ((0, 0), (0, 1)):
+        acc = tile_product(grid, mask2d, R, x0, ty, tx)
+        for m in range(0, TM, 7):
+            for n in range(TN):
+                y, x = R + ty * TM + m, x0 + tx * TN + n
+                if y + R >= ydim or x + R >= xdim:
+                    continue
+                want = sum(mask2d[dy + R, dx + R] * grid[y + dy, x + dx]
+                           for dy in range(-R, R + 1) for dx in range(-R, R + 1))
+                assert acc[m, n] == want, (m, n)

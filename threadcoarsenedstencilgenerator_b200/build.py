@@ -33,7 +33,7 @@ HOST_SOURCES = ["tcs_capi.cpp"]
 CUDA_LIB = Path("/usr/local/cuda/lib64")
 NVRTC_STATIC = [str(CUDA_LIB / "libnvrtc_static.a"), str(CUDA_LIB / "libnvrtc-builtins_static.a"),
                 str(CUDA_LIB / "libnvptxcompiler_static.a")]
-CUDA_SOURCES: list[str] = ["tcs_field.cu", "tcs_mlp.cu"]  # AOT device code compiled straight into libtcs.so
+CUDA_SOURCES: list[str] = ["tcs_field.cu", "tcs_mlp.cu", "tcs_tc.cu"]  # AOT device code compiled straight into libtcs.so
 
 
 def _run(cmd: list[str]) -> None:

@@ -354,6 +354,8 @@ struct tcs_stencil {
   double* scratch = nullptr;              // per-block partials of the field reductions
   size_t scratch_len = 0;                 // in doubles
   std::vector<PipeMod*> pipes;            // pipelined-sweep modules, one per launch shape
+  void* tc_bops = nullptr;                // tensor-core Toeplitz operands (built from mask_host)
+  bool tc_stale = true;                   // mask changed since tc_bops was built
   std::mutex mu;
   std::vector<MapEntry> maps;
 };
@@ -1015,6 +1017,7 @@ int tcs_create(const tcs_spec* spec, tcs_stencil** out) {
 int tcs_destroy(tcs_stencil* h) {
   if (!h) return TCS_OK;
   if (h->scratch) cudaFree(h->scratch);
+  if (h->tc_bops) cudaFree(h->tc_bops);
   for (PipeMod* p : h->pipes) {
     if (p->mod && g_drv.ModuleUnload) g_drv.ModuleUnload(p->mod);
     delete p;
@@ -1037,6 +1040,7 @@ int tcs_copy_mask(tcs_stencil* h, const double* mask, unsigned n) {
   if (n > h->S)
     return fail(TCS_ERR_INVALID_VALUE, "mask larger than the stencil (" + std::to_string(h->S) + ")");
   std::copy(mask, mask + n, h->mask_host.begin());
+  h->tc_stale = true;
   int rc = upload_mask(h, h->mask_ptr);
   if (rc) return rc;
   for (PipeMod* p : h->pipes) {
@@ -1708,6 +1712,119 @@ int tcs_batch_graph_launch(tcs_batch* b, void* stream) {
 
 int tcs_batch_destroy(tcs_batch* b) {
   if (b) batch_free(b);
+  return TCS_OK;
+}
+
+}  // extern "C"
+
+// =============================================================================================
+// Tensor-core sweep of 2D Box stencils on FP32 grids (tcs_tc.cu).
+
+namespace {
+
+uint16_t bf16_bits(float f) {  // round to nearest even
+  uint32_t u;
+  std::memcpy(&u, &f, 4);
+  if ((u & 0x7F800000u) == 0x7F800000u && (u & 0x007FFFFFu)) return 0x7FC0u;
+  u += 0x7FFFu + ((u >> 16) & 1u);
+  return (uint16_t)(u >> 16);
+}
+
+float bf16_value(uint16_t b) {
+  uint32_t u = (uint32_t)b << 16;
+  float f;
+  std::memcpy(&f, &u, 4);
+  return f;
+}
+
+int tc_check(const tcs_spec& s) {
+  if (s.dimension != 2 || s.neighbourhood != TCS_BOX)
+    return fail(TCS_ERR_UNSUPPORTED, "tensor-core sweep: 2D Box stencils only");
+  if (s.precision != TCS_F32) return fail(TCS_ERR_UNSUPPORTED, "tensor-core sweep: FP32 grids only");
+  if (s.range < 1 || s.range > 8) return fail(TCS_ERR_UNSUPPORTED, "tensor-core sweep: range 1..8");
+  return TCS_OK;
+}
+
+// Toeplitz operands of the 2R+1 mask rows in the kernel's shared-memory layout: for row offset dy,
+// 16-byte column c and output column n, bytes dy*6144 + c*1024 + n*16 hold the BF16 high parts of
+// mask[dy][k - n] for k = 8c .. 8c+7 (zero outside 0 <= k - n <= 2R), and bytes
+// dy*6144 + c*1024 + (32 + n)*16 the low parts.  Jacobi stencils use the weight 1/S everywhere.
+int tc_build(tcs_stencil* h) {
+  if (h->tc_bops && !h->tc_stale) return TCS_OK;
+  const tcs_spec& s = h->spec;
+  const int R = s.range, D = 2 * R + 1;
+  const int TN = 32, NCH = 6;
+  std::vector<uint16_t> buf((size_t)D * NCH * 2 * TN * 8, 0);
+  const double c = 1.0 / (double)h->S;
+  for (int dy = 0; dy < D; ++dy)
+    for (int ch = 0; ch < NCH; ++ch)
+      for (int n = 0; n < TN; ++n)
+        for (int e = 0; e < 8; ++e) {
+          const int k = 8 * ch + e, j = k - n;
+          if (j < 0 || j > 2 * R) continue;
+          const double m = s.coefficients == TCS_JACOBI ? c : h->mask_host[(size_t)j + (size_t)dy * D];
+          const uint16_t hb = bf16_bits((float)m);
+          const uint16_t lb = bf16_bits((float)(m - (double)bf16_value(hb)));
+          const size_t at = (((size_t)dy * NCH + ch) * 2 * TN + n) * 8 + e;
+          buf[at] = hb;
+          buf[at + (size_t)TN * 8] = lb;
+        }
+  if (!h->tc_bops) TCS_RT(cudaMalloc(&h->tc_bops, buf.size() * sizeof(uint16_t)));
+  TCS_RT(cudaMemcpy(h->tc_bops, buf.data(), buf.size() * sizeof(uint16_t), cudaMemcpyHostToDevice));
+  h->tc_stale = false;
+  return TCS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int tcs_tc_supported(const tcs_spec* spec) {
+  int rc = validate(spec);
+  if (rc) return rc;
+  return tc_check(*spec);
+}
+
+int tcs_tc_update_grid(tcs_stencil* h, const unsigned grid[3], unsigned right_offset, const float* in,
+                       const float* src, float* out, void* stream) {
+  if (!h) return fail(TCS_ERR_INVALID_VALUE, "NULL handle");
+  int rc = tc_check(h->spec);
+  if (rc) return rc;
+  if (!in || !out) return fail(TCS_ERR_INVALID_VALUE, "NULL device buffer");
+  if ((const void*)in == (const void*)out || (const void*)src == (const void*)out)
+    return fail(TCS_ERR_INVALID_VALUE, "output must be distinct from input and source");
+  TcsGeo g;
+  if ((rc = make_geo(h, grid, right_offset, g))) return rc;
+  if ((rc = tc_build(h))) return rc;
+  const unsigned R = (unsigned)h->spec.range;
+  TcsTcGeo tg;
+  tg.xdim = g.xdim;
+  tg.ydim = g.ydim;
+  tg.x0 = g.x0;
+  tg.x_lim = g.x_lim;
+  tg.y_lim = g.y_lim;
+  tg.R = R;
+  const unsigned long long ex = g.x_lim > g.x0 ? g.x_lim - g.x0 : 0, ey = g.y_lim - R;
+  tg.ntx = std::max(1u, cdiv(ex, 32));
+  tg.nty = std::max(1u, cdiv(ey, 128));
+  if ((unsigned long long)tg.ntx * tg.nty > 0x7fffffffull) return fail(TCS_ERR_UNSUPPORTED, "grid too large");
+  // TMA staging needs a 16-byte row pitch, base and tile start (x0 - R = the left offset).
+  const bool tma = (g.xdim * 4) % 16 == 0 && reinterpret_cast<uintptr_t>(in) % 16 == 0 && (g.x0 - R) % 4 == 0;
+  alignas(64) CUtensorMap map;
+  if (tma) {
+    cuuint64_t gdim[2] = {g.xdim, g.ydim};
+    cuuint64_t gstride[1] = {g.xdim * 4};
+    cuuint32_t box[2] = {48, tcs_tc_box_rows(R)};
+    cuuint32_t estride[2] = {1, 1};
+    CUresult cr = g_drv.TensorMapEncodeTiled(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(in), gdim,
+                                             gstride, box, estride, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                                             CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                                             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (cr != CUDA_SUCCESS) return fail(TCS_ERR_CUDA, "cuTensorMapEncodeTiled: " + cu_msg(cr));
+  }
+  const int e = tcs_tc_launch(in, src, out, h->tc_bops, tma ? &map : nullptr, tg, (unsigned*)h->status_ptr,
+                              h->num_sms, (cudaStream_t)stream);
+  if (e) return fail(TCS_ERR_CUDA, std::string("tensor-core sweep: ") + cudaGetErrorString((cudaError_t)e));
   return TCS_OK;
 }
 

@@ -14,6 +14,15 @@ struct TcsFieldGeo {
   uint32_t x0, x_lim, y0, y_lim, z0, z_lim;
 };
 
+// Tile grid of the tensor-core sweep of a 2D Box stencil (tcs_tc.cu).
+struct TcsTcGeo {
+  uint64_t xdim, ydim;     // padded row pitch, rows
+  uint32_t x0, x_lim;      // interior columns [x0, x_lim)
+  uint32_t y_lim;          // interior rows [R, y_lim)
+  uint32_t ntx, nty;       // tiles of 32 columns x 128 rows
+  uint32_t R;              // range (1..8)
+};
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -27,6 +36,15 @@ int tcs_field_launch_compare(const void* a, int a_f32, const double* b, TcsField
 int tcs_field_launch_add(double* x, const float* e, TcsFieldGeo g, int nblocks, cudaStream_t st);
 // Device address of the static scratch array on the current device (cudaError_t value).
 int tcs_field_static_scratch(double** out);
+// Tensor-core sweep: dynamic shared memory of a launch for range R, and the launch itself
+// (`bops`: the Toeplitz operands built by the host, BF16 high parts of all 2R+1 rows then low
+// parts; `nctas` persistent CTAs).  Returns a cudaError_t value.
+// `map`: a 2D tensor map of `in` (FP32, box 48 x tcs_tc_box_rows(R)) for the TMA-fed form, or
+// NULL for direct loads.
+unsigned tcs_tc_smem_bytes(unsigned R);
+unsigned tcs_tc_box_rows(unsigned R);
+int tcs_tc_launch(const float* in, const float* src, float* out, const void* bops, const void* map, TcsTcGeo g,
+                  unsigned* status, int nctas, cudaStream_t st);
 // Set the calling thread's message returned by tcs_last_error (for the other .cu files).
 void tcs_internal_set_error(const char* msg);
 #ifdef __cplusplus

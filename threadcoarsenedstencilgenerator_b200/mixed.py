@@ -10,7 +10,9 @@ of the fixed border.  Every ``period`` sweeps the engine
 In exact arithmetic e after k steps equals sum_{i<k} A^i r, so x + e is exactly the FP64 state k
 sweeps later; rounding enters only through the FP32 correction, whose size is the change of the
 state over the period, so the result tracks the FP64 iteration to far better than FP32 precision
-once the iteration settles.  The FP32 sweeps are the engine's ordinary single-precision kernels.
+once the iteration settles.  The FP32 sweeps are the engine's ordinary single-precision kernels,
+or, with ``tensor_cores=True`` (2D Box stencils), the tcgen05 banded contraction with BF16 high and
+low parts and FP32 accumulation (``tcs_tc_update_grid``).
 """
 
 from __future__ import annotations
@@ -33,7 +35,7 @@ class DefectCorrectedSweeps:
     """Run n sweeps of ``spec`` (FP64 semantics) as FP32 sweeps with periodic FP64 defect correction."""
 
     def __init__(self, spec: StencilSpec, launch64: Launch | None = None, launch32: Launch | None = None,
-                 mask=None):
+                 mask=None, tensor_cores: bool = False):
         if spec.precision != "f64":
             spec = spec.replace(precision="f64")
         self.spec64 = spec
@@ -45,6 +47,7 @@ class DefectCorrectedSweeps:
             self.s32.copy_mask(mask)
         self.launch64 = launch64 or Launch()
         self.launch32 = launch32 or self.launch64
+        self.tensor_cores = tensor_cores
 
     def run(self, geom: Geometry, x, n: int, period: int = 20, stream=None, work=None) -> tuple:
         """Advance the FP64 state ``x`` (torch float64 tensor of geom.shape) by n sweeps in place.
@@ -71,7 +74,10 @@ class DefectCorrectedSweeps:
             e1.zero_()
             a, b = e0, e1
             for _ in range(k):
-                self.s32.update_grid_source(geom, a, r, b, self.launch32, stream)
+                if self.tensor_cores:
+                    self.s32.tc_update_grid(geom, a, b, source=r, stream=stream)
+                else:
+                    self.s32.update_grid_source(geom, a, r, b, self.launch32, stream)
                 a, b = b, a
             res.fp32_sweeps += k
             self.s64.accumulate(geom, x, a, stream)

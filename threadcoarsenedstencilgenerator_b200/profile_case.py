@@ -5,6 +5,8 @@
 
     python -m threadcoarsenedstencilgenerator_b200.profile_case --workload batch_3d_star_jacobi_r2_64 \
         --grids 16 --sweeps 3 --precision f32
+    python -m threadcoarsenedstencilgenerator_b200.profile_case --workload 2d_box_var_r6_16384x8192 \
+        --grid 16384 8192 --sweeps 3 --precision f32 --tensor-cores
 
 The workload's tuned launch (tuned.json) and seeded data are used.  Keep the grid above the L2
 size (126 MB per buffer) so that DRAM counters stay meaningful, and small enough for an ncu
@@ -30,6 +32,7 @@ def main(argv=None) -> int:
     ap.add_argument("--grids", type=int, default=0, help="batch workloads: first K grids (0 = all)")
     ap.add_argument("--sweeps", type=int, default=3)
     ap.add_argument("--precision", default="f64", choices=["f64", "f32"])
+    ap.add_argument("--tensor-cores", action="store_true", help="2D Box FP32: the tcgen05 sweep")
     a = ap.parse_args(argv)
     if a.workload in BATCH_WORKLOADS:
         return _batch(a)
@@ -48,7 +51,10 @@ def main(argv=None) -> int:
     x = torch.from_numpy(w.make_input(geom)).to("cuda", dtype=dt)
     y = x.clone()
     for _ in range(a.sweeps):
-        st.update_grid(geom, x, y, launch)
+        if a.tensor_cores:
+            st.tc_update_grid(geom, x, y)
+        else:
+            st.update_grid(geom, x, y, launch)
         x, y = y, x
     torch.cuda.synchronize()
     if st.device_status() != 0:

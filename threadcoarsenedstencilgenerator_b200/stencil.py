@@ -145,6 +145,13 @@ class Stencil:
                                                     ctypes.byref(launch.to_c()), _ptr(src), _ptr(source),
                                                     _ptr(dst), _stream(stream)))
 
+    def tc_update_grid(self, geom: Geometry, src, dst, source=None, stream=None) -> None:
+        """One FP32 sweep dst = stencil(src) (+ source) on the tensor cores (2D Box only; BF16
+        hi/lo split, FP32 accumulation: a precision option, not the reference's bits)."""
+        _lib.check(self._lib.tcs_tc_update_grid(self._h, _lib.U3(*geom.grid), geom.right_offset, _ptr(src),
+                                                None if source is None else _ptr(source), _ptr(dst),
+                                                _stream(stream)))
+
     def residual(self, geom: Geometry, x, sx, r, stream=None, norms: bool = True):
         """r = fl32(sx - x) on the interior; returns (max |sx - x|, ||sx - x||_2) when norms."""
         out = (ctypes.c_double * 2)()
