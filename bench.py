@@ -399,6 +399,25 @@ def run_precision(args) -> dict | None:
     t32 = e0.elapsed_time(e1)
     s32 = dc.s64.compare(geom, r32, ref, "f32")
     del x32, y32
+    # FP32 with compensated (two-sum) accumulation: direct or march kernel (block of the tuned launch)
+    s32c = tcs.Stencil(spec.replace(precision="f32c"))
+    if mask is not None:
+        s32c.copy_mask(mask)
+    lc = tcs.Launch(block=(128, 1, 1) if spec.dimension == 2 else (32, 4, 1), variant="auto")
+    x32 = torch.from_numpy(a.astype(np.float32)).cuda()
+    y32 = x32.clone()
+    s32c.sweeps(geom, x32, y32, 3, lc)
+    x32.copy_(torch.from_numpy(a.astype(np.float32)))
+    y32.copy_(x32)
+    e0, e1 = ev(), ev()
+    e0.record(stream)
+    r32c = s32c.sweeps(geom, x32, y32, n, lc, stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t32c = e0.elapsed_time(e1)
+    s32c_err = dc.s64.compare(geom, r32c, ref, "f32")
+    p32c = s32c.plan(geom, lc)
+    del x32, y32
     # FP32 + FP64 defect correction
     xm = torch.from_numpy(a).cuda()
     work = {"sx": xm.clone(), "r": torch.zeros(geom.shape, dtype=torch.float32, device="cuda"),
@@ -452,6 +471,8 @@ def run_precision(args) -> dict | None:
         "precision": {
             "f64": {"glups": glups(t64), "ms": t64},
             "f32": {"glups": glups(t32), "ms": t32, "max_rel": s32["max_rel"], "rms_rel": s32["rms_rel"]},
+            "f32_compensated": {"glups": glups(t32c), "ms": t32c, "max_rel": s32c_err["max_rel"],
+                                "rms_rel": s32c_err["rms_rel"], "variant": p32c.variant, "block": list(p32c.block)},
             "f32_defect_corrected": {"glups": glups(tmix), "ms": tmix, "max_rel": smix["max_rel"],
                                      "rms_rel": smix["rms_rel"], "fp64_sweeps": res.fp64_sweeps,
                                      "fp32_sweeps": res.fp32_sweeps,

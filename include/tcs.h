@@ -43,6 +43,9 @@ extern "C" {
 #define TCS_ALIGN_WRITE 2
 #define TCS_F64 0 /* the reference's arithmetic (double) */
 #define TCS_F32 1 /* single-precision grids */
+#define TCS_F32C 2 /* single-precision grids, compensated accumulation: every output also sums the
+                      rounding errors of its additions (two-sum) and products (fma(v,m,-v*m)) in the
+                      reference's term order and adds them at the end (direct and march kernels) */
 
 /* Kernel variants. */
 #define TCS_VARIANT_AUTO 0   /* pipe, else march, else direct: the first that supports the shape */

@@ -153,7 +153,7 @@ int validate(const tcs_spec* s) {
     return fail(TCS_ERR_INVALID_VALUE, "Unknown alignment: either 'None', 'Write' or 'Read'");
   if (s->alignment != TCS_ALIGN_NONE && s->cl_size <= 0)
     return fail(TCS_ERR_INVALID_VALUE, "size of alignment has to be > 0 when alignment is given");
-  if (s->precision != TCS_F64 && s->precision != TCS_F32)
+  if (s->precision != TCS_F64 && s->precision != TCS_F32 && s->precision != TCS_F32C)
     return fail(TCS_ERR_INVALID_VALUE, "Unknown precision");
   // Practical limits of one instantiation (the reference has none but its unrolled code
   // stops compiling long before these).
@@ -225,6 +225,7 @@ std::string instance_macros(const tcs_spec& s, const PipeKey* pk) {
       << "\n#define TCS_CH " << pk->ch << "\n#define TCS_LSHIFT " << pk->lshift << "\n";
   if (pk && pk->batch) m << "#define TCS_BATCH 1\n";
   m << "#define TCS_T " << (s.precision == TCS_F64 ? "double" : "float") << "\n"
+    << "#define TCS_COMP " << (s.precision == TCS_F32C ? 1 : 0) << "\n"
     << "#define TCS_DIM " << s.dimension << "\n"
     << "#define TCS_SHAPE " << s.neighbourhood << "\n"
     << "#define TCS_ORIENT " << s.orientation << "\n"
@@ -655,6 +656,8 @@ unsigned pipe_loader(const tcs_spec& s, unsigned long long xdim, const void* in)
 int resolve_pipe(tcs_stencil* h, const TcsGeo& g, const tcs_launch* L, Resolved& out,
                  bool batch = false) {
   const tcs_spec& s = h->spec;
+  if (s.precision == TCS_F32C)
+    return fail(TCS_ERR_UNSUPPORTED, "compensated FP32 runs on the direct kernel only");
   const unsigned R = (unsigned)s.range;
   const unsigned es = (unsigned)elem_size(s);
   const unsigned vec = 16u / es;

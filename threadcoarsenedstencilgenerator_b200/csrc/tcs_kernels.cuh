@@ -194,7 +194,7 @@ extern "C" __global__ void tcs_direct(const T* __restrict__ in, T* __restrict__ 
     auto ld = [&](int gx, int gy, int gz) {
       return __ldg(p + (tcs_i64)gx + (tcs_i64)gy * xdim + (tcs_i64)gz * plane);
     };
-    T acc[NE];
+    Acc acc[NE];
     traverse(ld, acc);
     store(out + base, acc, g.xdim, (tcs_u64)plane, src ? src + base : nullptr);
   }
@@ -352,7 +352,7 @@ extern "C" __global__ void tcs_march(const __grid_constant__ TcsTmaMap tmap,
     if (ok) {
       tcs_u32 pb = ring_base + tm;  // ring plane of the thread's footprint start (offset -R)
       if (pb >= ring_planes) pb -= ring_planes;
-      T acc[NE];
+      Acc acc[NE];
 #if TCS_DIM == 2
       auto ld = [&](int gx, int gy, int) {
         tcs_u32 rr = pb + (tcs_u32)(gy + R);

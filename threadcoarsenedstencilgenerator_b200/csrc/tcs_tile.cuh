@@ -36,6 +36,25 @@ constexpr int W1 = 2 * R + 1;
 // stencilSize as in cuda/generate2DStencil_cuda.py:63-67 and cuda/generate3DStencil_cuda.py:66-70
 constexpr int S = (SHAPE == 0) ? (DIM == 2 ? W1 * W1 : W1 * W1 * W1) : (2 * DIM * R + 1);
 constexpr int VEC = 16 / (int)sizeof(T);    // elements per 16-byte TMA granule
+#ifndef TCS_COMP
+#define TCS_COMP 0
+#endif
+// Compensated accumulation (FP32 grids, precision TCS_F32C): every output keeps a running sum and
+// the rounding errors of its additions (Knuth's two-sum) and of its products (fma(v, m, -v*m)),
+// added back at the end.  The terms still arrive in the reference's order.
+constexpr bool COMP = TCS_COMP != 0;
+struct CompAcc {
+  T s, c;
+};
+template <bool B, class X, class Y>
+struct pick {
+  typedef X type;
+};
+template <class X, class Y>
+struct pick<false, X, Y> {
+  typedef Y type;
+};
+typedef typename pick<COMP, CompAcc, T>::type Acc;  // one output's accumulator
 }  // namespace tcs
 
 // Stencil coefficients (Variable); the reference's `__constant__ double d_mask[S]`.
@@ -128,8 +147,37 @@ __device__ __forceinline__ void static_for(F&& f) {
 // Variable stencils keep the first value v0 of an output in its accumulator until the second
 // term arrives and then form fma(v0, m0, v1*m1): the nvcc -fmad=true fusion of the reference's
 // `result = v0*m0; result += v1*m1;` (an add of two products fuses its left operand).
+__device__ __forceinline__ void two_sum_add(CompAcc& a, const T p, const T ep) {
+  const T t = a.s + p;
+  const T z = t - a.s;
+  a.c = a.c + ((a.s - (t - z)) + (p - z) + ep);
+  a.s = t;
+}
+__device__ __forceinline__ T acc_value(const T& a) { return a; }
+__device__ __forceinline__ T acc_value(const CompAcc& a) { return a.s + a.c; }
+__device__ __forceinline__ void acc_zero(T& a) { a = T(0); }
+__device__ __forceinline__ void acc_zero(CompAcc& a) { a.s = T(0); a.c = T(0); }
+// First term: the plain accumulator holds v (a Variable product forms at the second term); the
+// compensated one starts from v*m and its rounding error (m = 1 for Jacobi).
+__device__ __forceinline__ void acc_first(T& a, const T v, const T) { a = v; }
+__device__ __forceinline__ void acc_first(CompAcc& a, const T v, const T m) {
+  a.s = v * m;
+  a.c = fmat(v, m, -a.s);
+}
+__device__ __forceinline__ void acc_add(T& a, const T v) { a = a + v; }
+__device__ __forceinline__ void acc_add(CompAcc& a, const T v) { two_sum_add(a, v, T(0)); }
+__device__ __forceinline__ void acc_fma(T& a, const T v, const T m) { a = fmat(v, m, a); }
+__device__ __forceinline__ void acc_fma(CompAcc& a, const T v, const T m) {
+  const T p = v * m;
+  two_sum_add(a, p, fmat(v, m, -p));
+}
+// Second Variable term: fma(v0, m0, fl(v1*m1)) for the plain accumulator; for the compensated one
+// the first product is already formed.
+__device__ __forceinline__ void acc_second(T& a, const T m0, const T v, const T m) { a = fmat(a, m0, v * m); }
+__device__ __forceinline__ void acc_second(CompAcc& a, const T, const T v, const T m) { acc_fma(a, v, m); }
+
 template <int GX, int GY, int GZ>
-__device__ __forceinline__ void apply(T (&acc)[NE], const T v) {
+__device__ __forceinline__ void apply(Acc (&acc)[NE], const T v) {
   static_for<0, CZ>([&](auto ez) {
     static_for<0, CY>([&](auto ey) {
       static_for<0, CX>([&](auto ex) {
@@ -139,13 +187,13 @@ __device__ __forceinline__ void apply(T (&acc)[NE], const T v) {
         constexpr int e = decltype(ex)::value + decltype(ey)::value * CX + decltype(ez)::value * CX * CY;
         if constexpr (contributes(rx, ry, rz)) {
           if constexpr (is_first(rx, ry, rz)) {
-            acc[e] = v;
+            acc_first(acc[e], v, (COEFF == 0) ? T(1) : tcs_mask[mask_index(rx, ry, rz)]);
           } else if constexpr (COEFF == 0) {
-            acc[e] = acc[e] + v;
+            acc_add(acc[e], v);
           } else if constexpr (is_second(rx, ry, rz)) {
-            acc[e] = fmat(acc[e], tcs_mask[first_mask_index()], v * tcs_mask[mask_index(rx, ry, rz)]);
+            acc_second(acc[e], tcs_mask[first_mask_index()], v, tcs_mask[mask_index(rx, ry, rz)]);
           } else {
-            acc[e] = fmat(v, tcs_mask[mask_index(rx, ry, rz)], acc[e]);
+            acc_fma(acc[e], v, tcs_mask[mask_index(rx, ry, rz)]);
           }
         }
       });
@@ -154,7 +202,7 @@ __device__ __forceinline__ void apply(T (&acc)[NE], const T v) {
 }
 
 template <int GX, int GY, int GZ, class LD>
-__device__ __forceinline__ void point(const LD& ld, T (&acc)[NE]) {
+__device__ __forceinline__ void point(const LD& ld, Acc (&acc)[NE]) {
   apply<GX, GY, GZ>(acc, ld(GX, GY, GZ));
 }
 
@@ -162,7 +210,7 @@ __device__ __forceinline__ void point(const LD& ld, T (&acc)[NE]) {
 // (cuda/generate2DStencil_cuda.py:244-297, cuda/generate3DStencil_cuda.py:265-360).
 // Loops run over [-R, ...) as [0, ...) shifted by R.
 template <int GZ, class LD>
-__device__ __forceinline__ void traverse_slice(const LD& ld, T (&acc)[NE]) {
+__device__ __forceinline__ void traverse_slice(const LD& ld, Acc (&acc)[NE]) {
   // one z slice of a Box stencil (or the whole 2D Box stencil with GZ = 0)
   if constexpr (ORIENT == 1) {
     static_for<0, 2 * R + CX>([&](auto ix) {
@@ -180,7 +228,7 @@ __device__ __forceinline__ void traverse_slice(const LD& ld, T (&acc)[NE]) {
 }
 
 template <int GZ, class LD>
-__device__ __forceinline__ void traverse_cross(const LD& ld, T (&acc)[NE]) {
+__device__ __forceinline__ void traverse_cross(const LD& ld, Acc (&acc)[NE]) {
   // the in-slice cross of a Star stencil
   if constexpr (ORIENT == 1) {
     static_for<0, R>([&](auto i) {  // gx in [-R, 0)
@@ -206,7 +254,7 @@ __device__ __forceinline__ void traverse_cross(const LD& ld, T (&acc)[NE]) {
 }
 
 template <int GZ, class LD>
-__device__ __forceinline__ void traverse_column(const LD& ld, T (&acc)[NE]) {
+__device__ __forceinline__ void traverse_column(const LD& ld, Acc (&acc)[NE]) {
   // the thread's own columns in a z slice outside the centre (Star, 3D)
   if constexpr (ORIENT == 1) {
     static_for<0, CX>([&](auto gx) {
@@ -220,9 +268,9 @@ __device__ __forceinline__ void traverse_column(const LD& ld, T (&acc)[NE]) {
 }
 
 template <class LD>
-__device__ __forceinline__ void traverse(const LD& ld, T (&acc)[NE]) {
+__device__ __forceinline__ void traverse(const LD& ld, Acc (&acc)[NE]) {
 #pragma unroll
-  for (int e = 0; e < NE; ++e) acc[e] = T(0);
+  for (int e = 0; e < NE; ++e) acc_zero(acc[e]);
   if constexpr (DIM == 2) {
     if constexpr (SHAPE == 0)
       traverse_slice<0>(ld, acc);
@@ -241,7 +289,7 @@ __device__ __forceinline__ void traverse(const LD& ld, T (&acc)[NE]) {
 // An optional source array `src` (same layout, positioned like `o`) is added after the stencil
 // value: out = stencil(in) + src.  Sweeps without a source (src == nullptr, every drop-in sweep)
 // store the reference's value unchanged.
-__device__ __forceinline__ void store(T* __restrict__ o, const T (&acc)[NE], tcs_u64 xdim,
+__device__ __forceinline__ void store(T* __restrict__ o, const Acc (&acc)[NE], tcs_u64 xdim,
                                       tcs_u64 plane, const T* __restrict__ src = nullptr) {
   constexpr T c = T(1) / T(S);
 #pragma unroll
@@ -252,7 +300,7 @@ __device__ __forceinline__ void store(T* __restrict__ o, const T (&acc)[NE], tcs
       for (int ex = 0; ex < CX; ++ex) {
         const int e = ex + ey * CX + ez * CX * CY;
         const tcs_i64 off = (tcs_i64)ex + (tcs_i64)ey * (tcs_i64)xdim + (tcs_i64)ez * (tcs_i64)plane;
-        T v = (COEFF == 0) ? acc[e] * c : acc[e];
+        T v = (COEFF == 0) ? acc_value(acc[e]) * c : acc_value(acc[e]);
         if (src) v = v + src[off];
         o[off] = v;
       }

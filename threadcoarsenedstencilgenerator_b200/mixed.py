@@ -5,7 +5,8 @@ of the fixed border.  Every ``period`` sweeps the engine
   1. computes the defect r = S(x) - x in FP64 on the GPU (one FP64 sweep plus ``tcs_residual``,
      which also returns the global residual norms in FP64),
   2. runs ``period`` FP32 sweeps of the correction recurrence e <- A e + r from e = 0 (zero border;
-     the source term r is added in the sweep epilogue, ``tcs_update_grid_source``),
+     the source term r is added in the sweep epilogue, ``tcs_update_grid_source``).  The first
+     step gives e = r exactly (A 0 = 0), so it is a copy of r instead of a sweep,
   3. accumulates x += e in FP64 (``tcs_accumulate``).
 In exact arithmetic e after k steps equals sum_{i<k} A^i r, so x + e is exactly the FP64 state k
 sweeps later; rounding enters only through the FP32 correction, whose size is the change of the
@@ -27,7 +28,7 @@ from .stencil import Launch, Stencil
 class MixedResult:
     sweeps: int
     fp64_sweeps: int
-    fp32_sweeps: int
+    fp32_sweeps: int  # steps of the FP32 recurrence (the first of every period is a copy of r)
     residual_history: list = field(default_factory=list)  # (max |r|, ||r||_2) per period
 
 
@@ -62,6 +63,8 @@ class DefectCorrectedSweeps:
                     "e1": torch.zeros(geom.shape, dtype=torch.float32, device=x.device)}
         sx, r, e0, e1 = work["sx"], work["r"], work["e0"], work["e1"]
         sx.copy_(x)  # the border of S(x) is x's border
+        r.zero_()    # the correction fields keep a zero border: r's is copied into e0 each period
+        e1.zero_()
         res = MixedResult(n, 0, 0)
         done = 0
         while done < n:
@@ -70,10 +73,9 @@ class DefectCorrectedSweeps:
             norms = self.s64.residual(geom, x, sx, r, stream)
             res.residual_history.append(norms)
             res.fp64_sweeps += 1
-            e0.zero_()
-            e1.zero_()
+            e0.copy_(r)  # e after the first step: A 0 + r = r
             a, b = e0, e1
-            for _ in range(k):
+            for _ in range(k - 1):
                 if self.tensor_cores:
                     self.s32.tc_update_grid(geom, a, b, source=r, stream=stream)
                 else:

@@ -17,7 +17,7 @@ NEIGHBOURHOODS = ("Box", "Star")
 ORIENTATIONS = ("Row", "Column")
 COEFFICIENTS = ("Jacobi", "Variable")
 ALIGNMENTS = ("None", "Read", "Write")
-PRECISIONS = ("f64", "f32")
+PRECISIONS = ("f64", "f32", "f32c")  # f32c: FP32 grids, compensated (two-sum) accumulation
 
 
 @dataclass(frozen=True)
