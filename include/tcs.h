@@ -120,6 +120,15 @@ int tcs_stencil_size(const tcs_spec* spec, unsigned* stencil_size, unsigned* flo
 /* Truncation to a coarsening multiple and Read/Write row padding (cuda/benchmark.cpp:142-179). */
 int tcs_compute_geometry(const tcs_spec* spec, unsigned nx, unsigned ny, unsigned nz,
                          tcs_geometry* out);
+/* The same geometry without the truncation of the interior to a coarsening multiple (no
+ * counterpart in the reference, which truncates: cuda/benchmark.cpp:142-166).  Sweeps of such a
+ * "ragged" grid update every interior point: the kernels sweep the whole coarsening tiles and a
+ * coarsening-1 instance of the direct kernel sweeps the partial tiles at the far x, y and z ends,
+ * with the reference's per-point term order (the values equal a coarsening-1 sweep bit for bit).
+ * threads[] counts the partial tiles. */
+int tcs_compute_geometry_ragged(const tcs_spec* spec, unsigned nx, unsigned ny, unsigned nz,
+                                tcs_geometry* out);
+
 /* Left offset baked into Write-aligned kernels (cuda/generate2DStencil_cuda.py:83-85). */
 int tcs_left_offset(const tcs_spec* spec, unsigned* left_offset);
 

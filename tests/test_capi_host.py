@@ -104,3 +104,17 @@ def test_precompile_without_gpu(tmp_path, monkeypatch):
     path = tcs.precompile(tcs.StencilSpec(dimension=3, neighbourhood="Star", coefficients="Variable", range=2,
                                           cx=2, cy=1, cz=2))
     assert Path(path).exists() and Path(path).stat().st_size > 1000
+
+
+def test_ragged_geometry_keeps_the_whole_interior():
+    from threadcoarsenedstencilgenerator_b200 import StencilSpec
+
+    s = StencilSpec(dimension=3, neighbourhood="Star", coefficients="Variable", range=4, cx=2, cy=4, cz=3,
+                    alignment="Read", cl_size=16)
+    g = s.geometry(61, 47, 39, ragged=True)
+    t = s.geometry(61, 47, 39)
+    assert g.elements == (53, 39, 31) and t.elements == (52, 36, 30)
+    assert g.threads == (27, 10, 11) and g.grid[1:] == (47, 39)
+    assert g.grid[0] % 16 == 0 and g.grid[0] - g.right_offset == 61
+    # multiples of the coarsening: identical to the reference geometry
+    assert s.geometry(64, 48, 41, ragged=True) == s.geometry(64, 48, 41)

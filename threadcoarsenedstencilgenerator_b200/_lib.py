@@ -109,6 +109,7 @@ SIGNATURES = {
     "tcs_spec_validate": [_P(CSpec)],
     "tcs_stencil_size": [_P(CSpec), _P(_u), _P(_u)],
     "tcs_compute_geometry": [_P(CSpec), _u, _u, _u, _P(CGeometry)],
+    "tcs_compute_geometry_ragged": [_P(CSpec), _u, _u, _u, _P(CGeometry)],
     "tcs_left_offset": [_P(CSpec), _P(_u)],
     "tcs_create": [_P(CSpec), _P(_vp)],
     "tcs_destroy": [_vp],

@@ -356,6 +356,9 @@ struct tcs_stencil {
   size_t scratch_len = 0;                 // in doubles
   std::vector<PipeMod*> pipes;            // pipelined-sweep modules, one per launch shape
   void* tc_bops = nullptr;                // tensor-core Toeplitz operands (built from mask_host)
+  CUmodule fringe_mod = nullptr;          // coarsening-1 instance for the ragged fringe of a grid
+  CUfunction f_fringe = nullptr;
+  CUdeviceptr fringe_mask = 0;
   bool tc_stale = true;                   // mask changed since tc_bops was built
   std::mutex mu;
   std::vector<MapEntry> maps;
@@ -848,6 +851,69 @@ int tensor_map(tcs_stencil* h, const void* ptr, const Resolved& r, CUtensorMap**
   return TCS_OK;
 }
 
+// ---- ragged grids --------------------------------------------------------------------------
+// Every kernel updates whole coarsening tiles only, like the reference's.  When the interior is
+// not a multiple of the coarsening (a grid from tcs_compute_geometry_ragged), the points of the
+// partial tiles -- the fringe -- are swept by a second instance of the direct kernel with
+// coarsening 1 x 1 x 1.  The per-point term order does not depend on the coarsening, so the fringe
+// values are the ones a coarsening-1 sweep of the whole grid would give, bit for bit.
+int fringe_module(tcs_stencil* h) {
+  std::lock_guard<std::mutex> lock(h->mu);
+  if (h->fringe_mod) return TCS_OK;
+  tcs_spec s1 = h->spec;
+  s1.cx = s1.cy = s1.cz = 1;
+  std::vector<char> cubin;
+  int rc = instantiate(s1, nullptr, cubin, nullptr);
+  if (rc) return rc;
+  CUmodule mod = nullptr;
+  CUresult cr = g_drv.ModuleLoadData(&mod, cubin.data());
+  if (cr != CUDA_SUCCESS) return fail(TCS_ERR_CUDA, "cuModuleLoadData (fringe): " + cu_msg(cr));
+  size_t bytes = 0;
+  if ((cr = g_drv.ModuleGetFunction(&h->f_fringe, mod, "tcs_direct")) != CUDA_SUCCESS ||
+      (cr = g_drv.ModuleGetGlobal(&h->fringe_mask, &bytes, mod, "tcs_mask")) != CUDA_SUCCESS) {
+    g_drv.ModuleUnload(mod);
+    return fail(TCS_ERR_CUDA, "fringe module symbols: " + cu_msg(cr));
+  }
+  h->fringe_mod = mod;
+  return upload_mask(h, h->fringe_mask);
+}
+
+int launch_fringe(tcs_stencil* h, const TcsGeo& g, const void* in, void* out, const void* src, CUstream st) {
+  const tcs_spec& s = h->spec;
+  const bool d3 = s.dimension == 3;
+  const unsigned R = (unsigned)s.range;
+  const unsigned cz = d3 ? (unsigned)s.cz : 1u;
+  const unsigned ex = g.x_lim > g.x0 ? g.x_lim - g.x0 : 0, ey = g.y_lim - R, ez = d3 ? g.z_lim - R : 0;
+  const unsigned xf = g.x0 + ex / s.cx * s.cx, yf = R + ey / s.cy * s.cy, zf = d3 ? R + ez / cz * cz : g.z_lim;
+  if (xf == g.x0 + ex && yf == g.y_lim && zf == g.z_lim) return TCS_OK;
+  int rc = fringe_module(h);
+  if (rc) return rc;
+  const size_t es = (size_t)elem_size(s);
+  // regions [xa, xb) x [ya, yb) x [za, zb): the partial x tiles, then partial y, then partial z
+  const unsigned z0 = d3 ? R : 0;
+  const unsigned reg[3][6] = {{xf, g.x_lim, R, g.y_lim, z0, g.z_lim},
+                              {g.x0, xf, yf, g.y_lim, z0, g.z_lim},
+                              {g.x0, xf, R, yf, zf, g.z_lim}};
+  for (int k = 0; k < (d3 ? 3 : 2); ++k) {
+    const unsigned xa = reg[k][0], xb = reg[k][1], ya = reg[k][2], yb = reg[k][3], za = reg[k][4], zb = reg[k][5];
+    if (xa >= xb || ya >= yb || (d3 && za >= zb)) continue;
+    // The direct kernel starts at row R and plane R: shift the buffers so that those are ya, za.
+    const size_t shift = ((size_t)(ya - R) * g.xdim + (d3 ? (size_t)(za - R) * g.xdim * g.ydim : 0)) * es;
+    TcsGeo f = g;
+    f.x0 = xa;
+    f.x_lim = xb;
+    f.y_lim = yb - (ya - R);
+    f.z_lim = d3 ? zb - (za - R) : g.z_lim;
+    CUdeviceptr pin = (CUdeviceptr)in + shift, pout = (CUdeviceptr)out + shift;
+    CUdeviceptr psrc = src ? (CUdeviceptr)src + shift : 0;
+    void* args[] = {&pin, &pout, &psrc, &f};
+    const unsigned bx = 32, by = 4, bz = d3 ? 2 : 1;
+    TCS_CU(g_drv.LaunchKernel(h->f_fringe, cdiv(xb - xa, bx), cdiv(yb - ya, by), d3 ? cdiv(zb - za, bz) : 1, bx, by,
+                              bz, 0, st, args, nullptr));
+  }
+  return TCS_OK;
+}
+
 // `pre`: an already encoded tensor map of `in` for the pipe kernel (skips the map cache).
 int launch_resolved(tcs_stencil* h, const Resolved& r, const void* in, void* out, CUstream st,
                     const void* src = nullptr, const CUtensorMap* pre = nullptr) {
@@ -861,7 +927,7 @@ int launch_resolved(tcs_stencil* h, const Resolved& r, const void* in, void* out
     void* args[] = {&pin, &pout, &psrc, &geo};
     TCS_CU(g_drv.LaunchKernel(h->f_direct, r.grid[0], r.grid[1], r.grid[2], r.block[0],
                               r.block[1], r.block[2], 0, st, args, nullptr));
-    return TCS_OK;
+    return launch_fringe(h, r.geo, in, out, src, st);
   }
   if (r.variant == TCS_VARIANT_PIPE) {
     TcsPipeGeo pg = r.pgeo;
@@ -880,7 +946,7 @@ int launch_resolved(tcs_stencil* h, const Resolved& r, const void* in, void* out
     void* args[] = {&pmap, &pin, &pout, &psrc, &pg};
     TCS_CU(g_drv.LaunchKernel(r.pipe->f, r.grid[0], 1, 1, r.block[0], r.block[1], 1, r.smem, st,
                               args, nullptr));
-    return TCS_OK;
+    return launch_fringe(h, r.geo, in, out, src, st);
   }
   // The TMA loader also needs a 16-byte aligned base address; otherwise copy with cp.async.
   if (geo.loader == 0 && reinterpret_cast<uintptr_t>(in) % 16 != 0) geo.loader = 1;
@@ -896,7 +962,7 @@ int launch_resolved(tcs_stencil* h, const Resolved& r, const void* in, void* out
   void* args[] = {&mcopy, &pin, &pout, &psrc, &geo};
   TCS_CU(g_drv.LaunchKernel(h->f_march, r.grid[0], r.grid[1], r.grid[2], r.block[0], r.block[1],
                             r.block[2], r.smem, st, args, nullptr));
-  return TCS_OK;
+  return launch_fringe(h, r.geo, in, out, src, st);
 }
 
 }  // namespace
@@ -928,8 +994,13 @@ int tcs_left_offset(const tcs_spec* spec, unsigned* left_offset) {
   return TCS_OK;
 }
 
-int tcs_compute_geometry(const tcs_spec* spec, unsigned nx, unsigned ny, unsigned nz,
-                         tcs_geometry* out) {
+}  // extern "C"
+
+namespace {
+
+// The reference's geometry (cuda/benchmark.cpp:142-179); with `ragged` the truncation of the
+// interior to a coarsening multiple is skipped (threads then counts partial tiles).
+int geometry_impl(const tcs_spec* spec, unsigned nx, unsigned ny, unsigned nz, bool ragged, tcs_geometry* out) {
   int rc = validate(spec);
   if (rc) return rc;
   if (!out) return fail(TCS_ERR_INVALID_VALUE, "geometry output is NULL");
@@ -950,9 +1021,9 @@ int tcs_compute_geometry(const tcs_spec* spec, unsigned nx, unsigned ny, unsigne
       g.threads[2] = 1;
       continue;
     }
-    g.grid[i] = n[i] - (n[i] - 2 * R) % c[i];
+    g.grid[i] = ragged ? n[i] : n[i] - (n[i] - 2 * R) % c[i];
     g.elements[i] = g.grid[i] - 2 * R;
-    g.threads[i] = g.elements[i] / c[i];
+    g.threads[i] = (g.elements[i] + (ragged ? c[i] - 1 : 0)) / c[i];
   }
   unsigned long long xmem = g.grid[0];
   unsigned right = 0, left = 0;
@@ -973,6 +1044,18 @@ int tcs_compute_geometry(const tcs_spec* spec, unsigned nx, unsigned ny, unsigne
   g.n_points = (unsigned long long)g.grid[0] * g.grid[1] * g.grid[2];
   *out = g;
   return TCS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int tcs_compute_geometry(const tcs_spec* spec, unsigned nx, unsigned ny, unsigned nz, tcs_geometry* out) {
+  return geometry_impl(spec, nx, ny, nz, false, out);
+}
+
+int tcs_compute_geometry_ragged(const tcs_spec* spec, unsigned nx, unsigned ny, unsigned nz, tcs_geometry* out) {
+  return geometry_impl(spec, nx, ny, nz, true, out);
 }
 
 int tcs_create(const tcs_spec* spec, tcs_stencil** out) {
@@ -1019,6 +1102,7 @@ int tcs_create(const tcs_spec* spec, tcs_stencil** out) {
 
 int tcs_destroy(tcs_stencil* h) {
   if (!h) return TCS_OK;
+  if (h->fringe_mod && g_drv.ModuleUnload) g_drv.ModuleUnload(h->fringe_mod);
   if (h->scratch) cudaFree(h->scratch);
   if (h->tc_bops) cudaFree(h->tc_bops);
   for (PipeMod* p : h->pipes) {
@@ -1050,6 +1134,7 @@ int tcs_copy_mask(tcs_stencil* h, const double* mask, unsigned n) {
     rc = upload_mask(h, p->mask_ptr);
     if (rc) return rc;
   }
+  if (h->fringe_mod && (rc = upload_mask(h, h->fringe_mask))) return rc;
   TCS_RT(cudaDeviceSynchronize());
   return TCS_OK;
 }
@@ -1473,6 +1558,8 @@ struct tcs_batch {
   CUdeviceptr table[2] = {0, 0};        // grid tables: a -> b, b -> a
   std::vector<Resolved> single;         // per-grid single-grid launches (filled on first use)
   std::vector<CUtensorMap> maps[2];     // per-grid tensor maps of the input, per direction
+  std::vector<TcsGeo> ragged;           // grids whose interior is not a coarsening multiple
+  std::vector<unsigned> ragged_ids;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
 };
@@ -1494,6 +1581,11 @@ int batch_launch(tcs_batch* b, int from_b, CUstream st) {
   void* args[] = {&table, &ngrids, &total, &per, &nslot};
   TCS_CU(g_drv.LaunchKernel(b->pm->f, b->nctas, 1, 1, b->block[0], b->block[1], 1, b->smem, st, args,
                             nullptr));
+  for (size_t k = 0; k < b->ragged.size(); ++k) {  // partial coarsening tiles of ragged grids
+    const unsigned i = b->ragged_ids[k];
+    int rc = launch_fringe(b->h, b->ragged[k], from_b ? b->b[i] : b->a[i], from_b ? b->a[i] : b->b[i], nullptr, st);
+    if (rc) return rc;
+  }
   return TCS_OK;
 }
 
@@ -1582,6 +1674,15 @@ int tcs_batch_create(tcs_stencil* h, unsigned ngrids, const unsigned* grids,
       B->block[1] = r.block[1];
     }
     const TcsPipeGeo& pg = r.pgeo;
+    {
+      const unsigned cz = s.dimension == 3 ? (unsigned)s.cz : 1u;
+      const bool rx = (g.x_lim - g.x0) % (unsigned)s.cx != 0, ry = (g.y_lim - (unsigned)s.range) % (unsigned)s.cy != 0;
+      const bool rz = s.dimension == 3 && (g.z_lim - (unsigned)s.range) % cz != 0;
+      if (rx || ry || rz) {
+        B->ragged.push_back(g);
+        B->ragged_ids.push_back(i);
+      }
+    }
     for (int d = 0; d < 2; ++d) {
       TcsBatchGrid& e = tab[d][i];
       std::memset(&e, 0, sizeof(e));

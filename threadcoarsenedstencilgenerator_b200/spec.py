@@ -78,9 +78,12 @@ class StencilSpec:
     def itemsize(self) -> int:
         return 8 if self.precision == "f64" else 4
 
-    def geometry(self, nx: int, ny: int, nz: int = 1) -> "Geometry":
+    def geometry(self, nx: int, ny: int, nz: int = 1, ragged: bool = False) -> "Geometry":
+        """The reference's geometry; ``ragged=True`` keeps the interior whole instead of truncating
+        it to a coarsening multiple (sweeps then also update the partial tiles)."""
         g = _lib.CGeometry()
-        _lib.check(_lib.load().tcs_compute_geometry(ctypes.byref(self.to_c()), nx, ny, nz, ctypes.byref(g)))
+        fn = _lib.load().tcs_compute_geometry_ragged if ragged else _lib.load().tcs_compute_geometry
+        _lib.check(fn(ctypes.byref(self.to_c()), nx, ny, nz, ctypes.byref(g)))
         return Geometry(tuple(g.grid), tuple(g.elements), tuple(g.threads), g.left_offset, g.right_offset,
                         g.n_points, self.dimension)
 
