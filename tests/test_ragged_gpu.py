@@ -18,7 +18,7 @@ CASES = [
     ((3, "Star", "Row", "Variable", 4, 2, 4, 3, "Read", 16), (16, 4, 1), (61, 47, 39)),
     ((2, "Box", "Row", "Variable", 3, 4, 3, 1, "None", 0), (16, 4, 1), (103, 77, 1)),
     ((3, "Box", "Column", "Jacobi", 1, 2, 2, 2, "Write", 8), (16, 4, 1), (33, 29, 27)),
-    ((2, "Star", "Column", "Variable", 2, 3, 2, 1, "Read", 8), (32, 4, 1), (91, 58, 1)),
+    ((2, "Star", "Column", "Variable", 2, 3, 2, 1, "Read", 8), (32, 4, 1), (92, 59, 1)),
 ]
 
 
