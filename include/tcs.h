@@ -277,6 +277,18 @@ int tcs_batch_destroy(tcs_batch* b);
 int tcs_precompile_batch(const tcs_spec* spec, unsigned bx, unsigned by, unsigned chunk,
                          char* cubin_path, unsigned path_cap);
 
+/* n ping-pong sweeps starting from `a` with temporal blocking (2D only; no counterpart in the
+ * reference): every pair of sweeps is one pass over the grid -- a CTA computes the first sweep on
+ * its tile plus a range-wide halo in shared memory and the second from it -- so HBM is read and
+ * written once per two sweeps.  Each point's terms keep the reference's order: results equal n
+ * ordinary sweeps bit for bit (ragged grids included).  An odd last sweep is an ordinary sweep.
+ * *result_in_b tells which buffer holds the result. */
+int tcs_sweeps_tb2(tcs_stencil* h, const unsigned grid[3], unsigned right_offset, void* a, void* b,
+                   unsigned n, void* stream, int* result_in_b);
+/* Instantiate the coarsening-1 instance of a parameter set (fringe of ragged grids, temporal
+ * blocking) into the cubin cache (NVRTC only). */
+int tcs_precompile_fringe(const tcs_spec* spec, char* cubin_path, unsigned path_cap);
+
 /* ---- Tensor-core sweep of 2D Box stencils on FP32 grids (no counterpart in the reference, which
  * runs the generated kernel on the FP64 pipe: cuda/generate2DStencil_cuda.py:146-198) ----
  * out = stencil(in) (+ src when src != NULL) over the interior, as a banded dense contraction on the

@@ -151,6 +151,8 @@ SIGNATURES = {
     "tcs_mlp_adam_step": [_vp, _vp, _vp, _u, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float,
                           _P(ctypes.c_float), _vp],
     "tcs_mlp_destroy": [_vp],
+    "tcs_sweeps_tb2": [_vp, U3, _u, _vp, _vp, _u, _vp, _P(_i)],
+    "tcs_precompile_fringe": [_P(CSpec), ctypes.c_char_p, _u],
     "tcs_tc_supported": [_P(CSpec)],
     "tcs_tc_update_grid": [_vp, U3, _u, _vp, _vp, _vp, _vp],
 }

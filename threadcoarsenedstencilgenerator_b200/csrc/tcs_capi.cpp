@@ -242,8 +242,8 @@ std::atomic<unsigned long long> g_tmp_counter{0};
 // NVRTC programs are independent, so instantiations run concurrently (the build step compiles
 // many in parallel); a finished cubin is published into the cache by an atomic rename.
 int instantiate(const tcs_spec& s, const PipeKey* pk, std::vector<char>& cubin,
-                std::string* path_out) {
-  const std::string src = instance_macros(s, pk) + "#include \"tcs_kernels.cuh\"\n";
+                std::string* path_out, const char* extra = nullptr) {
+  const std::string src = instance_macros(s, pk) + (extra ? extra : "") + "#include \"tcs_kernels.cuh\"\n";
   const char* opts[] = {"--gpu-architecture=sm_100a", "--std=c++17", "--fmad=false",
                         "--device-as-default-execution-space"};
   const int nopts = sizeof(opts) / sizeof(opts[0]);
@@ -358,6 +358,8 @@ struct tcs_stencil {
   void* tc_bops = nullptr;                // tensor-core Toeplitz operands (built from mask_host)
   CUmodule fringe_mod = nullptr;          // coarsening-1 instance for the ragged fringe of a grid
   CUfunction f_fringe = nullptr;
+  CUfunction f_tb2 = nullptr;             // two sweeps per pass (2D, same instance)
+  int tb2_smem_attr = 0;
   CUdeviceptr fringe_mask = 0;
   bool tc_stale = true;                   // mask changed since tc_bops was built
   std::mutex mu;
@@ -852,6 +854,7 @@ int tensor_map(tcs_stencil* h, const void* ptr, const Resolved& r, CUtensorMap**
 }
 
 // ---- ragged grids --------------------------------------------------------------------------
+// (The coarsening-1 instance also carries tcs_tb2 for 2D parameter sets: two sweeps per pass.)
 // Every kernel updates whole coarsening tiles only, like the reference's.  When the interior is
 // not a multiple of the coarsening (a grid from tcs_compute_geometry_ragged), the points of the
 // partial tiles -- the fringe -- are swept by a second instance of the direct kernel with
@@ -863,13 +866,15 @@ int fringe_module(tcs_stencil* h) {
   tcs_spec s1 = h->spec;
   s1.cx = s1.cy = s1.cz = 1;
   std::vector<char> cubin;
-  int rc = instantiate(s1, nullptr, cubin, nullptr);
+  const bool d2 = s1.dimension == 2;
+  int rc = instantiate(s1, nullptr, cubin, nullptr, d2 ? "#define TCS_TB 1\n" : nullptr);
   if (rc) return rc;
   CUmodule mod = nullptr;
   CUresult cr = g_drv.ModuleLoadData(&mod, cubin.data());
   if (cr != CUDA_SUCCESS) return fail(TCS_ERR_CUDA, "cuModuleLoadData (fringe): " + cu_msg(cr));
   size_t bytes = 0;
   if ((cr = g_drv.ModuleGetFunction(&h->f_fringe, mod, "tcs_direct")) != CUDA_SUCCESS ||
+      (d2 && (cr = g_drv.ModuleGetFunction(&h->f_tb2, mod, "tcs_tb2")) != CUDA_SUCCESS) ||
       (cr = g_drv.ModuleGetGlobal(&h->fringe_mask, &bytes, mod, "tcs_mask")) != CUDA_SUCCESS) {
     g_drv.ModuleUnload(mod);
     return fail(TCS_ERR_CUDA, "fringe module symbols: " + cu_msg(cr));
@@ -1933,3 +1938,83 @@ int tcs_tc_update_grid(tcs_stencil* h, const unsigned grid[3], unsigned right_of
 }
 
 }  // extern "C"
+
+// =============================================================================================
+// Temporal blocking: two sweeps per pass over the grid (2D; tcs_tb2 in tcs_kernels.cuh).
+
+namespace {
+
+constexpr unsigned TB_TX = 128, TB_TY = 32;
+
+int launch_tb2(tcs_stencil* h, const TcsGeo& g, const void* in, void* out, CUstream st) {
+  const unsigned R = (unsigned)h->spec.range;
+  const unsigned es = (unsigned)elem_size(h->spec);
+  const unsigned smem = ((TB_TX + 4 * R) * (TB_TY + 4 * R) + (TB_TX + 2 * R) * (TB_TY + 2 * R)) * es;
+  if (smem > (unsigned)h->smem_optin) return fail(TCS_ERR_UNSUPPORTED, "tb2: tile does not fit in shared memory");
+  {
+    std::lock_guard<std::mutex> lock(h->mu);
+    if ((int)smem > h->tb2_smem_attr) {
+      TCS_CU(g_drv.FuncSetAttribute(h->f_tb2, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, (int)smem));
+      h->tb2_smem_attr = (int)smem;
+    }
+  }
+  const unsigned long long ex = g.x_lim > g.x0 ? g.x_lim - g.x0 : 0, ey = g.y_lim - R;
+  const unsigned gx = std::max(1u, cdiv(ex, TB_TX)), gy = std::max(1u, cdiv(ey, TB_TY));
+  if (gy > 65535) return fail(TCS_ERR_UNSUPPORTED, "tb2: too many tile rows");
+  CUdeviceptr pin = (CUdeviceptr)in, pout = (CUdeviceptr)out;
+  TcsGeo geo = g;
+  void* args[] = {&pin, &pout, &geo};
+  TCS_CU(g_drv.LaunchKernel(h->f_tb2, gx, gy, 1, 256, 1, 1, smem, st, args, nullptr));
+  return TCS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int tcs_sweeps_tb2(tcs_stencil* h, const unsigned grid[3], unsigned right_offset, void* a, void* b, unsigned n,
+                   void* stream, int* result_in_b) {
+  if (!h) return fail(TCS_ERR_INVALID_VALUE, "NULL handle");
+  if (h->spec.dimension != 2) return fail(TCS_ERR_UNSUPPORTED, "tb2: 2D stencils only");
+  if (!a || !b || a == b) return fail(TCS_ERR_INVALID_VALUE, "need two distinct buffers");
+  TcsGeo g;
+  int rc = make_geo(h, grid, right_offset, g);
+  if (rc) return rc;
+  if ((rc = fringe_module(h))) return rc;
+  void* src = a;
+  void* dst = b;
+  for (unsigned i = 0; i + 1 < n; i += 2) {  // pairs of sweeps, one pass each
+    if ((rc = launch_tb2(h, g, src, dst, (CUstream)stream))) return rc;
+    std::swap(src, dst);
+  }
+  if (n % 2 == 1) {  // the last odd sweep: one ordinary sweep
+    tcs_launch L{};
+    L.block[0] = 128;
+    L.block[1] = 1;
+    L.block[2] = 1;
+    L.variant = TCS_VARIANT_AUTO;
+    Resolved r;
+    if ((rc = resolve(h, grid, right_offset, &L, r))) return rc;
+    if ((rc = launch_resolved(h, r, src, dst, (CUstream)stream))) return rc;
+    std::swap(src, dst);
+  }
+  if (result_in_b) *result_in_b = (src == b) ? 1 : 0;
+  return TCS_OK;
+}
+
+}  // extern "C"
+
+extern "C" int tcs_precompile_fringe(const tcs_spec* spec, char* cubin_path, unsigned path_cap) {
+  int rc = validate(spec);
+  if (rc) return rc;
+  tcs_spec s1 = *spec;
+  s1.cx = s1.cy = s1.cz = 1;
+  std::vector<char> cubin;
+  std::string path;
+  if ((rc = instantiate(s1, nullptr, cubin, &path, s1.dimension == 2 ? "#define TCS_TB 1\n" : nullptr))) return rc;
+  if (cubin_path && path_cap) {
+    std::strncpy(cubin_path, path.c_str(), path_cap - 1);
+    cubin_path[path_cap - 1] = '\0';
+  }
+  return TCS_OK;
+}

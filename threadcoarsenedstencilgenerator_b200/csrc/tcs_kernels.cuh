@@ -378,6 +378,65 @@ extern "C" __global__ void tcs_march(const __grid_constant__ TcsTmaMap tmap,
   }
 }
 
+
+#if defined(TCS_TB) && TCS_DIM == 2
+// ---- tcs_tb2: two sweeps in one pass over HBM (temporal blocking, 2D) -------------------------
+// Runs on the coarsening-1 instance of a parameter set.  A CTA loads an input tile of
+// (TB_TY + 4R) x (TB_TX + 4R) points into shared memory, computes the first sweep on the
+// (TB_TY + 2R) x (TB_TX + 2R) points around its outputs into a second tile -- interior points
+// with the stencil, every other point keeps its input value (the fixed border, as in the second
+// buffer of a ping-pong pair) -- and the second sweep of its TB_TY x TB_TX outputs from that.
+// Each point's terms are summed in the reference's order by the same tile arithmetic, so
+// out = S(S(in)) bit for bit; `out` needs in's border (the ping-pong invariant).
+constexpr int TB_TX = 128, TB_TY = 32, TB_THREADS = 256;
+
+extern "C" __global__ void __launch_bounds__(TB_THREADS)
+    tcs_tb2(const T* __restrict__ in, T* __restrict__ out, const TcsGeo g) {
+  using namespace tcs;
+  static_assert(CX == 1 && CY == 1, "tcs_tb2 runs on the coarsening-1 instance");
+  extern __shared__ __align__(16) unsigned char tb_smem[];
+  constexpr int AW = TB_TX + 4 * R, AH = TB_TY + 4 * R;  // input tile
+  constexpr int BW = TB_TX + 2 * R, BH = TB_TY + 2 * R;  // first-sweep tile
+  T* A = reinterpret_cast<T*>(tb_smem);
+  T* Bt = A + AW * AH;
+  constexpr T c = T(1) / T(S);
+  const tcs_i64 xdim = (tcs_i64)g.xdim, ydim = (tcs_i64)g.ydim;
+  const tcs_i64 xs = (tcs_i64)g.x0 + (tcs_i64)blockIdx.x * TB_TX;  // first output column
+  const tcs_i64 ys = (tcs_i64)R + (tcs_i64)blockIdx.y * TB_TY;     // first output row
+  for (int q = threadIdx.x; q < AW * AH; q += TB_THREADS) {
+    const int r = q / AW, cc = q - r * AW;
+    const tcs_i64 gy = ys - 2 * R + r, gx = xs - 2 * R + cc;
+    A[q] = (gy >= 0 && gy < ydim && gx >= 0 && gx < xdim) ? __ldg(in + gy * xdim + gx) : T(0);
+  }
+  __syncthreads();
+  for (int q = threadIdx.x; q < BW * BH; q += TB_THREADS) {
+    const int r = q / BW, cc = q - r * BW;
+    const tcs_i64 gy = ys - R + r, gx = xs - R + cc;
+    const T* p = A + (r + R) * AW + (cc + R);
+    if (gx >= (tcs_i64)g.x0 && gx < (tcs_i64)g.x_lim && gy >= R && gy < (tcs_i64)g.y_lim) {
+      auto ld = [&](int dx, int dy, int) { return p[dx + dy * AW]; };
+      Acc acc[NE];
+      traverse(ld, acc);
+      Bt[q] = (COEFF == 0) ? acc_value(acc[0]) * c : acc_value(acc[0]);
+    } else {
+      Bt[q] = *p;  // not swept: keeps its value
+    }
+  }
+  __syncthreads();
+  for (int q = threadIdx.x; q < TB_TX * TB_TY; q += TB_THREADS) {
+    const int r = q / TB_TX, cc = q - r * TB_TX;
+    const tcs_i64 gy = ys + r, gx = xs + cc;
+    if (gx < (tcs_i64)g.x_lim && gy < (tcs_i64)g.y_lim) {
+      const T* p = Bt + (r + R) * BW + (cc + R);
+      auto ld = [&](int dx, int dy, int) { return p[dx + dy * BW]; };
+      Acc acc[NE];
+      traverse(ld, acc);
+      out[gy * xdim + gx] = (COEFF == 0) ? acc_value(acc[0]) * c : acc_value(acc[0]);
+    }
+  }
+}
+#endif
+
 // ---- tcs_init: the reference's initial pattern -----------------------------------------------
 // 2D: border columns x < R (right of the Write left offset) and rows y < R are 1.0, else 0.0
 // (cuda/generate2DStencil_cuda.py:321-350).  3D: those and planes z < R are 0.75 / 0.25 by the

@@ -145,6 +145,14 @@ class Stencil:
                                                     ctypes.byref(launch.to_c()), _ptr(src), _ptr(source),
                                                     _ptr(dst), _stream(stream)))
 
+    def sweeps_tb2(self, geom: Geometry, a, b, n: int, stream=None):
+        """n ping-pong sweeps starting from a with temporal blocking (2D: two sweeps per pass over
+        HBM, bit-identical to n ordinary sweeps); returns the buffer holding the result."""
+        in_b = ctypes.c_int()
+        _lib.check(self._lib.tcs_sweeps_tb2(self._h, _lib.U3(*geom.grid), geom.right_offset, _ptr(a), _ptr(b),
+                                            int(n), _stream(stream), ctypes.byref(in_b)))
+        return b if in_b.value else a
+
     def tc_update_grid(self, geom: Geometry, src, dst, source=None, stream=None) -> None:
         """One FP32 sweep dst = stencil(src) (+ source) on the tensor cores (2D Box only; BF16
         hi/lo split, FP32 accumulation: a precision option, not the reference's bits)."""
@@ -216,6 +224,13 @@ def precompile_pipe(spec: StencilSpec, block, chunk: int) -> str:
     buf = ctypes.create_string_buffer(1024)
     b = tuple(block) + (1,) * (3 - len(block))
     _lib.check(_lib.load().tcs_precompile_pipe(ctypes.byref(spec.to_c()), b[0], b[1], int(chunk), buf, 1024))
+    return buf.value.decode()
+
+
+def precompile_fringe(spec: StencilSpec) -> str:
+    """Instantiate the coarsening-1 instance of ``spec`` (ragged fringe, temporal blocking)."""
+    buf = ctypes.create_string_buffer(1024)
+    _lib.check(_lib.load().tcs_precompile_fringe(ctypes.byref(spec.to_c()), buf, 1024))
     return buf.value.decode()
 
 
