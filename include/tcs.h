@@ -285,8 +285,8 @@ int tcs_precompile_batch(const tcs_spec* spec, unsigned bx, unsigned by, unsigne
  * *result_in_b tells which buffer holds the result. */
 int tcs_sweeps_tb2(tcs_stencil* h, const unsigned grid[3], unsigned right_offset, void* a, void* b,
                    unsigned n, void* stream, int* result_in_b);
-/* Instantiate the coarsening-1 instance of a parameter set (fringe of ragged grids, temporal
- * blocking) into the cubin cache (NVRTC only). */
+/* Instantiate the coarsening-1 instance of a parameter set (fringe of ragged grids) and, for 2D
+ * sets, the 1 x 8 temporal-blocking instance into the cubin cache (NVRTC only). */
 int tcs_precompile_fringe(const tcs_spec* spec, char* cubin_path, unsigned path_cap);
 
 /* ---- Tensor-core sweep of 2D Box stencils on FP32 grids (no counterpart in the reference, which

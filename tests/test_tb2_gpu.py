@@ -14,6 +14,8 @@ CASES = [
     ((2, "Star", "Column", "Variable", 2, 1, 2, 1, "Write", 8), "f64", (261, 180), False),
     ((2, "Box", "Row", "Variable", 6, 4, 1, 1, "None", 0), "f32", (400, 333), False),
     ((2, "Box", "Row", "Variable", 3, 4, 3, 1, "None", 0), "f64", (103, 77), True),
+    ((2, "Star", "Row", "Jacobi", 8, 1, 1, 1, "None", 0), "f64", (291, 170), True),
+    ((2, "Box", "Column", "Jacobi", 1, 2, 2, 1, "None", 0), "f32", (7, 5), False),
 ]
 
 

@@ -358,9 +358,11 @@ struct tcs_stencil {
   void* tc_bops = nullptr;                // tensor-core Toeplitz operands (built from mask_host)
   CUmodule fringe_mod = nullptr;          // coarsening-1 instance for the ragged fringe of a grid
   CUfunction f_fringe = nullptr;
-  CUfunction f_tb2 = nullptr;             // two sweeps per pass (2D, same instance)
-  int tb2_smem_attr = 0;
   CUdeviceptr fringe_mask = 0;
+  CUmodule tb_mod = nullptr;              // 1 x 8 instance with tcs_tb2: two sweeps per pass (2D)
+  CUfunction f_tb2 = nullptr;
+  int tb2_smem_attr = 0;
+  CUdeviceptr tb_mask = 0;
   bool tc_stale = true;                   // mask changed since tc_bops was built
   std::mutex mu;
   std::vector<MapEntry> maps;
@@ -854,7 +856,6 @@ int tensor_map(tcs_stencil* h, const void* ptr, const Resolved& r, CUtensorMap**
 }
 
 // ---- ragged grids --------------------------------------------------------------------------
-// (The coarsening-1 instance also carries tcs_tb2 for 2D parameter sets: two sweeps per pass.)
 // Every kernel updates whole coarsening tiles only, like the reference's.  When the interior is
 // not a multiple of the coarsening (a grid from tcs_compute_geometry_ragged), the points of the
 // partial tiles -- the fringe -- are swept by a second instance of the direct kernel with
@@ -866,15 +867,13 @@ int fringe_module(tcs_stencil* h) {
   tcs_spec s1 = h->spec;
   s1.cx = s1.cy = s1.cz = 1;
   std::vector<char> cubin;
-  const bool d2 = s1.dimension == 2;
-  int rc = instantiate(s1, nullptr, cubin, nullptr, d2 ? "#define TCS_TB 1\n" : nullptr);
+  int rc = instantiate(s1, nullptr, cubin, nullptr);
   if (rc) return rc;
   CUmodule mod = nullptr;
   CUresult cr = g_drv.ModuleLoadData(&mod, cubin.data());
   if (cr != CUDA_SUCCESS) return fail(TCS_ERR_CUDA, "cuModuleLoadData (fringe): " + cu_msg(cr));
   size_t bytes = 0;
   if ((cr = g_drv.ModuleGetFunction(&h->f_fringe, mod, "tcs_direct")) != CUDA_SUCCESS ||
-      (d2 && (cr = g_drv.ModuleGetFunction(&h->f_tb2, mod, "tcs_tb2")) != CUDA_SUCCESS) ||
       (cr = g_drv.ModuleGetGlobal(&h->fringe_mask, &bytes, mod, "tcs_mask")) != CUDA_SUCCESS) {
     g_drv.ModuleUnload(mod);
     return fail(TCS_ERR_CUDA, "fringe module symbols: " + cu_msg(cr));
@@ -1108,6 +1107,7 @@ int tcs_create(const tcs_spec* spec, tcs_stencil** out) {
 int tcs_destroy(tcs_stencil* h) {
   if (!h) return TCS_OK;
   if (h->fringe_mod && g_drv.ModuleUnload) g_drv.ModuleUnload(h->fringe_mod);
+  if (h->tb_mod && g_drv.ModuleUnload) g_drv.ModuleUnload(h->tb_mod);
   if (h->scratch) cudaFree(h->scratch);
   if (h->tc_bops) cudaFree(h->tc_bops);
   for (PipeMod* p : h->pipes) {
@@ -1140,6 +1140,7 @@ int tcs_copy_mask(tcs_stencil* h, const double* mask, unsigned n) {
     if (rc) return rc;
   }
   if (h->fringe_mod && (rc = upload_mask(h, h->fringe_mask))) return rc;
+  if (h->tb_mod && (rc = upload_mask(h, h->tb_mask))) return rc;
   TCS_RT(cudaDeviceSynchronize());
   return TCS_OK;
 }
@@ -1944,12 +1945,46 @@ int tcs_tc_update_grid(tcs_stencil* h, const unsigned grid[3], unsigned right_of
 
 namespace {
 
-constexpr unsigned TB_TX = 128, TB_TY = 32;
+// The tile sizes match tcs_tb2's constants.  Thread tile 1 x 8: a warp reads 32 consecutive points
+// of a row (no bank conflicts) and each value loaded serves up to 8 outputs of a column.
+constexpr unsigned TB_TX = 128, TB_CX = 1, TB_CY = 8, TB_THREADS = 256;
+unsigned tb_ty(unsigned es) { return 256 / es; }  // tile rows: 32 FP64, 64 FP32
+
+// A parameter set's 2D spec with the TB thread tile; every other parameter as given.
+tcs_spec tb_spec(const tcs_spec& s) {
+  tcs_spec t = s;
+  t.cx = TB_CX;
+  t.cy = TB_CY;
+  t.cz = 1;
+  return t;
+}
+
+int tb_module(tcs_stencil* h) {
+  std::lock_guard<std::mutex> lock(h->mu);
+  if (h->tb_mod) return TCS_OK;
+  std::vector<char> cubin;
+  int rc = instantiate(tb_spec(h->spec), nullptr, cubin, nullptr, "#define TCS_TB 1\n");
+  if (rc) return rc;
+  CUmodule mod = nullptr;
+  CUresult cr = g_drv.ModuleLoadData(&mod, cubin.data());
+  if (cr != CUDA_SUCCESS) return fail(TCS_ERR_CUDA, "cuModuleLoadData (tb2): " + cu_msg(cr));
+  size_t bytes = 0;
+  if ((cr = g_drv.ModuleGetFunction(&h->f_tb2, mod, "tcs_tb2")) != CUDA_SUCCESS ||
+      (cr = g_drv.ModuleGetGlobal(&h->tb_mask, &bytes, mod, "tcs_mask")) != CUDA_SUCCESS) {
+    g_drv.ModuleUnload(mod);
+    return fail(TCS_ERR_CUDA, "tb2 module symbols: " + cu_msg(cr));
+  }
+  h->tb_mod = mod;
+  return upload_mask(h, h->tb_mask);
+}
 
 int launch_tb2(tcs_stencil* h, const TcsGeo& g, const void* in, void* out, CUstream st) {
   const unsigned R = (unsigned)h->spec.range;
   const unsigned es = (unsigned)elem_size(h->spec);
-  const unsigned smem = ((TB_TX + 4 * R) * (TB_TY + 4 * R) + (TB_TX + 2 * R) * (TB_TY + 2 * R)) * es;
+  // first-sweep tile rounded up to whole thread tiles, input tile R wider on each side
+  const unsigned TB_TY = tb_ty(es);
+  const unsigned bw = cdiv(TB_TX + 2 * R, TB_CX) * TB_CX, bh = cdiv(TB_TY + 2 * R, TB_CY) * TB_CY;
+  const unsigned smem = ((bw + 2 * R) * (bh + 2 * R) + bw * bh) * es;
   if (smem > (unsigned)h->smem_optin) return fail(TCS_ERR_UNSUPPORTED, "tb2: tile does not fit in shared memory");
   {
     std::lock_guard<std::mutex> lock(h->mu);
@@ -1964,7 +1999,7 @@ int launch_tb2(tcs_stencil* h, const TcsGeo& g, const void* in, void* out, CUstr
   CUdeviceptr pin = (CUdeviceptr)in, pout = (CUdeviceptr)out;
   TcsGeo geo = g;
   void* args[] = {&pin, &pout, &geo};
-  TCS_CU(g_drv.LaunchKernel(h->f_tb2, gx, gy, 1, 256, 1, 1, smem, st, args, nullptr));
+  TCS_CU(g_drv.LaunchKernel(h->f_tb2, gx, gy, 1, TB_THREADS, 1, 1, smem, st, args, nullptr));
   return TCS_OK;
 }
 
@@ -1980,7 +2015,7 @@ int tcs_sweeps_tb2(tcs_stencil* h, const unsigned grid[3], unsigned right_offset
   TcsGeo g;
   int rc = make_geo(h, grid, right_offset, g);
   if (rc) return rc;
-  if ((rc = fringe_module(h))) return rc;
+  if ((rc = tb_module(h))) return rc;
   void* src = a;
   void* dst = b;
   for (unsigned i = 0; i + 1 < n; i += 2) {  // pairs of sweeps, one pass each
@@ -2011,7 +2046,9 @@ extern "C" int tcs_precompile_fringe(const tcs_spec* spec, char* cubin_path, uns
   s1.cx = s1.cy = s1.cz = 1;
   std::vector<char> cubin;
   std::string path;
-  if ((rc = instantiate(s1, nullptr, cubin, &path, s1.dimension == 2 ? "#define TCS_TB 1\n" : nullptr))) return rc;
+  if ((rc = instantiate(s1, nullptr, cubin, &path))) return rc;
+  if (s1.dimension == 2 && (rc = instantiate(tb_spec(*spec), nullptr, cubin, nullptr, "#define TCS_TB 1\n")))
+    return rc;
   if (cubin_path && path_cap) {
     std::strncpy(cubin_path, path.c_str(), path_cap - 1);
     cubin_path[path_cap - 1] = '\0';

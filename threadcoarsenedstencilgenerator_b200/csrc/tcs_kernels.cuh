@@ -381,58 +381,76 @@ extern "C" __global__ void tcs_march(const __grid_constant__ TcsTmaMap tmap,
 
 #if defined(TCS_TB) && TCS_DIM == 2
 // ---- tcs_tb2: two sweeps in one pass over HBM (temporal blocking, 2D) -------------------------
-// Runs on the coarsening-1 instance of a parameter set.  A CTA loads an input tile of
-// (TB_TY + 4R) x (TB_TX + 4R) points into shared memory, computes the first sweep on the
-// (TB_TY + 2R) x (TB_TX + 2R) points around its outputs into a second tile -- interior points
+// Runs on an instance with coarsening CX x CY = 1 x 8 (the thread tile; independent of the
+// caller's coarsening).  A CTA loads an input tile into shared memory, computes the first sweep on
+// the region of TB_TY x TB_TX outputs plus a range-wide halo into a second tile -- interior points
 // with the stencil, every other point keeps its input value (the fixed border, as in the second
-// buffer of a ping-pong pair) -- and the second sweep of its TB_TY x TB_TX outputs from that.
-// Each point's terms are summed in the reference's order by the same tile arithmetic, so
-// out = S(S(in)) bit for bit; `out` needs in's border (the ping-pong invariant).
-constexpr int TB_TX = 128, TB_TY = 32, TB_THREADS = 256;
+// buffer of a ping-pong pair) -- and then the second sweep of its outputs from that.  Both stages
+// run the tile arithmetic on CX x CY thread tiles, so every footprint value read from shared
+// memory serves all the outputs it touches.  The per-point term order does not depend on the
+// tile, so out = S(S(in)) bit for bit; `out` needs in's border (the ping-pong invariant).
+constexpr int TB_TX = 128, TB_TY = 256 / (int)sizeof(T), TB_THREADS = 256;  // TB_TY: 32 FP64, 64 FP32
 
 extern "C" __global__ void __launch_bounds__(TB_THREADS)
     tcs_tb2(const T* __restrict__ in, T* __restrict__ out, const TcsGeo g) {
   using namespace tcs;
-  static_assert(CX == 1 && CY == 1, "tcs_tb2 runs on the coarsening-1 instance");
+  static_assert(TB_TX % CX == 0 && TB_TY % CY == 0, "output tile is a multiple of the thread tile");
   extern __shared__ __align__(16) unsigned char tb_smem[];
-  constexpr int AW = TB_TX + 4 * R, AH = TB_TY + 4 * R;  // input tile
-  constexpr int BW = TB_TX + 2 * R, BH = TB_TY + 2 * R;  // first-sweep tile
+  constexpr int BW = (TB_TX + 2 * R + CX - 1) / CX * CX;  // first-sweep tile (rounded to thread tiles)
+  constexpr int BH = (TB_TY + 2 * R + CY - 1) / CY * CY;
+  constexpr int AW = BW + 2 * R, AH = BH + 2 * R;         // input tile
   T* A = reinterpret_cast<T*>(tb_smem);
   T* Bt = A + AW * AH;
   constexpr T c = T(1) / T(S);
   const tcs_i64 xdim = (tcs_i64)g.xdim, ydim = (tcs_i64)g.ydim;
   const tcs_i64 xs = (tcs_i64)g.x0 + (tcs_i64)blockIdx.x * TB_TX;  // first output column
   const tcs_i64 ys = (tcs_i64)R + (tcs_i64)blockIdx.y * TB_TY;     // first output row
+  // Input tile through the async copy unit: every thread issues all its copies before waiting, so
+  // the whole tile is in flight at once; points outside the grid read as zero.
+  const tcs_u32 a_s = (tcs_u32)__cvta_generic_to_shared(A);
   for (int q = threadIdx.x; q < AW * AH; q += TB_THREADS) {
     const int r = q / AW, cc = q - r * AW;
     const tcs_i64 gy = ys - 2 * R + r, gx = xs - 2 * R + cc;
-    A[q] = (gy >= 0 && gy < ydim && gx >= 0 && gx < xdim) ? __ldg(in + gy * xdim + gx) : T(0);
+    const bool inside = gy >= 0 && gy < ydim && gx >= 0 && gx < xdim;
+    cp_async_elem(a_s + (tcs_u32)q * (tcs_u32)sizeof(T), in + (inside ? gy * xdim + gx : 0),
+                  inside ? (tcs_u32)sizeof(T) : 0u);
+  }
+  cp_async_wait_all();
+  __syncthreads();
+  constexpr int NT1 = (BW / CX) * (BH / CY);
+  for (int t = threadIdx.x; t < NT1; t += TB_THREADS) {
+    const int r0 = (t / (BW / CX)) * CY, c0 = (t % (BW / CX)) * CX;  // first-sweep tile coordinates
+    const T* p = A + (r0 + R) * AW + (c0 + R);
+    auto ld = [&](int dx, int dy, int) { return p[dx + dy * AW]; };
+    Acc acc[NE];
+    traverse(ld, acc);
+    static_for<0, CY>([&](auto ey) {
+      static_for<0, CX>([&](auto ex) {
+        constexpr int e = decltype(ex)::value + decltype(ey)::value * CX;
+        const tcs_i64 gy = ys - R + r0 + decltype(ey)::value, gx = xs - R + c0 + decltype(ex)::value;
+        const bool interior = gx >= (tcs_i64)g.x0 && gx < (tcs_i64)g.x_lim && gy >= R && gy < (tcs_i64)g.y_lim;
+        const T v = (COEFF == 0) ? acc_value(acc[e]) * c : acc_value(acc[e]);
+        Bt[(r0 + decltype(ey)::value) * BW + c0 + decltype(ex)::value] =
+            interior ? v : p[decltype(ex)::value + decltype(ey)::value * AW];  // not swept: keeps its value
+      });
+    });
   }
   __syncthreads();
-  for (int q = threadIdx.x; q < BW * BH; q += TB_THREADS) {
-    const int r = q / BW, cc = q - r * BW;
-    const tcs_i64 gy = ys - R + r, gx = xs - R + cc;
-    const T* p = A + (r + R) * AW + (cc + R);
-    if (gx >= (tcs_i64)g.x0 && gx < (tcs_i64)g.x_lim && gy >= R && gy < (tcs_i64)g.y_lim) {
-      auto ld = [&](int dx, int dy, int) { return p[dx + dy * AW]; };
-      Acc acc[NE];
-      traverse(ld, acc);
-      Bt[q] = (COEFF == 0) ? acc_value(acc[0]) * c : acc_value(acc[0]);
-    } else {
-      Bt[q] = *p;  // not swept: keeps its value
-    }
-  }
-  __syncthreads();
-  for (int q = threadIdx.x; q < TB_TX * TB_TY; q += TB_THREADS) {
-    const int r = q / TB_TX, cc = q - r * TB_TX;
-    const tcs_i64 gy = ys + r, gx = xs + cc;
-    if (gx < (tcs_i64)g.x_lim && gy < (tcs_i64)g.y_lim) {
-      const T* p = Bt + (r + R) * BW + (cc + R);
-      auto ld = [&](int dx, int dy, int) { return p[dx + dy * BW]; };
-      Acc acc[NE];
-      traverse(ld, acc);
-      out[gy * xdim + gx] = (COEFF == 0) ? acc_value(acc[0]) * c : acc_value(acc[0]);
-    }
+  constexpr int NT2 = (TB_TX / CX) * (TB_TY / CY);
+  for (int t = threadIdx.x; t < NT2; t += TB_THREADS) {
+    const int r0 = (t / (TB_TX / CX)) * CY, c0 = (t % (TB_TX / CX)) * CX;  // output tile coordinates
+    const T* p = Bt + (r0 + R) * BW + (c0 + R);
+    auto ld = [&](int dx, int dy, int) { return p[dx + dy * BW]; };
+    Acc acc[NE];
+    traverse(ld, acc);
+    static_for<0, CY>([&](auto ey) {
+      static_for<0, CX>([&](auto ex) {
+        constexpr int e = decltype(ex)::value + decltype(ey)::value * CX;
+        const tcs_i64 gy = ys + r0 + decltype(ey)::value, gx = xs + c0 + decltype(ex)::value;
+        if (gx < (tcs_i64)g.x_lim && gy < (tcs_i64)g.y_lim)
+          out[gy * xdim + gx] = (COEFF == 0) ? acc_value(acc[e]) * c : acc_value(acc[e]);
+      });
+    });
   }
 }
 #endif

@@ -228,7 +228,8 @@ def precompile_pipe(spec: StencilSpec, block, chunk: int) -> str:
 
 
 def precompile_fringe(spec: StencilSpec) -> str:
-    """Instantiate the coarsening-1 instance of ``spec`` (ragged fringe, temporal blocking)."""
+    """Instantiate the coarsening-1 instance of ``spec`` (ragged fringe) and, in 2D, the 1 x 8
+    temporal-blocking instance."""
     buf = ctypes.create_string_buffer(1024)
     _lib.check(_lib.load().tcs_precompile_fringe(ctypes.byref(spec.to_c()), buf, 1024))
     return buf.value.decode()
