@@ -4,9 +4,11 @@ Default workload: 3D Star Variable stencil, range 4 (25 points), FP64, 512^3 gri
 16 points, seeded synthetic data (numpy default_rng; mask N(0,1) normalised to sum 1, values
 U[0,1)).  A step is one sweep of the whole grid; `value` is the whole-job GLup/s (interior points
 x steps / device time, max over ranks), with both 1 GiB buffers resident in HBM (inputs larger than
-L2, so no flush is needed between sweeps).  `e2e` runs the reference's job shape through the
-public Python API with host buffers: upload the grid from pinned memory, the workload's sweeps,
-download the result, timed with CUDA events around all of it.
+L2, so no flush is needed between sweeps).  `e2e` runs the reference's job shape through the C
+ABI's host-buffer call (tcs_sweep_host_jobs): each job uploads the grid from pinned memory, runs
+the workload's sweeps and downloads the result; --e2e-steps jobs rotate over 3 device slots so
+uploads, sweeps and downloads of different jobs overlap (`serial_value`: the same jobs on one
+slot), timed with CUDA events joined across the slots' streams.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--workload NAME] [--impl ours|reference]
 
@@ -296,25 +298,31 @@ def run_ours(args) -> dict | None:
                     "vs_single_sweep_kernel": tb_glups / (geom.interior_points * args.steps / (ms / 1e3) / 1e9),
                     "method": "tcs_sweeps_tb2: two sweeps per pass over HBM, bit-identical results"}
 
-    # e2e: the reference's job shape through the public API with host buffers
+    # e2e: the reference's job shape (upload a grid from pinned host memory, w.sweeps sweeps,
+    # download the result) through the C ABI's host-buffer entry point, e2e_steps jobs per step.
+    # Jobs rotate over 3 device slots with a stream each, so one job's upload, another's sweeps and
+    # a third's download overlap; the serial figure runs the same jobs on one slot.  Device time
+    # from CUDA events joined across the slots' streams, max over ranks.
     e2e_steps = max(1, args.e2e_steps)
-    out_host = torch.empty_like(host).pin_memory()
-    torch.cuda.synchronize()
-    f0 = torch.cuda.Event(enable_timing=True)
-    f1 = torch.cuda.Event(enable_timing=True)
-    f0.record(stream)
-    for _ in range(e2e_steps):
-        x.copy_(host, non_blocking=True)
-        y.copy_(x)  # both buffers carry the fixed border
-        res = st.sweeps(geom, x, y, w.sweeps, launch, stream)
-        out_host.copy_(res, non_blocking=True)
-    f1.record(stream)
-    torch.cuda.synchronize()
-    e2e_ms = f0.elapsed_time(f1)
-    te = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
-    if dist:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e_value = world * points * w.sweeps * e2e_steps / (float(te.item()) / 1e3) / 1e9
+    slots = min(3, e2e_steps)
+    outs = [torch.empty_like(host).pin_memory() for _ in range(slots)]
+    dev = [(x, y)] + [(torch.empty_like(x), torch.empty_like(x)) for _ in range(slots - 1)]
+    jobs_in = [host] * e2e_steps
+    jobs_out = [outs[j % slots] for j in range(e2e_steps)]
+
+    def _e2e(nslot):
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        out_ = jobs_out if nslot > 1 else [outs[0]] * e2e_steps
+        ms_ = st.sweep_host_jobs(geom, jobs_in, out_, w.sweeps, launch, dev=dev[:nslot])
+        te_ = torch.tensor([ms_], dtype=torch.float64, device="cuda")
+        if dist:
+            dist.all_reduce(te_, op=dist.ReduceOp.MAX)
+        return world * points * w.sweeps * e2e_steps / (float(te_.item()) / 1e3) / 1e9
+
+    e2e_value = _e2e(slots)
+    e2e_serial = _e2e(1)
     nbytes = host.numel() * host.element_size()
 
     ref_gpu = None
@@ -360,7 +368,9 @@ def run_ours(args) -> dict | None:
                      if peak_kind == "measured" else "fallback 6.65 TB/s",
                      "algorithmic_bytes_per_launch": bytes_per_launch},
         "e2e": {"value": e2e_value, "unit": "GLup/s", "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
-                "job": "upload grid, %d sweeps, download result (per step)" % w.sweeps, "steps": e2e_steps},
+                "job": "upload grid, %d sweeps, download result (per step)" % w.sweeps, "steps": e2e_steps,
+                "api": "tcs_sweep_host_jobs (C ABI, pinned host buffers)", "slots": slots,
+                "serial_value": e2e_serial},
         "clocks": clocks,
         "cpu_baseline": cpu,
         "reference_gpu": ref_gpu,
@@ -771,7 +781,7 @@ def main() -> int:
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS) + sorted(BATCH_WORKLOADS))
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--e2e-steps", type=int, default=6)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--precision", default="f64", choices=["f64", "mixed"],
                     help="mixed: FP64 vs FP32 vs FP32 with FP64 defect correction on the workload")

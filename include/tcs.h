@@ -168,6 +168,22 @@ int tcs_time_sweeps(tcs_stencil* h, const unsigned grid[3], unsigned right_offse
                     const tcs_launch* launch, void* a, void* b, unsigned n, void* stream,
                     float* ms);
 
+/* Sweep `njobs` host-resident grids of one geometry: job j copies host_in[j] to the device, runs
+ * `n` ping-pong sweeps and copies the result to host_out[j] (no counterpart in the reference,
+ * whose host program allocates one pair of device grids and fills them on the device:
+ * cuda/benchmark.cpp:194-196).  Jobs rotate over `nslots` slots, each a pair of
+ * device buffers (dev_a[s], dev_b[s], the grid's size) with a stream of its own, so the upload
+ * of one job, the sweeps of another and the download of a third overlap; with pinned host
+ * buffers the link runs both directions at once.  Every job's result equals the same sweeps run
+ * alone, bit for bit.  host_out buffers must not overlap any host_in, nor each other unless the
+ * two jobs share a slot (j = j' mod nslots: their downloads run in order).  Returns after every
+ * job's download completed; *ms (may be NULL) = device time from the first upload's start to the
+ * last download's end, measured with CUDA events joined across the slots' streams. */
+int tcs_sweep_host_jobs(tcs_stencil* h, const unsigned grid[3], unsigned right_offset,
+                        const tcs_launch* launch, const void* const* host_in, void* const* host_out,
+                        unsigned njobs, unsigned n, void* const* dev_a, void* const* dev_b,
+                        unsigned nslots, float* ms);
+
 /* benchmarkUpdateGrid (cuda/launchUpdateGrid.h:13, cuda/generateLaunchUpdateGrid.py:103-147):
  * runtime sanity check of the baked-in parameters, then the doubling loop of synchronous
  * launches with host timestamps.  Writes up to `cap` per-launch durations [s]; *n_out is the

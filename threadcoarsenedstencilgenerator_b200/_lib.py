@@ -120,6 +120,8 @@ SIGNATURES = {
     "tcs_update_grid": [_vp, U3, _u, _P(CLaunch), _vp, _vp, _vp],
     "tcs_sweeps": [_vp, U3, _u, _P(CLaunch), _vp, _vp, _u, _vp, _P(_i)],
     "tcs_time_sweeps": [_vp, U3, _u, _P(CLaunch), _vp, _vp, _u, _vp, _P(ctypes.c_float)],
+    "tcs_sweep_host_jobs": [_vp, U3, _u, _P(CLaunch), _P(_vp), _P(_vp), _u, _u, _P(_vp), _P(_vp), _u,
+                            _P(ctypes.c_float)],
     "tcs_benchmark_update_grid": [_vp, ctypes.c_char_p, ctypes.c_char_p, _u, _u, ctypes.c_char_p,
                                   ctypes.c_double, U3, U3, U3, _vp, _vp, _u, _P(ctypes.c_double), _u,
                                   _P(_u)],

@@ -1244,6 +1244,89 @@ int tcs_time_sweeps(tcs_stencil* h, const unsigned grid[3], unsigned right_offse
   return TCS_OK;
 }
 
+int tcs_sweep_host_jobs(tcs_stencil* h, const unsigned grid[3], unsigned right_offset,
+                        const tcs_launch* launch, const void* const* host_in, void* const* host_out,
+                        unsigned njobs, unsigned n, void* const* dev_a, void* const* dev_b, unsigned nslots,
+                        float* ms) {
+  if (!h || !host_in || !host_out || !dev_a || !dev_b) return fail(TCS_ERR_INVALID_VALUE, "NULL argument");
+  if (nslots < 1) return fail(TCS_ERR_INVALID_VALUE, "need at least one slot");
+  for (unsigned s = 0; s < nslots; ++s)
+    if (!dev_a[s] || !dev_b[s] || dev_a[s] == dev_b[s])
+      return fail(TCS_ERR_INVALID_VALUE, "every slot needs two distinct device buffers");
+  for (unsigned j = 0; j < njobs; ++j)
+    if (!host_in[j] || !host_out[j]) return fail(TCS_ERR_INVALID_VALUE, "NULL host buffer");
+  Resolved r;
+  int rc = resolve(h, grid, right_offset, launch, r);
+  if (rc) return rc;
+  TcsGeo g;
+  if ((rc = make_geo(h, grid, right_offset, g))) return rc;
+  const size_t bytes = (size_t)g.xdim * g.ydim * g.zdim * (size_t)elem_size(h->spec);
+  std::vector<cudaStream_t> st(nslots, nullptr);
+  std::vector<cudaEvent_t> ev(nslots + 1, nullptr);  // ev[0]: start; ev[s]: slot s done (s >= 1)
+  for (unsigned s = 0; s < nslots && rc == TCS_OK; ++s) {
+    cudaError_t e = cudaStreamCreateWithFlags(&st[s], cudaStreamNonBlocking);
+    if (e != cudaSuccess) rc = fail(TCS_ERR_CUDA, std::string("cudaStreamCreateWithFlags: ") + cudaGetErrorString(e));
+  }
+  for (unsigned k = 0; k <= nslots && rc == TCS_OK; ++k) {
+    cudaError_t e = cudaEventCreateWithFlags(&ev[k], k == 0 ? cudaEventDefault : cudaEventDisableTiming);
+    if (e != cudaSuccess) rc = fail(TCS_ERR_CUDA, std::string("cudaEventCreate: ") + cudaGetErrorString(e));
+  }
+  cudaEvent_t end = nullptr;
+  if (rc == TCS_OK && cudaEventCreate(&end) != cudaSuccess) rc = fail(TCS_ERR_CUDA, "cudaEventCreate failed");
+  // Device-side timing across the slots: every slot stream starts after ev[0] on slot 0, and slot 0
+  // records `end` after waiting for every other slot's last download.
+  if (rc == TCS_OK) {
+    cudaEventRecord(ev[0], st[0]);
+    for (unsigned s = 1; s < nslots; ++s) cudaStreamWaitEvent(st[s], ev[0], 0);
+  }
+  // Job j runs on slot j % nslots: upload, the border copy into b (the ping-pong invariant), n
+  // sweeps, download -- all ordered on the slot's stream, so the slot's buffers are reused only
+  // after its previous job's download has been issued behind them.
+  for (unsigned j = 0; j < njobs && rc == TCS_OK; ++j) {
+    const unsigned s = j % nslots;
+    cudaError_t e = cudaMemcpyAsync(dev_a[s], host_in[j], bytes, cudaMemcpyHostToDevice, st[s]);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dev_b[s], dev_a[s], bytes, cudaMemcpyDeviceToDevice, st[s]);
+    if (e != cudaSuccess) {
+      rc = fail(TCS_ERR_CUDA, std::string("host job upload: ") + cudaGetErrorString(e));
+      break;
+    }
+    void* src = dev_a[s];
+    void* dst = dev_b[s];
+    for (unsigned i = 0; i < n && rc == TCS_OK; ++i) {
+      rc = launch_resolved(h, r, src, dst, (CUstream)st[s]);
+      std::swap(src, dst);
+    }
+    if (rc) break;
+    e = cudaMemcpyAsync(host_out[j], src, bytes, cudaMemcpyDeviceToHost, st[s]);
+    if (e != cudaSuccess) rc = fail(TCS_ERR_CUDA, std::string("host job download: ") + cudaGetErrorString(e));
+  }
+  if (end && st[0]) {
+    for (unsigned s = 1; s < nslots; ++s) {
+      if (!st[s] || !ev[s]) continue;
+      cudaEventRecord(ev[s], st[s]);
+      cudaStreamWaitEvent(st[0], ev[s], 0);
+    }
+    cudaEventRecord(end, st[0]);
+  }
+  for (unsigned s = 0; s < nslots; ++s) {
+    if (!st[s]) continue;
+    cudaError_t e = cudaStreamSynchronize(st[s]);
+    if (e != cudaSuccess && rc == TCS_OK) rc = fail(TCS_ERR_CUDA, std::string("host jobs: ") + cudaGetErrorString(e));
+  }
+  if (rc == TCS_OK && ms) {
+    float t = 0.f;
+    cudaError_t e = cudaEventElapsedTime(&t, ev[0], end);
+    if (e != cudaSuccess) rc = fail(TCS_ERR_CUDA, std::string("host jobs timing: ") + cudaGetErrorString(e));
+    *ms = t;
+  }
+  for (unsigned s = 0; s < nslots; ++s)
+    if (st[s]) cudaStreamDestroy(st[s]);
+  for (cudaEvent_t e : ev)
+    if (e) cudaEventDestroy(e);
+  if (end) cudaEventDestroy(end);
+  return rc;
+}
+
 int tcs_benchmark_update_grid(tcs_stencil* h, const char* coeff_type, const char* neighbourhood,
                               unsigned stencil_range, unsigned dimension, const char* alignment,
                               double max_time, const unsigned grid[3], const unsigned block[3],

@@ -137,6 +137,46 @@ class Stencil:
                                              _stream(stream), ctypes.byref(ms)))
         return ms.value
 
+    def sweep_host_jobs(self, geom: Geometry, host_in: list, host_out: list, n: int, launch: Launch | None = None,
+                        slots: int = 3, dev: list | None = None) -> float:
+        """Sweep host-resident grids: job j uploads host_in[j], runs n ping-pong sweeps and
+        downloads the result into host_out[j].  Jobs rotate over ``slots`` pairs of device
+        buffers, one stream each, so the upload, the sweeps and the download of different jobs
+        overlap (pin the host tensors for that).  ``dev`` optionally gives the slots as (a, b)
+        device tensor pairs; they are allocated here otherwise.  Returns once every result is
+        on the host; each equals the same sweeps run alone, bit for bit.  Returns the device time
+        in milliseconds from the first upload's start to the last download's end."""
+        import torch
+
+        launch = launch or Launch()
+        if len(host_in) != len(host_out):
+            raise ValueError("need one host output per host input")
+        shape = tuple(geom.shape)
+        dtype = torch.float64 if self.spec.precision == "f64" else torch.float32
+        for t in list(host_in) + list(host_out):
+            if t.device.type != "cpu" or tuple(t.shape) != shape or t.dtype != dtype or not t.is_contiguous():
+                raise ValueError("host grids must be contiguous CPU tensors of shape %s and %s" % (shape, dtype))
+        nj = len(host_in)
+        ns = len(dev) if dev is not None else max(1, min(int(slots), nj))
+        ms = ctypes.c_float()
+        outs = [int(t.data_ptr()) for t in host_out]
+        first = {}
+        for j, o in enumerate(outs):  # a host output may repeat only within one slot's jobs
+            if first.setdefault(o, j) % ns != j % ns:
+                raise ValueError("host outputs of jobs on different slots must be distinct")
+        if set(outs) & {int(t.data_ptr()) for t in host_in}:
+            raise ValueError("host outputs must be distinct from the inputs")
+        if dev is None:
+            dev = [(torch.empty(shape, dtype=dtype, device="cuda"), torch.empty(shape, dtype=dtype, device="cuda"))
+                   for _ in range(ns)]
+        arr = ctypes.c_void_p * max(1, nj)
+        sarr = ctypes.c_void_p * max(1, ns)
+        _lib.check(self._lib.tcs_sweep_host_jobs(
+            self._h, _lib.U3(*geom.grid), geom.right_offset, ctypes.byref(launch.to_c()),
+            arr(*[int(t.data_ptr()) for t in host_in]), arr(*outs), nj, int(n),
+            sarr(*[_ptr(a) for a, _ in dev]), sarr(*[_ptr(b) for _, b in dev]), ns, ctypes.byref(ms)))
+        return ms.value
+
     def update_grid_source(self, geom: Geometry, src, source, dst, launch: Launch | None = None,
                            stream=None) -> None:
         """One sweep dst = stencil(src) + source (asynchronous)."""
