@@ -7,6 +7,8 @@
         --grids 16 --sweeps 3 --precision f32
     python -m threadcoarsenedstencilgenerator_b200.profile_case --workload 2d_box_var_r6_16384x8192 \
         --grid 16384 8192 --sweeps 3 --precision f32 --tensor-cores
+    python -m threadcoarsenedstencilgenerator_b200.profile_case --workload 2d_box_jacobi_r1_4096 \
+        --grid 4096 4096 --sweeps 4 --temporal
 
 The workload's tuned launch (tuned.json) and seeded data are used.  Keep the grid above the L2
 size (126 MB per buffer) so that DRAM counters stay meaningful, and small enough for an ncu
@@ -33,6 +35,7 @@ def main(argv=None) -> int:
     ap.add_argument("--sweeps", type=int, default=3)
     ap.add_argument("--precision", default="f64", choices=["f64", "f32"])
     ap.add_argument("--tensor-cores", action="store_true", help="2D Box FP32: the tcgen05 sweep")
+    ap.add_argument("--temporal", action="store_true", help="2D: two sweeps per pass (tcs_tb2)")
     a = ap.parse_args(argv)
     if a.workload in BATCH_WORKLOADS:
         return _batch(a)
@@ -50,7 +53,9 @@ def main(argv=None) -> int:
     dt = torch.float64 if a.precision == "f64" else torch.float32
     x = torch.from_numpy(w.make_input(geom)).to("cuda", dtype=dt)
     y = x.clone()
-    for _ in range(a.sweeps):
+    if a.temporal:
+        st.sweeps_tb2(geom, x, y, a.sweeps)
+    for _ in range(0 if a.temporal else a.sweeps):
         if a.tensor_cores:
             st.tc_update_grid(geom, x, y)
         else:
