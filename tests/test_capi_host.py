@@ -118,3 +118,16 @@ def test_ragged_geometry_keeps_the_whole_interior():
     assert g.grid[0] % 16 == 0 and g.grid[0] - g.right_offset == 61
     # multiples of the coarsening: identical to the reference geometry
     assert s.geometry(64, 48, 41, ragged=True) == s.geometry(64, 48, 41)
+
+
+def test_entry_points_reject_null_handles_without_a_device():
+    """Argument checks run before any device work: a NULL handle or buffer list is an invalid value."""
+    lib = _lib.load()
+    grid = _lib.U3(64, 64, 1)
+    launch = _lib.CLaunch()
+    rc = lib.tcs_sweep_host_jobs(None, grid, 0, ctypes.byref(launch), None, None, 1, 1, None, None, 1, None)
+    assert rc == _lib.TCS_ERR_INVALID_VALUE
+    assert "NULL" in lib.tcs_last_error().decode()
+    res = ctypes.c_int()
+    rc = lib.tcs_sweeps_tb2(None, grid, 0, None, None, 2, None, ctypes.byref(res))
+    assert rc == _lib.TCS_ERR_INVALID_VALUE
