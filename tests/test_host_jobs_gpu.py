@@ -14,8 +14,9 @@ import oracle as O
 pytestmark = pytest.mark.gpu
 
 CASES = [
-    ((3, "Star", "Row", "Variable", 2, 2, 2, 1, "Read", 16), "f64", (45, 30, 24), 3),
-    ((2, "Box", "Row", "Jacobi", 1, 2, 2, 1, "None", 0), "f32", (130, 70), 2),
+    ((3, "Star", "Row", "Variable", 2, 2, 2, 1, "Read", 16), "f64", (45, 30, 24), 3, False),
+    ((2, "Box", "Row", "Jacobi", 1, 2, 2, 1, "None", 0), "f32", (130, 70), 2, False),
+    ((3, "Box", "Row", "Variable", 1, 2, 4, 1, "None", 0), "f64", (37, 23, 19), 2, True),
 ]
 
 
@@ -27,14 +28,15 @@ def tcs():
 
 
 @pytest.mark.parametrize("slots", [1, 2, 3])
-@pytest.mark.parametrize("case", CASES, ids=lambda c: "%dD_%s_%s" % (c[0][0], c[0][1], c[1]))
+@pytest.mark.parametrize("case", CASES, ids=lambda c: "%dD_%s_%s%s" % (c[0][0], c[0][1], c[1],
+                                                                         "_ragged" if c[4] else ""))
 def test_host_jobs_match_oracle(tcs, case, slots):
     import torch
 
-    cfg, prec, sides, n = case
+    cfg, prec, sides, n, ragged = case
     spec = G.spec_of(cfg, prec)
     st = tcs.Stencil(spec)
-    geom = spec.geometry(*sides)
+    geom = spec.geometry(*sides, ragged=ragged)
     dt = np.float64 if prec == "f64" else np.float32
     rng = np.random.default_rng(slots)
     mask = rng.standard_normal(spec.stencil_size) if cfg[3] == "Variable" else None
@@ -47,7 +49,9 @@ def test_host_jobs_match_oracle(tcs, case, slots):
     ms = st.sweep_host_jobs(geom, host_in, host_out, n, tcs.Launch(block=(32, 4, 1)), slots=slots)
     assert ms > 0
     assert st.device_status() == 0
-    ospec = O.make_spec(*cfg)
+    # the per-point term order does not depend on the coarsening, so a ragged grid (its partial
+    # tiles swept with coarsening 1) equals the coarsening-1 oracle
+    ospec = O.make_spec(*(cfg[:5] + ((1, 1, 1) if ragged else cfg[5:8]) + cfg[8:]))
     for a, r in zip(ins, host_out):
         assert np.array_equal(r.numpy(), O.sweeps(ospec, a, n, geom.right_offset, mask))
 
