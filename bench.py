@@ -22,7 +22,6 @@ from __future__ import annotations
 
 import argparse
 import json
-import os
 import statistics
 import subprocess
 import sys
@@ -147,10 +146,9 @@ class ClockSampler:
 
 
 def _dist():
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return world, rank, local
+    from threadcoarsenedstencilgenerator_b200 import replicas
+
+    return replicas.rank_env()
 
 
 def _traffic(workload: str):
@@ -228,13 +226,11 @@ def run_ours(args) -> dict | None:
     import threadcoarsenedstencilgenerator_b200 as tcs
     from threadcoarsenedstencilgenerator_b200.workloads import WORKLOADS
 
+    from threadcoarsenedstencilgenerator_b200 import replicas
+
     world, rank, local = _dist()
     torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import torch.distributed as dist
-
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    dist = replicas.init_group(world, "nccl")
     w = WORKLOADS[args.workload]
     spec = w.tuned_spec()
     launch = w.tuned_launch()
@@ -255,8 +251,7 @@ def run_ours(args) -> dict | None:
     torch.cuda.synchronize()
     sampler = ClockSampler(local)
     sampler.start()
-    if dist:
-        dist.barrier()
+    replicas.barrier(dist)
     torch.cuda.synchronize()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
@@ -266,18 +261,14 @@ def run_ours(args) -> dict | None:
         x, y = y, x
     e1.record(stream)
     torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
+    replicas.barrier(dist)
     ms = e0.elapsed_time(e1)
     clocks = sampler.stop()
     if st.device_status() != 0:
         raise RuntimeError("device status word set during the timed sweeps")
-    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-    if dist:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
+    ms_max = replicas.max_over_ranks(ms, dist)
     points = geom.interior_points
-    value = world * points * args.steps / (ms_max / 1e3) / 1e9
+    value = replicas.whole_job_rate(world, points * args.steps, ms_max) / 1e9
 
     # 2D: the same sweeps with temporal blocking (two sweeps per pass over HBM; same bits)
     temporal = None
@@ -312,14 +303,10 @@ def run_ours(args) -> dict | None:
 
     def _e2e(nslot):
         torch.cuda.synchronize()
-        if dist:
-            dist.barrier()
+        replicas.barrier(dist)
         out_ = jobs_out if nslot > 1 else [outs[0]] * e2e_steps
         ms_ = st.sweep_host_jobs(geom, jobs_in, out_, w.sweeps, launch, dev=dev[:nslot])
-        te_ = torch.tensor([ms_], dtype=torch.float64, device="cuda")
-        if dist:
-            dist.all_reduce(te_, op=dist.ReduceOp.MAX)
-        return world * points * w.sweeps * e2e_steps / (float(te_.item()) / 1e3) / 1e9
+        return replicas.whole_job_rate(world, points * w.sweeps * e2e_steps, replicas.max_over_ranks(ms_, dist)) / 1e9
 
     e2e_value = _e2e(slots)
     e2e_serial = _e2e(1)
@@ -331,9 +318,7 @@ def run_ours(args) -> dict | None:
         ref_gpu = reference_gpu_timing(w, geom)
         if not args.no_cpu_baseline:
             cpu = cpu_baseline(w, geom, a, mask)
-    if dist:
-        dist.barrier()
-        dist.destroy_process_group()
+    replicas.close_group(dist)
     if rank != 0:
         return None
 
@@ -553,13 +538,11 @@ def run_batch(args) -> dict | None:
     from threadcoarsenedstencilgenerator_b200.batch import BatchedSweeps
     from threadcoarsenedstencilgenerator_b200.workloads import BATCH_WORKLOADS
 
+    from threadcoarsenedstencilgenerator_b200 import replicas
+
     world, rank, local = _dist()
     torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import torch.distributed as dist
-
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    dist = replicas.init_group(world, "nccl")
     w = BATCH_WORKLOADS[args.workload]
     stream = torch.cuda.current_stream()
     ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
@@ -598,8 +581,7 @@ def run_batch(args) -> dict | None:
         if main:
             sampler = ClockSampler(local)
             sampler.start()
-            if dist:
-                dist.barrier()
+            replicas.barrier(dist)
         torch.cuda.synchronize()
         e0, e1 = ev(), ev()
         e0.record(stream)
@@ -609,8 +591,7 @@ def run_batch(args) -> dict | None:
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1)
         if main:
-            if dist:
-                dist.barrier()
+            replicas.barrier(dist)
             clocks = sampler.stop()
         if st.device_status() != 0:
             raise RuntimeError("device status word set during the timed sweeps")
@@ -633,10 +614,7 @@ def run_batch(args) -> dict | None:
             "depth": plan.depth,
         }
         if main:
-            t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-            if dist:
-                dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms_max = float(t.item())
+            ms_max = replicas.max_over_ranks(ms, dist)
             # e2e: every step uploads all grids from pinned memory, replays the graph, downloads
             outs = [torch.empty_like(h).pin_memory() for h in hosts]
             e2e_steps = max(1, args.e2e_steps)
@@ -652,13 +630,11 @@ def run_batch(args) -> dict | None:
                     o.copy_(r, non_blocking=True)
             f1.record(stream)
             torch.cuda.synchronize()
-            te = torch.tensor([f0.elapsed_time(f1)], dtype=torch.float64, device="cuda")
-            if dist:
-                dist.all_reduce(te, op=dist.ReduceOp.MAX)
+            te_max = replicas.max_over_ranks(f0.elapsed_time(f1), dist)
             nbytes = sum(h.numel() * h.element_size() for h in hosts)
             line_parts = {
                 "ms_max": ms_max, "points": points, "nbytes": nbytes, "plan": plan, "clocks": clocks,
-                "e2e": {"value": world * points * n * e2e_steps / (float(te.item()) / 1e3) / 1e9, "unit": "GLup/s",
+                "e2e": {"value": replicas.whole_job_rate(world, points * n * e2e_steps, te_max) / 1e9, "unit": "GLup/s",
                         "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
                         "job": "upload %d grids, %d batched sweeps (graph), download results" % (len(geoms), n),
                         "steps": e2e_steps},
@@ -676,9 +652,7 @@ def run_batch(args) -> dict | None:
         cpu = {"value": v, "unit": "GLup/s", "cores": threads, "kind": "port",
                "sample": "%d sweeps of all %d grids (%.1f s, OpenMP restatement, grid after grid)" % (
                    nsw, w.n_grids, dt)}
-    if dist:
-        dist.barrier()
-        dist.destroy_process_group()
+    replicas.close_group(dist)
     if rank != 0:
         return None
     peak, peak_kind = _peaks()
@@ -691,7 +665,7 @@ def run_batch(args) -> dict | None:
     plan = line_parts["plan"]
     return {
         "metric": "GLup/s (FP64 batched sweeps, %s)" % w.name,
-        "value": world * points * n * args.steps / (ms_max / 1e3) / 1e9,
+        "value": replicas.whole_job_rate(world, points * n * args.steps, ms_max) / 1e9,
         "unit": "GLup/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic (numpy default_rng seed %d)" % w.seed,
