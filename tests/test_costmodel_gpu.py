@@ -105,3 +105,45 @@ def test_trained_model_gains_over_choosing_without_it():
     assert r["mean_ratio_to_best"] >= 0.9
     assert r["timed_fraction"] < 0.1
     m.close()
+
+
+def test_tuner_on_a_held_out_set():
+    """The learned tuner on a held-out 2D parameter set of the corpus, at the corpus grid size:
+    it times the model's top 5 (or falls back to the sweep with the reason recorded), and its
+    block comes within reach of the exhaustive sweep's, which times every runnable candidate."""
+    import torch
+
+    from threadcoarsenedstencilgenerator_b200 import Stencil
+    from threadcoarsenedstencilgenerator_b200.autotune import (CORPUS_PATH, MODEL_PATH, Autotuner, CostModel,
+                                                               _alloc, corpus_grid, load_corpus, sample_configs,
+                                                               split, time_block)
+
+    if not (CORPUS_PATH.exists() and MODEL_PATH.exists()):
+        pytest.skip("no corpus / trained model committed yet")
+    cfg, _, _ = load_corpus()
+    hold, _ = split(cfg)
+    specs = sample_configs(400, 7)
+    cid = next(c for c in hold if specs[c].dimension == 2)
+    spec = specs[cid]
+    geom = spec.geometry(*corpus_grid(spec))
+    st = Stencil(spec)
+    if spec.coefficients == "Variable":
+        st.copy_mask(np.random.default_rng(cid).standard_normal(spec.stencil_size) / spec.stencil_size)
+    x, y = _alloc(spec, geom, cid)
+    m = CostModel.load()
+    learned = Autotuner(m).tune(st, geom, x, y)
+    full = Autotuner(None).tune(st, geom, x, y)
+    assert full.fell_back and full.reason == "no model" and full.timed == len(full.measured) >= 5
+    if learned.fell_back:  # outside the corpus's feature ranges, or the model disagreed with timings
+        assert "outside" in learned.reason or learned.model_error > 0.25
+    else:
+        assert learned.timed == 5 and learned.model_error <= 0.25
+        assert learned.block in learned.measured
+    g_l = time_block(st, geom, x, y, learned.block, 6)
+    g_f = time_block(st, geom, x, y, full.block, 6)
+    assert g_l >= 0.7 * g_f
+    assert st.device_status() == 0
+    m.close()
+    st.close()
+    del x, y
+    torch.cuda.empty_cache()

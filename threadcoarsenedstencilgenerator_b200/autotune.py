@@ -11,10 +11,11 @@ cuda/generateLaunchUpdateGrid.py:103-147).  Here
   that parameter set's candidates (the targets are centred per parameter set: ranking the blocks
   of one set needs only the differences).  It is trained and evaluated on the GPU by libtcs.so's
   own kernels (``tcs_mlp_*``);
-* ``Autotuner.tune`` ranks all candidates with the model, times only the top k, and falls back to
-  the exhaustive sweep when the model is missing, the parameter set lies outside the corpus the
+* ``Autotuner.tune`` ranks all candidates with the model, times only the top k (5), and falls back
+  to the exhaustive sweep when the model is missing, the parameter set lies outside the corpus the
   model was trained on, or the measured differences between the timed candidates disagree with the
-  predicted ones by more than a tolerance (the sweep then also records the model's error).
+  predicted ones by more than a tolerance even after the candidates are timed again over more
+  sweeps (the sweep then also records the model's error).
 
 ``python -m threadcoarsenedstencilgenerator_b200.autotune corpus|train|evaluate`` builds the
 timing corpus on a GPU, trains the model on it and reports its held-out quality.
@@ -349,7 +350,7 @@ class TuneResult:
 class Autotuner:
     """Picks the direct kernel's block for (stencil, grid): model-ranked top-k, exhaustive fallback."""
 
-    def __init__(self, model: CostModel | None = None, top_k: int = 3, tolerance: float = 0.25,
+    def __init__(self, model: CostModel | None = None, top_k: int = 5, tolerance: float = 0.25,
                  sweeps: int = 2):
         self.model = model
         self.top_k = top_k
@@ -385,8 +386,16 @@ class Autotuner:
             predicted[keep[i]] = float(pred[i])
         if not measured:
             return self._exhaustive(st, geom, x, y, keep, t0, "no predicted candidate runs")
-        best = max(measured, key=measured.get)
-        err = max(abs((predicted[b] - predicted[best]) - math.log(measured[b] / measured[best])) for b in measured)
+        best, err = self._model_error(measured, predicted)
+        if err > self.tolerance:
+            # A timing over a couple of sweeps can be off by more than the tolerance on its own:
+            # before giving up on the model, time the same candidates again over twice the sweeps
+            # and judge the model on the mean of both timings.
+            for b in list(measured):
+                g = time_block(st, geom, x, y, b, 2 * self.sweeps)
+                if g is not None:
+                    measured[b] = (measured[b] + 2.0 * g) / 3.0  # weighted by sweeps timed
+            best, err = self._model_error(measured, predicted)
         if err > self.tolerance:
             r = self._exhaustive(st, geom, x, y, keep, t0, "prediction error %.2f (log) above %.2f" % (
                 err, self.tolerance))
@@ -395,6 +404,14 @@ class Autotuner:
             return r
         return TuneResult(best, measured[best], timed, len(keep), False, time.perf_counter() - t0,
                           "model top-%d" % self.top_k, predicted, measured, err)
+
+    @staticmethod
+    def _model_error(measured: dict, predicted: dict) -> tuple:
+        """(best timed block, largest gap between the measured and the predicted log-throughput
+        difference of a timed block to the best one)."""
+        best = max(measured, key=measured.get)
+        err = max(abs((predicted[b] - predicted[best]) - math.log(measured[b] / measured[best])) for b in measured)
+        return best, err
 
     def _exhaustive(self, st, geom, x, y, blocks, t0, reason) -> TuneResult:
         res = exhaustive(st, geom, x, y, blocks, self.sweeps)
@@ -509,7 +526,7 @@ def evaluate(model: CostModel, cfg, X, y, ids, top_k: int = 3, seed: int = 3) ->
 
 
 def live(model: CostModel, ids, n_configs: int = 400, seed: int = 7, log=print) -> dict:
-    """Tune held-out parameter sets on the GPU twice -- the learned tuner (model top-3, fallback)
+    """Tune held-out parameter sets on the GPU twice -- the learned tuner (model top-5, fallback)
     and the exhaustive sweep -- and compare the chosen blocks re-timed with 10 sweeps each, and the
     wall time each method spent."""
     import torch
