@@ -89,7 +89,7 @@ def simulate(dim, shape, R, c, block, grid, left_offset, right_offset, aligned, 
         while ch * 2 <= want:
             ch *= 2
     W = pipe_width(TX, R, lshift, vec, ch, rows, es)
-    if W > 256 or rows > 256:
+    if rows > 256:  # wider rows than a TMA box stream through cp.async (single-grid sweeps)
         return None
     plane = W * rows
     CHUNK = ch * plane

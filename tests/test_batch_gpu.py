@@ -216,3 +216,33 @@ def test_fp32_pipe_loaders_match_oracle(tcs, cx, sides, offset, loader):
     assert st.device_status() == 0
     want = O.sweeps(O.make_spec(*cfg), a, 3, geom.right_offset)
     assert np.array_equal(res.cpu().numpy(), want)
+
+
+@pytest.mark.parametrize("cfg, block, sides, precision, loader", [
+    ((2, "Box", "Row", "Variable", 6, 8, 1, 1, "None", 0), (32, 1, 1), (300, 30), "f32", "cp.async pairs"),
+    ((2, "Box", "Row", "Variable", 6, 8, 1, 1, "None", 0), (32, 1, 1), (300, 30), "f64", "cp.async"),
+    ((3, "Star", "Row", "Jacobi", 2, 2, 2, 1, "Read", 16), (128, 1, 1), (290, 12, 10), "f64", "cp.async"),
+])
+def test_pipe_tiles_wider_than_a_tma_box(tcs, cfg, block, sides, precision, loader):
+    """Single-grid pipe tiles wider than a 256-element TMA box stream their rows through cp.async
+    and give the oracle's bits."""
+    import torch
+
+    spec = G.spec_of(cfg, precision)
+    st = tcs.Stencil(spec)
+    geom = spec.geometry(*sides)
+    launch = tcs.Launch(block=block, variant="pipe")
+    plan = st.plan(geom, launch)
+    assert plan.loader == loader and plan.width > 256
+    rng = np.random.default_rng(13)
+    dt = np.float64 if precision == "f64" else np.float32
+    a = rng.uniform(-1, 1, geom.shape).astype(dt)
+    mask = rng.standard_normal(spec.stencil_size) if cfg[3] == "Variable" else None
+    if mask is not None:
+        st.copy_mask(mask)
+    x = torch.from_numpy(a).cuda()
+    y = x.clone()
+    res = st.sweeps(geom, x, y, 3, launch)
+    torch.cuda.synchronize()
+    assert st.device_status() == 0
+    assert np.array_equal(res.cpu().numpy(), O.sweeps(O.make_spec(*cfg), a, 3, geom.right_offset, mask))

@@ -128,6 +128,9 @@ PIPE_CASES = [
     (3, "Star", 2, (1, 2, 1), (16, 2, 1), (31, 29, 27), "None", 0),
     (3, "Box", 1, (2, 1, 1), (8, 3, 1), (35, 26, 22), "Write", 16),
     (3, "Box", 2, (1, 1, 1), (16, 8, 1), (22, 21, 20), "None", 0),
+    # tiles wider than a 256-element TMA box (cp.async loaders)
+    (2, "Box", 6, (8, 1, 1), (32, 1, 1), (300, 30, 1), "None", 0),
+    (3, "Star", 2, (2, 2, 1), (128, 1, 1), (290, 12, 10), "Read", 16),
 ]
 
 

@@ -382,6 +382,7 @@ struct Resolved {
   unsigned depth = 0;
   unsigned box[3] = {1, 1, 1};
   int occ = 0;
+  bool no_tma = false;  // pipe: tile rows wider than one TMA box, streamed through cp.async
 };
 
 int elem_size(const tcs_spec& s) { return s.precision == TCS_F64 ? 8 : 4; }
@@ -652,12 +653,18 @@ unsigned pipe_width(unsigned tx, unsigned R, unsigned lshift, unsigned vec, unsi
 // Loader of the pipe kernel for a row pitch (and input base, when known): 0 = TMA (pitch and
 // base on 16 bytes), 2 = cp.async of element pairs (FP32 with an even pitch and an 8-byte base),
 // 1 = cp.async of single elements.
+// cp.async loaders: pairs of floats where the pitch and the base allow it, else single elements.
+unsigned pipe_loader_cp(const tcs_spec& s, unsigned long long xdim, const void* in) {
+  const uintptr_t base = reinterpret_cast<uintptr_t>(in);
+  if (elem_size(s) == 4 && xdim % 2 == 0 && base % 8 == 0) return 2u;
+  return 1u;
+}
+
 unsigned pipe_loader(const tcs_spec& s, unsigned long long xdim, const void* in) {
   const unsigned es = (unsigned)elem_size(s);
   const uintptr_t base = reinterpret_cast<uintptr_t>(in);
   if ((xdim * es) % 16 == 0 && base % 16 == 0) return 0u;
-  if (es == 4 && xdim % 2 == 0 && base % 8 == 0) return 2u;
-  return 1u;
+  return pipe_loader_cp(s, xdim, in);
 }
 
 int resolve_pipe(tcs_stencil* h, const TcsGeo& g, const tcs_launch* L, Resolved& out,
@@ -681,8 +688,12 @@ int resolve_pipe(tcs_stencil* h, const TcsGeo& g, const tcs_launch* L, Resolved&
   const unsigned lshift = h->left_off % vec;
   const unsigned ch = L->chunk ? L->chunk : pipe_auto_chunk(s, L->block[0], L->block[1]);
   const unsigned W = pipe_width(TX, R, lshift, vec, ch, rows, es);
-  if (W > 256 || rows > 256 || ch > 256)
+  // A TMA box is at most 256 elements per dimension.  A single-grid sweep that asks for the pipe
+  // kernel with wider tile rows streams them through cp.async instead (the automatic choice keeps
+  // such shapes on the march and direct kernels; the batch's table holds one tensor map per grid).
+  if (rows > 256 || ch > 256 || (W > 256 && (batch || L->variant != TCS_VARIANT_PIPE)))
     return fail(TCS_ERR_UNSUPPORTED, "pipe: tile exceeds the 256-element TMA box limit");
+  const bool no_tma = W > 256;
   const unsigned chunk_bytes = ch * rows * W * es;
   PipeKey key{L->block[0], s.dimension == 3 ? L->block[1] : 1u, ch, lshift, batch ? 1u : 0u};
   PipeMod* pm = nullptr;
@@ -747,6 +758,7 @@ int resolve_pipe(tcs_stencil* h, const TcsGeo& g, const tcs_launch* L, Resolved&
   const unsigned long long grid = std::max<unsigned long long>(1, (total + per - 1) / per);
   if (grid > 0x7fffffffull) return fail(TCS_ERR_UNSUPPORTED, "pipe grid too large");
   out.variant = TCS_VARIANT_PIPE;
+  out.no_tma = no_tma;
   out.geo = g;
   out.geo.width = W;
   out.geo.nslot = nslot;
@@ -766,7 +778,7 @@ int resolve_pipe(tcs_stencil* h, const TcsGeo& g, const tcs_launch* L, Resolved&
   pg.ntx = ntx;
   pg.m = (unsigned)M;
   pg.nslot = nslot;
-  pg.loader = pipe_loader(s, g.xdim, nullptr);
+  pg.loader = no_tma ? pipe_loader_cp(s, g.xdim, nullptr) : pipe_loader(s, g.xdim, nullptr);
   out.geo.loader = pg.loader;
   out.geo.seg = (unsigned)std::min<unsigned long long>(per, 0xffffffffull);
   out.grid[0] = (unsigned)grid;
@@ -935,7 +947,7 @@ int launch_resolved(tcs_stencil* h, const Resolved& r, const void* in, void* out
   }
   if (r.variant == TCS_VARIANT_PIPE) {
     TcsPipeGeo pg = r.pgeo;
-    pg.loader = pipe_loader(h->spec, pg.xdim, in);
+    pg.loader = r.no_tma ? pipe_loader_cp(h->spec, pg.xdim, in) : pipe_loader(h->spec, pg.xdim, in);
     alignas(64) CUtensorMap pmap;
     std::memset(&pmap, 0, sizeof(pmap));
     if (pg.loader == 0 && pre) {

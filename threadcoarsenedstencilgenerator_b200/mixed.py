@@ -36,11 +36,17 @@ class DefectCorrectedSweeps:
     """Run n sweeps of ``spec`` (FP64 semantics) as FP32 sweeps with periodic FP64 defect correction."""
 
     def __init__(self, spec: StencilSpec, launch64: Launch | None = None, launch32: Launch | None = None,
-                 mask=None, tensor_cores: bool = False):
+                 mask=None, tensor_cores: bool = False, coarsening32: tuple | None = None):
+        """``launch32`` and ``coarsening32`` give the FP32 sweeps a launch shape of their own (FP32
+        keeps twice the values per register and runs at twice the FP64 rate, so its best shape
+        differs); the per-point arithmetic does not depend on either."""
         if spec.precision != "f64":
             spec = spec.replace(precision="f64")
         self.spec64 = spec
         self.spec32 = spec.replace(precision="f32")
+        if coarsening32 is not None:
+            c = tuple(coarsening32) + (1,) * (3 - len(coarsening32))
+            self.spec32 = self.spec32.replace(cx=c[0], cy=c[1], cz=c[2] if spec.dimension == 3 else 1)
         self.s64 = Stencil(self.spec64)
         self.s32 = Stencil(self.spec32)
         if mask is not None:

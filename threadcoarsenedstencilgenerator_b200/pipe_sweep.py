@@ -34,9 +34,10 @@ def main(argv=None) -> int:
     ap.add_argument("--chunks", type=int, nargs="+", default=[2, 3])
     ap.add_argument("--sweeps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--precision", default="f64", choices=["f64", "f32"])
     a = ap.parse_args(argv)
     w = WORKLOADS[a.workload]
-    base = w.tuned_spec()
+    base = w.tuned_spec().replace(precision=a.precision)
     geom = base.geometry(*w.grid)
     dt = torch.float64 if base.precision == "f64" else torch.float32
     x = torch.from_numpy(w.make_input(geom)).to("cuda", dtype=dt)

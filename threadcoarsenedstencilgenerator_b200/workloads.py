@@ -53,20 +53,30 @@ class Workload:
             return m / m.sum()
         return m / S
 
-    def tuned_launch(self) -> Launch:
-        """Launch chosen by the autotuner for this workload (falls back to the built-in default)."""
+    def _tuned(self, precision: str):
+        if not TUNED_PATH.exists():
+            return None
+        d = json.loads(TUNED_PATH.read_text())
+        return d.get(self.name + "_" + precision) if precision != "f64" and self.name + "_" + precision in d \
+            else d.get(self.name)
+
+    def tuned_launch(self, precision: str = "f64") -> Launch:
+        """Launch chosen by the autotuner for this workload and precision (an entry
+        ``<name>_<precision>`` when the precision has its own, else the FP64 one; falls back to the
+        built-in default)."""
         if TUNED_PATH.exists():
-            t = json.loads(TUNED_PATH.read_text()).get(self.name)
+            t = self._tuned(precision)
             if t:
                 return Launch(block=tuple(t["block"]), variant=t.get("variant", "auto"),
                               segments=int(t.get("segments", 0)), depth=int(t.get("depth", 0)),
                               chunk=int(t.get("chunk", 0)))
         return self.launch
 
-    def tuned_spec(self) -> StencilSpec:
-        """Parameter set with the coarsening chosen by the autotuner (same stencil arithmetic)."""
+    def tuned_spec(self, precision: str = "f64") -> StencilSpec:
+        """Parameter set with the coarsening chosen by the autotuner for this precision (same
+        stencil arithmetic; the precision of the result is the workload's own)."""
         if TUNED_PATH.exists():
-            t = json.loads(TUNED_PATH.read_text()).get(self.name)
+            t = self._tuned(precision)
             if t and "coarsening" in t:
                 c = t["coarsening"]
                 return self.spec.replace(cx=c[0], cy=c[1], cz=c[2] if self.spec.dimension == 3 else 1)
