@@ -224,3 +224,26 @@ def test_tensor_core_operand_layouts_reproduce_the_stencil(R, left):
                 want = sum(mask2d[dy + R, dx + R] * grid[y + dy, x + dx]
                            for dy in range(-R, R + 1) for dx in range(-R, R + 1))
                 assert acc[m, n] == want, (m, n)
+
+
+@pytest.mark.parametrize("es", [8, 4])
+@pytest.mark.parametrize("shape", ["Box", "Star"])
+@pytest.mark.parametrize("R", [1, 2, 3, 6, 8])
+def test_temporal_blocking_model(R, shape, es):
+    """tcs_tb2's tiles and phases (tests/tb_model.py): every shared-memory access stays inside its
+    tile, the shared memory fits, every interior point is written once and nothing else, and one
+    pass equals two plain sweeps (integer data and weights: exact in any order).  Grids: the
+    smallest interior, ragged sizes, and Write-style left and right padding."""
+    from tb_model import footprint, plain_sweep, sweep_tb2
+
+    rng = np.random.default_rng(R * 10 + es)
+    w = {o: int(rng.integers(-3, 4)) for o in footprint(shape, R)}
+    for xdim, ydim, left, right in ((2 * R + 3, 2 * R + 2, 0, 0), (150, 45, 0, 0), (300, 81, 3, 5)):
+        x0, x_lim, y_lim = R + left, xdim - R - right, ydim - R
+        a = rng.integers(-9, 10, size=(ydim, xdim)).astype(np.int64)
+        want = plain_sweep(plain_sweep(a, R, w, x0, x_lim, y_lim), R, w, x0, x_lim, y_lim)
+        got, writes = sweep_tb2(a, shape, R, w, es, x0, x_lim, y_lim)
+        interior = np.zeros(a.shape, dtype=bool)
+        interior[R:y_lim, x0:x_lim] = True
+        assert np.all(writes[interior] == 1) and np.all(writes[~interior] == 0)
+        assert np.array_equal(got, want)
