@@ -78,3 +78,25 @@ def test_features_and_sampler():
     assert d["log_S"] == pytest.approx(math.log2(13))
     assert d["log_warps_per_sm"] == pytest.approx(math.log2(2 * 256 / 32))
     assert d["tail_efficiency"] == pytest.approx(256 / 296)
+
+
+def test_tuned_entries_per_precision(tmp_path, monkeypatch):
+    """A workload's FP32 sweeps take the `<name>_f32` entry of tuned.json when there is one, else
+    the FP64 entry; the workload's own precision is kept."""
+    import json
+
+    from threadcoarsenedstencilgenerator_b200 import workloads as W
+
+    w = W.WORKLOADS["2d_box_var_r6_16384x8192"]
+    p = tmp_path / "tuned.json"
+    p.write_text(json.dumps({w.name: {"coarsening": [4, 1, 1], "block": [32, 1, 1], "variant": "pipe", "chunk": 1}}))
+    monkeypatch.setattr(W, "TUNED_PATH", p)
+    assert w.tuned_spec("f32").coarsening == w.tuned_spec().coarsening == (4, 1, 1)
+    assert w.tuned_launch("f32").block == (32, 1, 1)
+    d = json.loads(p.read_text())
+    d[w.name + "_f32"] = {"coarsening": [8, 1, 1], "block": [64, 1, 1], "variant": "pipe", "chunk": 2}
+    p.write_text(json.dumps(d))
+    assert w.tuned_spec("f32").coarsening == (8, 1, 1)
+    assert w.tuned_spec("f32").precision == w.spec.precision
+    assert w.tuned_launch("f32").block == (64, 1, 1) and w.tuned_launch("f32").chunk == 2
+    assert w.tuned_spec().coarsening == (4, 1, 1) and w.tuned_launch().block == (32, 1, 1)
