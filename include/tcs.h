@@ -201,6 +201,15 @@ int tcs_benchmark_update_grid(tcs_stencil* h, const char* coeff_type, const char
 int tcs_launch_init(tcs_stencil* h, const unsigned grid[3], const unsigned block[3],
                     const unsigned grid_blocks[3], void* d_array, unsigned right_offset);
 
+/* Failure-detection self-test (no counterpart in the reference, whose launcher only prints CUDA
+ * errors: cuda/generateLaunchUpdateGrid.py:62-69).  One warp waits on a barrier that nothing
+ * arrives at, through the same bounded wait the sweep kernels use, for at most `cycles` clock
+ * cycles (1e3..4e9; 2e6 is about a millisecond), then records the timeout in the handle's device
+ * status word as an expired sweep wait does.  The call reads and clears the word and returns
+ * TCS_ERR_DEVICE_TIMEOUT when the timeout was recorded -- the expected outcome -- with the
+ * context still usable. */
+int tcs_self_test_wait(tcs_stencil* h, long long cycles);
+
 /* Read (and optionally clear) the device status word of the handle's kernels. */
 int tcs_device_status(tcs_stencil* h, unsigned* status, int clear);
 

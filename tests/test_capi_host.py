@@ -131,3 +131,4 @@ def test_entry_points_reject_null_handles_without_a_device():
     res = ctypes.c_int()
     rc = lib.tcs_sweeps_tb2(None, grid, 0, None, None, 2, None, ctypes.byref(res))
     assert rc == _lib.TCS_ERR_INVALID_VALUE
+    assert lib.tcs_self_test_wait(None, 2_000_000) == _lib.TCS_ERR_INVALID_VALUE

@@ -127,6 +127,7 @@ SIGNATURES = {
                                   _P(_u)],
     "tcs_launch_init": [_vp, U3, U3, U3, _vp, _u],
     "tcs_device_status": [_vp, _P(_u), _i],
+    "tcs_self_test_wait": [_vp, ctypes.c_longlong],
     "tcs_set_dropin_launch": [_vp, _i, _u, _u],
     "tcs_precompile": [_P(CSpec), ctypes.c_char_p, _u],
     "tcs_precompile_pipe": [_P(CSpec), _u, _u, _u, ctypes.c_char_p, _u],

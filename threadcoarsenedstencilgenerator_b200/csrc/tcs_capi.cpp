@@ -1423,6 +1423,20 @@ int tcs_device_status(tcs_stencil* h, unsigned* status, int clear) {
   return TCS_OK;
 }
 
+int tcs_self_test_wait(tcs_stencil* h, long long cycles) {
+  if (!h) return fail(TCS_ERR_INVALID_VALUE, "NULL handle");
+  if (cycles < 1000 || cycles > 4000000000LL)
+    return fail(TCS_ERR_INVALID_VALUE, "self-test wait budget outside [1e3, 4e9] cycles");
+  int e = tcs_field_launch_wait_probe(reinterpret_cast<unsigned*>(h->status_ptr), cycles, nullptr);
+  if (e != 0) return fail(TCS_ERR_CUDA, std::string("wait probe launch: ") + cudaGetErrorString((cudaError_t)e));
+  TCS_RT(cudaDeviceSynchronize());
+  unsigned v = 0;
+  TCS_RT(cudaMemcpy(&v, (void*)h->status_ptr, sizeof(v), cudaMemcpyDeviceToHost));
+  TCS_RT(cudaMemset((void*)h->status_ptr, 0, sizeof(unsigned)));
+  if (v & 1u) return fail(TCS_ERR_DEVICE_TIMEOUT, "bounded device wait expired (self-test)");
+  return TCS_OK;
+}
+
 int tcs_set_dropin_launch(tcs_stencil* h, int variant, unsigned segments, unsigned depth) {
   if (!h) return fail(TCS_ERR_INVALID_VALUE, "NULL handle");
   if (variant != TCS_VARIANT_AUTO && variant != TCS_VARIANT_DIRECT && variant != TCS_VARIANT_MARCH)

@@ -144,6 +144,44 @@ extern "C" int tcs_field_launch_add(double* x, const float* e, TcsFieldGeo g, in
   return (int)cudaGetLastError();
 }
 
+// ---- failure-detection self-test -----------------------------------------------------------
+// One warp waits on a shared-memory mbarrier that expects one arrival and never gets it -- the
+// wait of a sweep kernel whose copy never lands -- through the same bounded loop the kernels use:
+// after `limit` cycles it gives up, sets bit 1 (TCS_DEV_TIMEOUT) of `status` and returns.  No copy
+// is in flight and nothing else waits on the barrier, so the context stays usable.
+namespace {
+
+__global__ void __launch_bounds__(32) tcs_k_wait_probe(unsigned* status, long long limit) {
+  __shared__ __align__(8) unsigned long long bar;
+  const unsigned b = (unsigned)__cvta_generic_to_shared(&bar);
+  if (threadIdx.x == 0) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(b) : "memory");
+  __syncthreads();
+  unsigned done = 0;
+  const long long t0 = clock64();
+  bool expired = false;
+  for (;;) {
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n"
+        " selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(done)
+        : "r"(b)
+        : "memory");
+    if (done) break;
+    if (clock64() - t0 > limit) {
+      expired = true;
+      break;
+    }
+  }
+  if (__syncthreads_or(expired) && threadIdx.x == 0) atomicOr(status, 1u);
+}
+
+}  // namespace
+
+extern "C" int tcs_field_launch_wait_probe(unsigned* status, long long limit, cudaStream_t st) {
+  tcs_k_wait_probe<<<1, 32, 0, st>>>(status, limit);
+  return (int)cudaGetLastError();
+}
+
 // ---- allocation-free residual: scratch in a static device array ------------------------------
 // Some callers cannot allocate device memory at the point where they need the residual norm: a
 // framework whose caching allocator owns the device memory, a solver loop that must not pay the

@@ -226,6 +226,16 @@ class Stencil:
         _lib.check(self._lib.tcs_device_status(self._h, ctypes.byref(v), 1 if clear else 0))
         return v.value
 
+    def self_test_wait(self, cycles: int = 2_000_000) -> bool:
+        """Failure-detection self-test: a bounded device wait on a barrier nothing arrives at.
+        True when the kernel gave up after ``cycles`` and the host read the timeout from the
+        device status word (the expected outcome; the word is cleared and the context usable)."""
+        rc = self._lib.tcs_self_test_wait(self._h, int(cycles))
+        if rc == _lib.TCS_ERR_DEVICE_TIMEOUT:
+            return True
+        _lib.check(rc)
+        return False
+
     def set_dropin_launch(self, variant: str = "auto", segments: int = 0, depth: int = 0) -> None:
         _lib.check(self._lib.tcs_set_dropin_launch(self._h, Launch._VARIANTS[variant], segments, depth))
 
