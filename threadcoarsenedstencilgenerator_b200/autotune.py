@@ -390,7 +390,7 @@ class Autotuner:
         if err > self.tolerance:
             # A timing over a couple of sweeps can be off by more than the tolerance on its own:
             # before giving up on the model, time the same candidates again over twice the sweeps
-            # and judge the model on the mean of both timings.
+            # and assess the model on the mean of both timings.
             for b in list(measured):
                 g = time_block(st, geom, x, y, b, 2 * self.sweeps)
                 if g is not None:
