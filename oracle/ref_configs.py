@@ -31,6 +31,20 @@ PARITY = [
     (3, "Star", "Column", "Variable", 2, 3, 1, 2, "Read", 16),
 ]
 
+# Further parameter sets that pin the CPU oracle only (fixtures from the reference's generated
+# kernels through the host shim; no GPU test runs them): the long ranges 5-8, 3D Box beyond range 1,
+# 3D Star Column at range 4, and coarsening factors of 4 in 3D.
+EXTRA = [
+    (2, "Box", "Row", "Jacobi", 5, 1, 2, 1, "Read", 8),
+    (2, "Box", "Column", "Variable", 7, 2, 1, 1, "None", 0),
+    (2, "Star", "Row", "Variable", 8, 2, 4, 1, "Write", 16),
+    (2, "Star", "Column", "Jacobi", 6, 4, 1, 1, "Read", 16),
+    (3, "Box", "Row", "Variable", 3, 1, 2, 1, "Read", 8),
+    (3, "Box", "Column", "Jacobi", 2, 2, 1, 2, "None", 0),
+    (3, "Star", "Column", "Variable", 4, 1, 2, 2, "Write", 16),
+    (3, "Star", "Row", "Jacobi", 5, 4, 1, 1, "None", 0),
+]
+
 # Parameter sets timed on the GPU for the benchmark workloads.
 BENCH = [
     (2, "Box", "Row", "Jacobi", 1, 1, 1, 1, "None", 0),

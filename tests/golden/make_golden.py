@@ -1,6 +1,7 @@
 """Generate the golden fixtures of tests/golden/ from the reference's own generated kernels.
 
-For every parameter set of ``oracle.ref_configs.PARITY`` this script
+For every parameter set of ``oracle.ref_configs.PARITY`` (seeds 1000 + i; with ``--extra`` the
+CPU-only sets of ``ref_configs.EXTRA``, seeds 2000 + i) this script
   1. runs the reference generators (through ``oracle.build_ref.generate``, i.e. straight from the
      read-only reference tree) to obtain that set's ``kernels.cu``;
   2. compiles it for the host CPU with ``ref_host_shim.cpp`` (g++ -O2 -mfma -ffp-contract=fast,
@@ -110,13 +111,15 @@ def gpu_outputs(cfg, seed):
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpu", action="store_true")
+    ap.add_argument("--extra", action="store_true", help="the CPU-only sets of ref_configs.EXTRA")
     ap.add_argument("--out", default=str(HERE))
     a = ap.parse_args()
     outdir = Path(a.out)
     outdir.mkdir(parents=True, exist_ok=True)
+    cfgs, seed0 = (ref_configs.EXTRA, 2000) if a.extra else (ref_configs.PARITY, 1000)
     with tempfile.TemporaryDirectory() as tmp:
-        for i, cfg in enumerate(ref_configs.PARITY):
-            seed = 1000 + i
+        for i, cfg in enumerate(cfgs):
+            seed = seed0 + i
             if a.gpu:
                 spec, raw, g, mask, out = gpu_outputs(cfg, seed)
             else:

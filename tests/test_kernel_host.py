@@ -16,7 +16,7 @@ from oracle import ref_configs
 from make_golden import fixture_input, HERE as GOLDEN
 
 
-@pytest.mark.parametrize("cfg", ref_configs.PARITY, ids=ref_configs.key)
+@pytest.mark.parametrize("cfg", ref_configs.PARITY + ref_configs.EXTRA, ids=ref_configs.key)
 def test_kernel_arithmetic_matches_reference_fixture(cfg):
     f = np.load(GOLDEN / ("%s.npz" % ref_configs.key(cfg)))
     spec, raw, g, a, mask = fixture_input(cfg, int(f["seed"]))
@@ -87,7 +87,7 @@ def test_march_addressing_model(case, es):
             assert cnt is None or cnt > 0
 
 
-PIPE_CFGS = [c for c in ref_configs.PARITY if not (c[0] == 2 and c[2] == "Column")]
+PIPE_CFGS = [c for c in ref_configs.PARITY + ref_configs.EXTRA if not (c[0] == 2 and c[2] == "Column")]
 
 
 @pytest.mark.parametrize("cfg", PIPE_CFGS, ids=ref_configs.key)

@@ -22,6 +22,18 @@ def test_oracle_matches_reference_fixture(cfg):
     assert np.array_equal(out, f["out"])
 
 
+@pytest.mark.parametrize("cfg", ref_configs.EXTRA, ids=ref_configs.key)
+def test_oracle_matches_reference_fixture_long_ranges(cfg):
+    """Ranges 5-8, 3D Box beyond range 1 and wider coarsening: the oracle against fixtures from
+    the reference's generated kernels (host build), bit for bit, and its OpenMP loop likewise."""
+    f = np.load(GOLDEN / ("%s.npz" % ref_configs.key(cfg)))
+    assert str(f["source"]) == "host-shim"
+    spec, raw, g, a, mask = fixture_input(cfg, int(f["seed"]))
+    assert tuple(int(v) for v in f["raw"]) == tuple(raw)
+    assert np.array_equal(O.sweeps(spec, a, int(f["nsweeps"]), g.right_offset, mask), f["out"])
+    assert np.array_equal(O.sweeps(spec, a, int(f["nsweeps"]), g.right_offset, mask, cpu_threads=4), f["out"])
+
+
 @pytest.mark.parametrize("cfg", ref_configs.PARITY, ids=ref_configs.key)
 def test_openmp_baseline_is_bit_identical(cfg):
     f = np.load(GOLDEN / ("%s.npz" % ref_configs.key(cfg)))
