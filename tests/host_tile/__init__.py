@@ -26,6 +26,8 @@ def build(cfg, precision="f64", source="tile_host.cpp") -> ctypes.CDLL:
         "TCS_DIM": d, "TCS_SHAPE": _SH[sh], "TCS_ORIENT": _OR[o], "TCS_COEFF": _CO[c], "TCS_R": r,
         "TCS_CX": cx, "TCS_CY": cy, "TCS_CZ": cz if d == 3 else 1,
     }
+    if precision == "f32c":  # FP32 grids, compensated accumulation
+        macros["TCS_COMP"] = 1
     src = (HERE / source).read_bytes() + (CSRC / "tcs_tile.cuh").read_bytes()
     tag = hashlib.sha1(src + repr(sorted(macros.items())).encode()).hexdigest()[:16]
     OUT.mkdir(parents=True, exist_ok=True)

@@ -34,7 +34,7 @@ extern "C" int tile_sweep(const unsigned grid[3], unsigned left_offset, unsigned
         const long long base = x + y * xdim + z * plane;
         const T* p = in + base;
         auto ld = [&](int gx, int gy, int gz) { return p[gx + gy * xdim + gz * plane]; };
-        T acc[NE];
+        Acc acc[NE];  // T, or the compensated pair with TCS_COMP
         traverse(ld, acc);
         store(out + base, acc, (tcs_u64)xdim, (tcs_u64)plane);
       }

@@ -247,3 +247,44 @@ def test_temporal_blocking_model(R, shape, es):
         interior[R:y_lim, x0:x_lim] = True
         assert np.all(writes[interior] == 1) and np.all(writes[~interior] == 0)
         assert np.array_equal(got, want)
+
+
+COMP_CASES = [
+    ((2, "Box", "Row", "Variable", 6, 4, 1, 1, "None", 0), (301, 207, 1)),
+    ((3, "Star", "Row", "Variable", 4, 2, 2, 1, "Read", 16), (60, 44, 38)),
+    ((2, "Box", "Column", "Jacobi", 3, 2, 2, 1, "None", 0), (150, 99, 1)),
+    ((3, "Box", "Row", "Variable", 2, 1, 2, 2, "Write", 8), (41, 37, 29)),
+]
+
+
+@pytest.mark.parametrize("case", COMP_CASES, ids=lambda c: ref_configs.key(c[0]))
+def test_compensated_arithmetic_within_rounding_of_fp64(case):
+    """The host build of the compensated FP32 arithmetic (tcs_tile.cuh with TCS_COMP): within
+    3 * 2^-24 |exact| + 4 S 2^-48 sum |m||in| of the float64 oracle on the same FP32 inputs and
+    FP32-rounded mask, the bound the GPU test applies to the f32c kernels; plain FP32 does worse
+    on the long Variable stencils; border and padding untouched."""
+    cfg, sides = case
+    d, sh, o, c, r, cx, cy, cz, al, cl = cfg
+    spec = O.make_spec(*cfg)
+    g = O.geometry(spec, *sides)
+    shape = (g.grid[1], g.grid[0]) if d == 2 else (g.grid[2], g.grid[1], g.grid[0])
+    rng = np.random.default_rng(r)
+    a = rng.uniform(-1, 1, shape).astype(np.float32)
+    S = O.stencil_size(spec)
+    mask = rng.standard_normal(S) / S if c == "Variable" else None
+    out_c = host_tile.sweeps(cfg, a, g.grid, g.left_offset, g.right_offset, 1, mask, "f32c").astype(np.float64)
+    out_p = host_tile.sweeps(cfg, a, g.grid, g.left_offset, g.right_offset, 1, mask, "f32").astype(np.float64)
+    m32 = None if mask is None else mask.astype(np.float32).astype(np.float64)
+    exact = O.sweep(spec, a.astype(np.float64), g.right_offset, m32)
+    x0, x_lim = r + g.left_offset, g.grid[0] - r - (g.right_offset if al != "None" else 0)
+    sl = (slice(r, g.grid[1] - r), slice(x0, x_lim)) if d == 2 else \
+        (slice(r, g.grid[2] - r), slice(r, g.grid[1] - r), slice(x0, x_lim))
+    mag = O.sweep(spec, np.abs(a.astype(np.float64)), g.right_offset, None if m32 is None else np.abs(m32))[sl]
+    bound = 3 * 2.0 ** -24 * np.abs(exact[sl]) + 4 * S * 2.0 ** -48 * mag
+    err_c, err_p = np.abs(out_c[sl] - exact[sl]), np.abs(out_p[sl] - exact[sl])
+    assert np.all(err_c <= bound), float((err_c / bound).max())
+    if c == "Variable" and r >= 4:
+        assert err_c.max() < err_p.max()
+    outside = np.ones(shape, dtype=bool)
+    outside[sl] = False
+    assert np.array_equal(out_c[outside], a.astype(np.float64)[outside])
