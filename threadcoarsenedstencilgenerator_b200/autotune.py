@@ -389,12 +389,13 @@ class Autotuner:
         best, err = self._model_error(measured, predicted)
         if err > self.tolerance:
             # A timing over a couple of sweeps can be off by more than the tolerance on its own:
-            # before giving up on the model, time the same candidates again over twice the sweeps
-            # and assess the model on the mean of both timings.
+            # before giving up on the model, time the same candidates again over twice the sweeps.
+            # Interference and clock dips only ever slow a run down, so each block keeps the
+            # faster of its two timings.
             for b in list(measured):
                 g = time_block(st, geom, x, y, b, 2 * self.sweeps)
                 if g is not None:
-                    measured[b] = (measured[b] + 2.0 * g) / 3.0  # weighted by sweeps timed
+                    measured[b] = max(measured[b], g)
             best, err = self._model_error(measured, predicted)
         if err > self.tolerance:
             r = self._exhaustive(st, geom, x, y, keep, t0, "prediction error %.2f (log) above %.2f" % (
