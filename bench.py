@@ -146,9 +146,12 @@ class ClockSampler:
 
 
 def _dist():
-    from threadcoarsenedstencilgenerator_b200 import replicas
+    """(world size, rank, local rank) from the launcher's environment (1, 0, 0 without one); read
+    here without importing the engine, which the reference arm must not load."""
+    import os
 
-    return replicas.rank_env()
+    return (int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")),
+            int(os.environ.get("LOCAL_RANK", "0")))
 
 
 def _traffic(workload: str):
@@ -160,29 +163,35 @@ def _traffic(workload: str):
     return None
 
 
-def cpu_baseline(w, geom, a, mask, budget_s: float = 12.0) -> dict:
-    """The oracle's OpenMP loop (all host threads) on the same grid: whole-grid sweeps until the
-    time budget is spent."""
+def cpu_baseline(w, spec, geom, a, mask, n: int, got=None) -> tuple[dict, dict | None]:
+    """The oracle's OpenMP loop (all host threads) runs the same n ping-pong sweeps of the same
+    grid that the GPU ran (warm-up and timed sweeps), from the same input.  Its time is the CPU
+    baseline; its result is the checker of the GPU's (``got``): every point, bit for bit."""
     import numpy as np
 
     import oracle as O
 
-    d, sh, o, c = w.spec.dimension, w.spec.neighbourhood, w.spec.orientation, w.spec.coefficients
-    ospec = O.make_spec(d, sh, o, c, w.spec.range, w.spec.cx, w.spec.cy, w.spec.cz, w.spec.alignment, w.spec.cl_size)
-    out = np.array(a, copy=True)
+    ospec = O.make_spec(spec.dimension, spec.neighbourhood, spec.orientation, spec.coefficients, spec.range,
+                        spec.cx, spec.cy, spec.cz, spec.alignment, spec.cl_size)
+    x = np.array(a, copy=True)
+    y = np.array(a, copy=True)
     threads = O.max_threads()
     t0 = time.perf_counter()
-    n = 0
-    while True:
-        O.cpu_sweep(ospec, a, out, geom.right_offset, mask, threads=threads)
-        n += 1
-        if time.perf_counter() - t0 > budget_s or n >= 200:
-            break
+    for _ in range(n):
+        O.cpu_sweep(ospec, x, y, geom.right_offset, mask, threads=threads)
+        x, y = y, x
     dt = time.perf_counter() - t0
     glups = geom.interior_points * n / dt / 1e9
-    return {"value": glups, "unit": "GLup/s", "cores": threads, "kind": "port",
-            "sample": "%d full sweeps of the %s grid (%.1f s, OpenMP over rows, x innermost)" % (
-                n, "x".join(str(v) for v in w.grid[:w.spec.dimension]), dt)}
+    base = {"value": glups, "unit": "GLup/s", "cores": threads, "kind": "port",
+            "sample": "%d full sweeps of the %s grid (%.1f s, OpenMP over rows, x innermost): the sweeps the GPU "
+                      "ran, from the same input" % (n, "x".join(str(v) for v in w.grid[:w.spec.dimension]), dt)}
+    parity = None
+    if got is not None:
+        same = bool(np.array_equal(got, x))
+        diff = 0.0 if same else float(np.nanmax(np.abs(got.astype(np.float64) - x.astype(np.float64))))
+        parity = {"equal": same, "sweeps": n, "points": "every point of both grids (interior, border, padding)",
+                  "max_abs_diff": diff, "checker": "oracle OpenMP loop (same per-output term order)"}
+    return base, parity
 
 
 def reference_gpu_timing(w, geom, steps: int = 20) -> dict | None:
@@ -266,6 +275,8 @@ def run_ours(args) -> dict | None:
     clocks = sampler.stop()
     if st.device_status() != 0:
         raise RuntimeError("device status word set during the timed sweeps")
+    # the state the timed sweeps left (warm-up + timed sweeps from the seeded input), for the check
+    result = x.cpu().numpy() if (rank == 0 and world == 1 and not args.no_cpu_baseline) else None
     ms_max = replicas.max_over_ranks(ms, dist)
     points = geom.interior_points
     value = replicas.whole_job_rate(world, points * args.steps, ms_max) / 1e9
@@ -314,10 +325,11 @@ def run_ours(args) -> dict | None:
 
     ref_gpu = None
     cpu = None
+    parity = None
     if rank == 0 and world == 1:
         ref_gpu = reference_gpu_timing(w, geom)
         if not args.no_cpu_baseline:
-            cpu = cpu_baseline(w, geom, a, mask)
+            cpu, parity = cpu_baseline(w, spec, geom, a, mask, args.warmup + args.steps, result)
     replicas.close_group(dist)
     if rank != 0:
         return None
@@ -358,6 +370,8 @@ def run_ours(args) -> dict | None:
                 "serial_value": e2e_serial},
         "clocks": clocks,
         "cpu_baseline": cpu,
+        "parity": None if parity is None else parity["equal"],
+        "parity_check": parity,
         "reference_gpu": ref_gpu,
     }
     if temporal:
@@ -694,72 +708,190 @@ def run_batch(args) -> dict | None:
     }
 
 
-def run_reference(args) -> dict | None:
-    """The reference's own stencil arithmetic on the host cores (oracle OpenMP restatement)."""
-    import numpy as np
+def _workload_params():
+    """The workload table, loaded from its file without importing the engine's package (the
+    reference arm must not map libtcs.so)."""
+    import importlib.util
 
+    path = ROOT / "threadcoarsenedstencilgenerator_b200" / "workload_params.py"
+    spec = importlib.util.spec_from_file_location("tcs_workload_params", path)
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def _oracle_shape(dimension: int, g) -> tuple:
+    return (g.grid[1], g.grid[0]) if dimension == 2 else (g.grid[2], g.grid[1], g.grid[0])
+
+
+def _oracle_points(dimension: int, g) -> int:
+    e = g.elements
+    return e[0] * e[1] * (e[2] if dimension == 3 else 1)
+
+
+def run_reference(args) -> dict | None:
+    """The reference's own stencil arithmetic on the host cores (oracle OpenMP restatement).  Only
+    the oracle is loaded: the workload table comes from its plain-data file and the geometry from
+    the oracle's restatement of cuda/benchmark.cpp:142-179."""
     import oracle as O
-    from threadcoarsenedstencilgenerator_b200.workloads import WORKLOADS
 
     world, rank, local = _dist()
     if rank != 0:
         return None
-    from threadcoarsenedstencilgenerator_b200.workloads import BATCH_WORKLOADS
-
-    if args.workload in BATCH_WORKLOADS:
-        w = BATCH_WORKLOADS[args.workload]
-        geoms = w.geometries()
-        arrs = w.make_inputs(geoms)
+    P = _workload_params()
+    if args.workload in P.BATCH:
+        p = P.BATCH[args.workload]
+        st = p["stencil"]
+        ospec = O.make_spec(*st)
+        sides = P.batch_sides(p["n_grids"], p["side_range"], p["multiple"], p["seed"])
+        geoms = [O.geometry(ospec, *sd) for sd in sides]
+        arrs = P.batch_inputs(p["seed"], [_oracle_shape(st[0], g) for g in geoms])
+        points = sum(_oracle_points(st[0], g) for g in geoms)
         threads = O.max_threads()
-        _batch_cpu(w, w.spec, geoms, arrs, 1.0, threads)  # warm-up
-        value, nsw, dt = _batch_cpu(w, w.spec, geoms, arrs, 20.0, threads)
+        outs = [a.copy() for a in arrs]
+
+        def batch_sweep():
+            for g, a, o in zip(geoms, arrs, outs):
+                O.cpu_sweep(ospec, a, o, g.right_offset, None, threads=threads)
+            return [(o, a) for a, o in zip(arrs, outs)]
+
+        for _ in range(args.warmup):
+            pairs = batch_sweep()
+            arrs, outs = [q for q, _ in pairs], [q for _, q in pairs]
+        t0 = time.perf_counter()
+        nsw = 0
+        while nsw < args.steps and (nsw == 0 or time.perf_counter() - t0 < 20.0):
+            pairs = batch_sweep()
+            arrs, outs = [q for q, _ in pairs], [q for _, q in pairs]
+            nsw += 1
+        dt = time.perf_counter() - t0
+        value = points * nsw / dt / 1e9
         return {
-            "metric": "GLup/s (FP64 batched sweeps, %s)" % w.name, "value": value, "unit": "GLup/s",
+            "metric": "GLup/s (FP64 batched sweeps, %s)" % args.workload, "value": value, "unit": "GLup/s",
             "n_gpus": world, "steps": nsw, "warmup": args.warmup, "ms_per_step": dt * 1e3 / nsw,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic (numpy default_rng seed %d)" % w.seed,
-            "config": {"workload": w.name, "grids": w.n_grids}, "impl": "reference",
+            "data": "synthetic (numpy default_rng seed %d)" % p["seed"],
+            "config": {"workload": args.workload, "grids": p["n_grids"]}, "impl": "reference",
             "cpu_baseline": {"value": value, "unit": "GLup/s", "cores": threads, "kind": "port",
                              "sample": "%d sweeps of all %d grids, OpenMP restatement of the reference kernel, "
-                                       "grid after grid" % (nsw, w.n_grids)},
+                                       "grid after grid" % (nsw, p["n_grids"])},
             "e2e": {"value": value, "unit": "GLup/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         }
-    w = WORKLOADS[args.workload]
-    spec = w.spec
-    geom = spec.geometry(*w.grid)
-    a = w.make_input(geom)
-    mask = w.make_mask()
-    ospec = O.make_spec(spec.dimension, spec.neighbourhood, spec.orientation, spec.coefficients, spec.range, spec.cx,
-                        spec.cy, spec.cz, spec.alignment, spec.cl_size)
+    p = P.SINGLE[args.workload]
+    st = p["stencil"]
+    ospec = O.make_spec(*st)
+    geom = O.geometry(ospec, *p["grid"])
+    right = geom.right_offset
+    a = P.make_input(p["seed"], p["value_range"], _oracle_shape(st[0], geom))
+    mask = P.make_mask(p["seed"], p["mask_kind"], st)
     out = a.copy()
     threads = O.max_threads()
     for _ in range(args.warmup):
-        O.cpu_sweep(ospec, a, out, geom.right_offset, mask, threads=threads)
+        O.cpu_sweep(ospec, a, out, right, mask, threads=threads)
+        a, out = out, a
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        O.cpu_sweep(ospec, a, out, geom.right_offset, mask, threads=threads)
+        O.cpu_sweep(ospec, a, out, right, mask, threads=threads)
         a, out = out, a
     dt = time.perf_counter() - t0
-    value = geom.interior_points * args.steps / dt / 1e9
+    value = _oracle_points(st[0], geom) * args.steps / dt / 1e9
     return {
-        "metric": "GLup/s (FP64 stencil sweep, %s)" % w.name, "value": value, "unit": "GLup/s", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3 / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (numpy default_rng seed %d)" % w.seed,
-        "config": {"workload": w.name, "grid": list(w.grid[:spec.dimension])}, "impl": "reference",
+        "metric": "GLup/s (FP64 stencil sweep, %s)" % args.workload, "value": value, "unit": "GLup/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3 / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (numpy default_rng seed %d)" % p["seed"],
+        "config": {"workload": args.workload, "grid": list(p["grid"][:st[0]])}, "impl": "reference",
         "cpu_baseline": {"value": value, "unit": "GLup/s", "cores": threads, "kind": "port",
                          "sample": "%d full sweeps of the grid, OpenMP restatement of the reference kernel" % args.steps},
         "e2e": {"value": value, "unit": "GLup/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
 
 
-def main() -> int:
-    from threadcoarsenedstencilgenerator_b200.workloads import BATCH_WORKLOADS, DEFAULT_WORKLOAD, WORKLOADS
+def run_case(args) -> dict:
+    """A few sweeps of a workload's tuned launch on a reduced grid (--grid) or on the first K grids
+    of a batch (--grids), for profilers: a small case of the same kernel that an ncu capture
+    finishes in a minute.  Keep each buffer above the L2 size (126 MB) so that DRAM counters
+    stay meaningful.  --case tensor-cores / temporal select the tcgen05 FP32 sweep / the
+    two-sweeps-per-pass kernel (2D)."""
+    import numpy as np
+    import torch
 
+    import threadcoarsenedstencilgenerator_b200 as tcs
+
+    torch.cuda.set_device(0)
+    P = _workload_params()
+    if args.workload in P.BATCH:
+        from threadcoarsenedstencilgenerator_b200.batch import BatchedSweeps
+        from threadcoarsenedstencilgenerator_b200.workloads import BATCH_WORKLOADS
+
+        w = BATCH_WORKLOADS[args.workload]
+        spec = w.spec.replace(precision=args.case_precision)
+        geoms = w.geometries(spec)
+        arrs = w.make_inputs(geoms, np.float64 if args.case_precision == "f64" else np.float32)
+        if args.grids:
+            geoms, arrs = geoms[:args.grids], arrs[:args.grids]
+        st = tcs.Stencil(spec)
+        xs = [torch.from_numpy(v).cuda() for v in arrs]
+        ys = [x.clone() for x in xs]
+        bt = BatchedSweeps(st, geoms, xs, ys, w.tuned_launch(args.case_precision))
+        bt.sweeps(args.steps)
+        torch.cuda.synchronize()
+        if st.device_status() != 0:
+            raise RuntimeError("device status word set")
+        plan = bt.plan()
+        bt.close()
+        return {"case": args.workload, "grids": len(geoms), "points": sum(g.interior_points for g in geoms),
+                "sweeps": args.steps, "block": list(plan.block), "loader": plan.loader}
+    from threadcoarsenedstencilgenerator_b200.workloads import WORKLOADS
+
+    w = WORKLOADS[args.workload]
+    spec = w.tuned_spec(args.case_precision).replace(precision=args.case_precision)
+    launch = w.tuned_launch(args.case_precision)
+    grid = tuple(args.grid) + (1,) * (3 - len(args.grid))
+    geom = spec.geometry(*grid)
+    st = tcs.Stencil(spec)
+    m = w.make_mask()
+    if m is not None:
+        st.copy_mask(m)
+    dt = torch.float64 if args.case_precision == "f64" else torch.float32
+    x = torch.from_numpy(w.make_input(geom)).to("cuda", dtype=dt)
+    y = x.clone()
+    if args.case == "temporal":
+        st.sweeps_tb2(geom, x, y, args.steps)
+    else:
+        for _ in range(args.steps):
+            if args.case == "tensor-cores":
+                st.tc_update_grid(geom, x, y)
+            else:
+                st.update_grid(geom, x, y, launch)
+            x, y = y, x
+    torch.cuda.synchronize()
+    if st.device_status() != 0:
+        raise RuntimeError("device status word set")
+    plan = st.plan(geom, launch)
+    return {"case": args.workload, "grid": list(grid), "points": geom.interior_points, "sweeps": args.steps,
+            "kernel": args.case, "variant": plan.variant, "block": list(plan.block), "chunk": plan.chunk}
+
+
+def check_world(gpus: int, world: int) -> str | None:
+    """An error message when --gpus disagrees with the launcher's world size, else None.  bench.py
+    runs one process per GPU: --gpus N > 1 needs N ranks from torch.distributed.run."""
+    if gpus < 1:
+        return "--gpus must be at least 1"
+    if gpus != world:
+        return ("--gpus %d but WORLD_SIZE is %d: launch one process per GPU, e.g. python -m "
+                "torch.distributed.run --nnodes=1 --nproc-per-node %d --master-addr 127.0.0.1 bench.py --gpus %d"
+                % (gpus, world, gpus, gpus))
+    return None
+
+
+def main(argv=None) -> int:
+    P = _workload_params()
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
-    ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS) + sorted(BATCH_WORKLOADS))
+    ap.add_argument("--workload", default=P.DEFAULT, choices=sorted(P.SINGLE) + sorted(P.BATCH))
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--e2e-steps", type=int, default=6)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -767,11 +899,22 @@ def main() -> int:
                     help="mixed: FP64 vs FP32 vs FP32 with FP64 defect correction on the workload")
     ap.add_argument("--sweeps", type=int, default=0, help="precision mode: sweeps (default: the workload's)")
     ap.add_argument("--period", type=int, default=20, help="precision mode: FP32 sweeps per FP64 defect")
-    args = ap.parse_args()
+    ap.add_argument("--grid", type=int, nargs="+", help="profiling case: --steps sweeps on this reduced grid")
+    ap.add_argument("--grids", type=int, default=0, help="profiling case (batch): the first K grids")
+    ap.add_argument("--case", default="sweep", choices=["sweep", "tensor-cores", "temporal"],
+                    help="profiling case: which kernel")
+    ap.add_argument("--case-precision", default="f64", choices=["f64", "f32"], help="profiling case: precision")
+    args = ap.parse_args(argv)
     args.warmup = max(3, args.warmup)
+    err = check_world(args.gpus, _dist()[0])
+    if err:
+        print(err, file=sys.stderr)
+        return 2
     if args.impl == "reference":
         line = run_reference(args)
-    elif args.workload in BATCH_WORKLOADS:
+    elif args.grid or args.grids:
+        line = run_case(args)
+    elif args.workload in P.BATCH:
         line = run_batch(args)
     elif args.precision == "mixed":
         line = run_precision(args)

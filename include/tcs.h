@@ -195,6 +195,12 @@ int tcs_benchmark_update_grid(tcs_stencil* h, const char* coeff_type, const char
                               unsigned right_offset, double* durations, unsigned cap,
                               unsigned* n_out);
 
+/* Every per-launch duration [s] of the handle's last tcs_benchmark_update_grid loop, however many
+ * it measured: writes up to `cap` and sets *n_out to the full count.  The reference's launcher
+ * returns them all as a std::vector (cuda/generateLaunchUpdateGrid.py:140-147); a caller sizes its
+ * buffer from *n_out of the benchmark call and collects them here. */
+int tcs_benchmark_durations(tcs_stencil* h, double* durations, unsigned cap, unsigned* n_out);
+
 /* launchInit (cuda/launchUpdateGrid.h:14, cuda/generateLaunchUpdateGrid.py:150-158): the
  * reference's `init` pattern (cuda/generate2DStencil_cuda.py:321-350,
  * cuda/generate3DStencil_cuda.py:386-430), synchronous. */
@@ -238,7 +244,8 @@ int tcs_update_grid_source(tcs_stencil* h, const unsigned grid[3], unsigned righ
 
 /* FP64 defect r = fl32(sx - x) (sx = one FP64 sweep of x) and, when norms != NULL, the global
  * residual norms {max |sx - x|, ||sx - x||_2} computed on the GPU in FP64 (synchronises
- * `stream`).  Uses library-allocated scratch memory for the per-block partial sums. */
+ * `stream`).  Uses library-allocated scratch memory for the per-block partial sums.  The calling
+ * thread's current device must be the handle's (TCS_ERR_INVALID_VALUE otherwise). */
 int tcs_residual(tcs_stencil* h, const unsigned grid[3], unsigned right_offset, const double* x,
                  const double* sx, float* r, double norms[2], void* stream);
 
@@ -250,14 +257,21 @@ int tcs_residual(tcs_stencil* h, const unsigned grid[3], unsigned right_offset, 
  * the per-block partial sums live in a static 32 KiB device array of libtcs.so (4096 doubles),
  * which every GPU that loads the library holds until the process exits.  `nblocks` partial
  * blocks (0 = 2 per SM) need 2*nblocks + 2 doubles, so at most 2047 blocks; larger requests
- * return TCS_ERR_INVALID_VALUE with the limit in the message.  The first call on a device looks
+ * return TCS_ERR_INVALID_VALUE with the limit in the message.  The first call in a context looks
  * up the array's device address (cudaGetSymbolAddress, with that device current), so make that
- * first call before any stream capture.  All calls share the array and it keeps the last call's
+ * first call before any stream capture; after cudaDeviceReset the recreated context is a new one,
+ * and its first call (again before any capture) looks the address up again.  The calling thread's
+ * current device must be the handle's (TCS_ERR_INVALID_VALUE otherwise, as for tcs_residual).
+ * All calls share the array and it keeps the last call's
  * contents (nothing in it needs to start at zero); calls that overlap on the GPU race on it, so
  * serialise them (one stream, or events).  Outputs and norms are those of tcs_residual. */
 int tcs_residual_static(tcs_stencil* h, const unsigned grid[3], unsigned right_offset,
                         const double* x, const double* sx, float* r, double norms[2],
                         unsigned nblocks, void* stream);
+
+/* Bytes of device scratch the handle has allocated for its field reductions (tcs_residual,
+ * tcs_compare); 0 until one of them runs.  tcs_residual_static never adds to it. */
+int tcs_scratch_bytes(tcs_stencil* h, unsigned long long* bytes);
 
 /* x += e (FP64 state, FP32 correction). */
 int tcs_accumulate(tcs_stencil* h, const unsigned grid[3], unsigned right_offset, double* x,

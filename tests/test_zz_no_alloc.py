@@ -59,7 +59,16 @@ def test_static_scratch_residual_matches_allocating_entry_point():
         assert n_static[0] == np.abs(d).max()
 
 
+def _scratch_bytes(lib, h) -> int:
+    v = ctypes.c_ulonglong(123)
+    assert lib.tcs_scratch_bytes(h, ctypes.byref(v)) == 0
+    return v.value
+
+
 def test_static_scratch_residual_allocates_nothing_and_enforces_its_limit():
+    """Free device memory is unchanged across the calls, and the handle's library scratch (which
+    tcs_residual allocates on first use) stays unallocated: a cudaMalloc undone by a cudaFree, or an
+    allocation below the driver's 2 MiB granularity, would escape the first check, not the second."""
     import torch
 
     import threadcoarsenedstencilgenerator_b200 as tcs
@@ -68,6 +77,7 @@ def test_static_scratch_residual_allocates_nothing_and_enforces_its_limit():
     lib = _lib.load()
     spec = tcs.StencilSpec(dimension=2, neighbourhood="Box", coefficients="Variable", range=6, cx=4)
     st = tcs.Stencil(spec)
+    assert _scratch_bytes(lib, st._h) == 0
     geom = spec.geometry(1024, 512)
     x = torch.rand(geom.shape, dtype=torch.float64, device="cuda")
     sx = x * 0.5
@@ -82,6 +92,11 @@ def test_static_scratch_residual_allocates_nothing_and_enforces_its_limit():
         assert norms[0] == first[0] and abs(norms[1] - first[1]) <= 1e-12 * first[1]
     torch.cuda.synchronize()
     assert torch.cuda.mem_get_info()[0] == free_before
+    assert _scratch_bytes(lib, st._h) == 0
     rc, _ = _call_residual(lib, "tcs_residual_static", st._h, geom, x, sx, r, (2048,))
     assert rc == _lib.TCS_ERR_INVALID_VALUE
     assert "4096" in _lib.last_error()
+    # the allocating entry point does allocate, through the same handle
+    rc, _ = _call_residual(lib, "tcs_residual", st._h, geom, x, sx, r)
+    assert rc == 0, _lib.last_error()
+    assert _scratch_bytes(lib, st._h) > 0

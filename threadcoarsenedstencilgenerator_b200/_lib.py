@@ -134,6 +134,8 @@ SIGNATURES = {
     "tcs_update_grid_source": [_vp, U3, _u, _P(CLaunch), _vp, _vp, _vp, _vp],
     "tcs_residual": [_vp, U3, _u, _vp, _vp, _vp, _P(ctypes.c_double), _vp],
     "tcs_residual_static": [_vp, U3, _u, _vp, _vp, _vp, _P(ctypes.c_double), _u, _vp],
+    "tcs_scratch_bytes": [_vp, _P(ctypes.c_ulonglong)],
+    "tcs_benchmark_durations": [_vp, _vp, _u, _P(_u)],
     "tcs_accumulate": [_vp, U3, _u, _vp, _vp, _vp],
     "tcs_compare": [_vp, U3, _u, _vp, _i, _vp, _P(ctypes.c_double), _vp],
     "tcs_device_sm_count": [_P(_i)],

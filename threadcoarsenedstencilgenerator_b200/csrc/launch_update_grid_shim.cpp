@@ -17,6 +17,7 @@
 // cuda/benchmark.cpp:244-249); other failures print a GPUassert-style line and continue.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdio>
 #include <string>
 #include <vector>
@@ -74,18 +75,23 @@ std::vector<double> benchmarkUpdateGrid(std::string coeffType, std::string stenc
   const unsigned grid[3] = {gridSize.x, gridSize.y, gridSize.z};
   const unsigned block[3] = {blockSize.x, blockSize.y, blockSize.z};
   const unsigned blocks[3] = {gridBlocks.x, gridBlocks.y, gridBlocks.z};
-  std::vector<double> durations(1u << 20);
   unsigned n = 0;
-  const int rc = tcs_benchmark_update_grid(
-      h, coeffType.c_str(), stencilType.c_str(), stencilRange, dimension, alignment.c_str(), maxTime,
-      grid, block, blocks, d_array0, d_array1, rightOffset, durations.data(),
-      (unsigned)durations.size(), &n);
+  const int rc = tcs_benchmark_update_grid(h, coeffType.c_str(), stencilType.c_str(), stencilRange,
+                                           dimension, alignment.c_str(), maxTime, grid, block, blocks,
+                                           d_array0, d_array1, rightOffset, nullptr, 0, &n);
   if (rc == TCS_ERR_INVALID_VALUE || rc == TCS_ERR_UNSUPPORTED) throw cudaErrorInvalidValue;
   if (rc != TCS_OK) {
     report("benchmarkUpdateGrid");
     return {};
   }
-  durations.resize(std::min<size_t>(n, durations.size()));
+  // every duration the loop measured, however many
+  std::vector<double> durations(std::max(1u, n));
+  unsigned got = 0;
+  if (tcs_benchmark_durations(h, durations.data(), (unsigned)durations.size(), &got) != TCS_OK) {
+    report("benchmarkUpdateGrid");
+    return {};
+  }
+  durations.resize(std::min<size_t>(got, durations.size()));
   return durations;
 }
 

@@ -64,6 +64,8 @@ struct Driver {
   decltype(&cuOccupancyMaxActiveBlocksPerMultiprocessor) OccMaxActive = nullptr;
   decltype(&cuOccupancyMaxPotentialBlockSize) OccMaxPotential = nullptr;
   decltype(&cuGetErrorString) GetErrorString = nullptr;
+  decltype(&cuCtxGetCurrent) CtxGetCurrent = nullptr;
+  decltype(&cuCtxGetId) CtxGetId = nullptr;
   bool ok = false;
   std::string why;
 };
@@ -96,7 +98,8 @@ void load_driver() {
             entry("cuTensorMapEncodeTiled", d.TensorMapEncodeTiled, d.why) &&
             entry("cuOccupancyMaxActiveBlocksPerMultiprocessor", d.OccMaxActive, d.why) &&
             entry("cuOccupancyMaxPotentialBlockSize", d.OccMaxPotential, d.why) &&
-            entry("cuGetErrorString", d.GetErrorString, d.why);
+            entry("cuGetErrorString", d.GetErrorString, d.why) &&
+            entry("cuCtxGetCurrent", d.CtxGetCurrent, d.why) && entry("cuCtxGetId", d.CtxGetId, d.why);
   d.ok = ok;
   g_drv = d;
 }
@@ -352,6 +355,7 @@ struct tcs_stencil {
   int dropin_variant = TCS_VARIANT_AUTO;  // variant used by tcs_benchmark_update_grid
   unsigned dropin_segments = 0, dropin_depth = 0;
   std::vector<double> mask_host;          // last mask uploaded (copied into new pipe modules)
+  std::vector<double> last_durations;     // per-launch durations [s] of the last benchmark loop
   double* scratch = nullptr;              // per-block partials of the field reductions
   size_t scratch_len = 0;                 // in doubles
   std::vector<PipeMod*> pipes;            // pipelined-sweep modules, one per launch shape
@@ -1387,9 +1391,18 @@ int tcs_benchmark_update_grid(tcs_stencil* h, const char* coeff_type, const char
     runtime = std::chrono::duration<double>(ts.back() - ts.front()).count();
   }
   const unsigned n = (unsigned)(ts.size() - 1);
-  for (unsigned i = 0; i < n && i < cap; ++i)
-    durations[i] = std::chrono::duration<double>(ts[i + 1] - ts[i]).count();
+  h->last_durations.resize(n);
+  for (unsigned i = 0; i < n; ++i) h->last_durations[i] = std::chrono::duration<double>(ts[i + 1] - ts[i]).count();
+  for (unsigned i = 0; i < n && i < cap && durations; ++i) durations[i] = h->last_durations[i];
   if (n_out) *n_out = n;
+  return TCS_OK;
+}
+
+int tcs_benchmark_durations(tcs_stencil* h, double* durations, unsigned cap, unsigned* n_out) {
+  if (!h || !n_out) return fail(TCS_ERR_INVALID_VALUE, "NULL argument");
+  const unsigned n = (unsigned)h->last_durations.size();
+  for (unsigned i = 0; i < n && i < cap && durations; ++i) durations[i] = h->last_durations[i];
+  *n_out = n;
   return TCS_OK;
 }
 
@@ -1536,11 +1549,24 @@ int tcs_precompile_batch(const tcs_spec* spec, unsigned bx, unsigned by, unsigne
   return precompile_pipe(spec, bx, by, chunk, true, cubin_path, path_cap);
 }
 
+// The residual entry points launch on the calling thread's current device: it must be the device
+// the handle (and the buffers) belong to.
+int check_current_device(const tcs_stencil* h) {
+  int dev = -1;
+  TCS_RT(cudaGetDevice(&dev));
+  if (dev != h->device)
+    return fail(TCS_ERR_INVALID_VALUE, "current device " + std::to_string(dev) + " is not the handle's device " +
+                                           std::to_string(h->device));
+  return TCS_OK;
+}
+
 int tcs_residual(tcs_stencil* h, const unsigned grid[3], unsigned right_offset, const double* x,
                  const double* sx, float* r, double norms[2], void* stream) {
   if (!h || !x || !sx || !r) return fail(TCS_ERR_INVALID_VALUE, "NULL argument");
+  int rc = check_current_device(h);
+  if (rc) return rc;
   TcsFieldGeo f;
-  int rc = field_geo(h, grid, right_offset, f);
+  rc = field_geo(h, grid, right_offset, f);
   if (rc) return rc;
   const int nb = field_blocks(h);
   rc = ensure_scratch(h, (size_t)nb * 4 + 8);
@@ -1562,8 +1588,10 @@ int tcs_residual_static(tcs_stencil* h, const unsigned grid[3], unsigned right_o
                         const double* x, const double* sx, float* r, double norms[2],
                         unsigned nblocks, void* stream) {
   if (!h || !x || !sx || !r) return fail(TCS_ERR_INVALID_VALUE, "NULL argument");
+  int rc = check_current_device(h);
+  if (rc) return rc;
   TcsFieldGeo f;
-  int rc = field_geo(h, grid, right_offset, f);
+  rc = field_geo(h, grid, right_offset, f);
   if (rc) return rc;
   const unsigned nb = nblocks ? nblocks : (unsigned)field_blocks(h);
   const unsigned long long need = 2ull * nb + 2ull;  // two partials per block + two results
@@ -1573,8 +1601,16 @@ int tcs_residual_static(tcs_stencil* h, const unsigned grid[3], unsigned right_o
                     " doubles of scratch; the static array holds " +
                     std::to_string(TCS_STATIC_SCRATCH_DOUBLES) + " (at most " +
                     std::to_string((TCS_STATIC_SCRATCH_DOUBLES - 2) / 2) + " blocks)");
+  // The array's address belongs to the module image loaded into the current context; a context
+  // recreated after cudaDeviceReset may place it elsewhere, so the cached address is keyed by the
+  // context's unique id.
+  CUcontext ctx = nullptr;
+  TCS_CU(g_drv.CtxGetCurrent(&ctx));
+  if (!ctx) return fail(TCS_ERR_CUDA, "tcs_residual_static: no current CUDA context");
+  unsigned long long ctx_id = 0;
+  TCS_CU(g_drv.CtxGetId(ctx, &ctx_id));
   double* scratch = nullptr;
-  const int se = tcs_field_static_scratch(&scratch);
+  const int se = tcs_field_static_scratch(ctx_id, &scratch);
   if (se != 0)
     return fail(TCS_ERR_CUDA, std::string("static scratch address: ") + cudaGetErrorString((cudaError_t)se));
   double* res = scratch + 2ull * nb;
@@ -1587,6 +1623,12 @@ int tcs_residual_static(tcs_stencil* h, const unsigned grid[3], unsigned right_o
     norms[0] = host[0];
     norms[1] = std::sqrt(host[1]);
   }
+  return TCS_OK;
+}
+
+int tcs_scratch_bytes(tcs_stencil* h, unsigned long long* bytes) {
+  if (!h || !bytes) return fail(TCS_ERR_INVALID_VALUE, "NULL argument");
+  *bytes = (unsigned long long)h->scratch_len * sizeof(double);
   return TCS_OK;
 }
 

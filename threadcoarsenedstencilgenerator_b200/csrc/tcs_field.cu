@@ -147,7 +147,7 @@ extern "C" int tcs_field_launch_add(double* x, const float* e, TcsFieldGeo g, in
 // ---- failure-detection self-test -----------------------------------------------------------
 // One warp waits on a shared-memory mbarrier that expects one arrival and never gets it -- the
 // wait of a sweep kernel whose copy never lands -- through the same bounded loop the kernels use:
-// after `limit` cycles it gives up, sets bit 1 (TCS_DEV_TIMEOUT) of `status` and returns.  No copy
+// after `limit` cycles it gives up, sets bit 0 (value 1, TCS_DEV_TIMEOUT) of `status` and returns.  No copy
 // is in flight and nothing else waits on the barrier, so the context stays usable.
 namespace {
 
@@ -194,23 +194,30 @@ static __device__ __align__(256) double tcs_static_scratch[TCS_STATIC_SCRATCH_DO
 
 #include <mutex>
 
-// Device address of tcs_static_scratch on the current device.  In host code the array's name is
-// only a host-side stand-in, so the address is looked up with cudaGetSymbolAddress, once per
-// device, with that device current (the first call on a device does it).
-extern "C" int tcs_field_static_scratch(double** out) {
+// Device address of tcs_static_scratch in the current context.  In host code the array's name
+// is only a host-side stand-in, so the address is looked up with cudaGetSymbolAddress, with the
+// device current, the first time a context of that device is seen: the entry is keyed by the
+// context's unique id (cuCtxGetId), so a context recreated after cudaDeviceReset, which may hold
+// the array elsewhere, gets a fresh lookup.
+extern "C" int tcs_field_static_scratch(unsigned long long ctx_id, double** out) {
+  struct Entry {
+    unsigned long long ctx_id;
+    double* addr;
+  };
   static std::mutex mu;
-  static double* addr[TCS_STATIC_SCRATCH_MAX_DEVICES] = {};
+  static Entry cache[TCS_STATIC_SCRATCH_MAX_DEVICES] = {};
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return (int)e;
   if (dev < 0 || dev >= TCS_STATIC_SCRATCH_MAX_DEVICES) return (int)cudaErrorInvalidDevice;
   std::lock_guard<std::mutex> lock(mu);
-  if (!addr[dev]) {
+  if (!cache[dev].addr || cache[dev].ctx_id != ctx_id) {
     void* p = nullptr;
     e = cudaGetSymbolAddress(&p, tcs_static_scratch);
     if (e != cudaSuccess) return (int)e;
-    addr[dev] = static_cast<double*>(p);
+    cache[dev].addr = static_cast<double*>(p);
+    cache[dev].ctx_id = ctx_id;
   }
-  *out = addr[dev];
+  *out = cache[dev].addr;
   return 0;
 }

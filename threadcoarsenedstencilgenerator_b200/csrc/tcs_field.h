@@ -35,10 +35,11 @@ int tcs_field_launch_compare(const void* a, int a_f32, const double* b, TcsField
                              double* scratch, int nblocks, double* result4, cudaStream_t st);
 int tcs_field_launch_add(double* x, const float* e, TcsFieldGeo g, int nblocks, cudaStream_t st);
 // Failure-detection self-test: a bounded wait on a barrier nothing arrives at (at most `limit`
-// clock cycles), which then sets bit 1 of `status`.  Returns a cudaError_t value.
+// clock cycles), which then sets bit 0 (value 1) of `status`.  Returns a cudaError_t value.
 int tcs_field_launch_wait_probe(unsigned* status, long long limit, cudaStream_t st);
-// Device address of the static scratch array on the current device (cudaError_t value).
-int tcs_field_static_scratch(double** out);
+// Device address of the static scratch array in the current context, whose unique id (cuCtxGetId)
+// is `ctx_id` (cudaError_t value).
+int tcs_field_static_scratch(unsigned long long ctx_id, double** out);
 // Tensor-core sweep: dynamic shared memory of a launch for range R, and the launch itself
 // (`bops`: the Toeplitz operands built by the host, BF16 high parts of all 2R+1 rows then low
 // parts; `nctas` persistent CTAs).  Returns a cudaError_t value.

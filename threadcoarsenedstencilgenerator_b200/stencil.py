@@ -242,15 +242,18 @@ class Stencil:
     # -- reference host interface (cuda/launchUpdateGrid.h:13-14) -------------------------------
     def benchmark_update_grid(self, coeff_type: str, neighbourhood: str, stencil_range: int, dimension: int,
                               alignment: str, max_time: float, grid_size, block_size, grid_blocks, d_array0,
-                              d_array1, right_offset: int, cap: int = 1 << 20) -> list:
-        dur = (ctypes.c_double * cap)()
+                              d_array1, right_offset: int) -> list:
+        """Every per-launch duration [s] of the doubling loop (2^k - 1 of them)."""
         n = ctypes.c_uint()
         _lib.check(self._lib.tcs_benchmark_update_grid(
             self._h, coeff_type.encode(), neighbourhood.encode(), int(stencil_range), int(dimension),
             alignment.encode(), float(max_time), _lib.U3(*_dim3(grid_size)), _lib.U3(*_dim3(block_size)),
-            _lib.U3(*_dim3(grid_blocks)), _ptr(d_array0), _ptr(d_array1), int(right_offset), dur, cap,
+            _lib.U3(*_dim3(grid_blocks)), _ptr(d_array0), _ptr(d_array1), int(right_offset), None, 0,
             ctypes.byref(n)))
-        return list(dur[: min(n.value, cap)])
+        dur = (ctypes.c_double * max(1, n.value))()
+        got = ctypes.c_uint()
+        _lib.check(self._lib.tcs_benchmark_durations(self._h, dur, n.value, ctypes.byref(got)))
+        return list(dur[: got.value])
 
     def launch_init(self, grid_size, block_size, grid_blocks, d_array, right_offset: int) -> None:
         _lib.check(self._lib.tcs_launch_init(self._h, _lib.U3(*_dim3(grid_size)), _lib.U3(*_dim3(block_size)),

@@ -14,6 +14,7 @@ from pathlib import Path
 
 import numpy as np
 
+from . import workload_params as P
 from .spec import StencilSpec
 from .stencil import Launch
 
@@ -36,22 +37,10 @@ class Workload:
         return self.spec.geometry(*self.grid)
 
     def make_input(self, geom, dtype=np.float64) -> np.ndarray:
-        rng = np.random.default_rng(self.seed)
-        lo, hi = self.value_range
-        a = rng.random(geom.shape, dtype=np.float64 if dtype == np.float64 else np.float32)
-        if (lo, hi) != (0.0, 1.0):
-            a = a * (hi - lo) + lo
-        return a.astype(dtype, copy=False)
+        return P.make_input(self.seed, self.value_range, geom.shape, dtype)
 
     def make_mask(self) -> np.ndarray | None:
-        if self.mask_kind is None or self.spec.coefficients == "Jacobi":
-            return None
-        S = self.spec.stencil_size
-        rng = np.random.default_rng(self.seed + 1)
-        m = rng.standard_normal(S)
-        if self.mask_kind == "normal_sum1":
-            return m / m.sum()
-        return m / S
+        return P.make_mask(self.seed, self.mask_kind, _stencil_tuple(self.spec))
 
     def _tuned(self, precision: str):
         if not TUNED_PATH.exists():
@@ -83,30 +72,26 @@ class Workload:
         return self.spec
 
 
+def _spec_of(t: tuple) -> StencilSpec:
+    d, sh, o, c, r, cx, cy, cz, al, cl = t
+    return StencilSpec(dimension=d, neighbourhood=sh, orientation=o, coefficients=c, range=r, cx=cx, cy=cy, cz=cz,
+                       alignment=al, cl_size=cl)
+
+
+def _stencil_tuple(s: StencilSpec) -> tuple:
+    return (s.dimension, s.neighbourhood, s.orientation, s.coefficients, s.range, s.cx, s.cy, s.cz, s.alignment,
+            s.cl_size)
+
+
 WORKLOADS = {
-    # 2D Box Jacobi r1 (9-point mean), FP64, 4096^2, coarsening 1x1, no alignment, 100 sweeps
-    "2d_box_jacobi_r1_4096": Workload(
-        name="2d_box_jacobi_r1_4096",
-        spec=StencilSpec(dimension=2, neighbourhood="Box", orientation="Row", coefficients="Jacobi", range=1),
-        grid=(4096, 4096, 1), sweeps=100, launch=Launch(block=(64, 4, 1), variant="march"),
-        reference=((2, 2, 1), (128, 1, 1))),
-    # 3D Star Variable r4 (25-point), FP64, 512^3, Read alignment to 16 points, 50 sweeps
-    "3d_star_var_r4_512": Workload(
-        name="3d_star_var_r4_512",
-        spec=StencilSpec(dimension=3, neighbourhood="Star", orientation="Row", coefficients="Variable", range=4,
-                         cx=1, cy=2, cz=2, alignment="Read", cl_size=16),
-        grid=(512, 512, 512), sweeps=50, mask_kind="normal_sum1", launch=Launch(block=(32, 8, 1), variant="march"),
-        reference=((1, 4, 2), (128, 2, 1))),
-    # 2D Box Variable r6 (169-point), FP64, 16384x8192, mask N(0,1)/169, values U[-1,1], 200 sweeps
-    "2d_box_var_r6_16384x8192": Workload(
-        name="2d_box_var_r6_16384x8192",
-        spec=StencilSpec(dimension=2, neighbourhood="Box", orientation="Row", coefficients="Variable", range=6,
-                         cx=2, cy=4),
-        grid=(16384, 8192, 1), sweeps=200, value_range=(-1.0, 1.0), mask_kind="normal_over_S",
-        launch=Launch(block=(32, 4, 1), variant="march"), reference=((2, 4, 1), (32, 4, 1))),
+    name: Workload(name=name, spec=_spec_of(p["stencil"]), grid=tuple(p["grid"]), sweeps=p["sweeps"],
+                   value_range=tuple(p["value_range"]), mask_kind=p["mask_kind"], seed=p["seed"],
+                   launch=Launch(block=tuple(p["launch"]["block"]), variant=p["launch"]["variant"]),
+                   reference=tuple(p["reference"]))
+    for name, p in P.SINGLE.items()
 }
 
-DEFAULT_WORKLOAD = "3d_star_var_r4_512"
+DEFAULT_WORKLOAD = P.DEFAULT
 
 
 @dataclass(frozen=True)
@@ -124,12 +109,7 @@ class BatchWorkload:
 
     def sides(self) -> list:
         """Grid extents (nx, ny, nz) per grid, drawn per axis from default_rng(seed)."""
-        rng = np.random.default_rng(self.seed)
-        lo, hi = self.side_range
-        u = rng.uniform(np.log(lo), np.log(hi), size=(self.n_grids, 3))
-        s = np.rint(np.exp(u) / self.multiple).astype(np.int64) * self.multiple
-        s = np.clip(s, lo, hi)
-        return [tuple(int(v) for v in row) for row in s]
+        return P.batch_sides(self.n_grids, self.side_range, self.multiple, self.seed)
 
     def geometries(self, spec: StencilSpec | None = None) -> list:
         spec = spec or self.spec
@@ -137,8 +117,7 @@ class BatchWorkload:
 
     def make_inputs(self, geoms, dtype=np.float64) -> list:
         """Values uniform [0, 1) per grid (one stream of draws, grid after grid)."""
-        rng = np.random.default_rng(self.seed + 1)
-        return [rng.random(g.shape, dtype=np.float64).astype(dtype, copy=False) for g in geoms]
+        return P.batch_inputs(self.seed, [g.shape for g in geoms], dtype)
 
     def tuned_launch(self, precision: str = "f64") -> Launch:
         """Launch chosen by the autotuner for this batch (per precision), else the default."""
@@ -151,11 +130,7 @@ class BatchWorkload:
 
 
 BATCH_WORKLOADS = {
-    # 64 independent 3D Star Jacobi r2 grids, sides log-uniform in [64, 256] (multiples of the
-    # coarsening 2x2x2), values U[0,1), 50 sweeps per run, FP64 and FP32
-    "batch_3d_star_jacobi_r2_64": BatchWorkload(
-        name="batch_3d_star_jacobi_r2_64",
-        spec=StencilSpec(dimension=3, neighbourhood="Star", orientation="Row", coefficients="Jacobi", range=2,
-                         cx=2, cy=2, cz=2),
-        n_grids=64, side_range=(64, 256), multiple=2, sweeps=50),
+    name: BatchWorkload(name=name, spec=_spec_of(p["stencil"]), n_grids=p["n_grids"],
+                        side_range=tuple(p["side_range"]), multiple=p["multiple"], sweeps=p["sweeps"], seed=p["seed"])
+    for name, p in P.BATCH.items()
 }
