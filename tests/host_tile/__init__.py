@@ -28,13 +28,13 @@ def build(cfg, precision="f64", source="tile_host.cpp") -> ctypes.CDLL:
     }
     if precision == "f32c":  # FP32 grids, compensated accumulation
         macros["TCS_COMP"] = 1
-    src = (HERE / source).read_bytes() + (CSRC / "tcs_tile.cuh").read_bytes()
+    src = (HERE / source).read_bytes() + (HERE / "host_cuda_shim.h").read_bytes() + (CSRC / "tcs_tile.cuh").read_bytes()
     tag = hashlib.sha1(src + repr(sorted(macros.items())).encode()).hexdigest()[:16]
     OUT.mkdir(parents=True, exist_ok=True)
     so = OUT / ("tile_%s.so" % tag)
     if not so.exists():
         cmd = ["g++", "-O1", "-std=c++17", "-ffp-contract=off", "-Wno-unknown-pragmas", "-shared", "-fPIC",
-               "-I", str(CSRC)] + ["-D%s=%s" % kv for kv in macros.items()] + [str(HERE / source),
+               "-I", str(CSRC), "-I", str(HERE)] + ["-D%s=%s" % kv for kv in macros.items()] + [str(HERE / source),
                                                                               "-o", str(so) + ".tmp"]
         proc = subprocess.run(cmd, capture_output=True, text=True)
         if proc.returncode != 0:

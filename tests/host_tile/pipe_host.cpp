@@ -8,14 +8,17 @@
 #include <cmath>
 #include <cstring>
 
-#define __device__
-#define __host__
-#define __forceinline__ inline
-#define __constant__
-static inline double __fma_rn(double a, double b, double c) { return std::fma(a, b, c); }
-static inline float __fmaf_rn(float a, float b, float c) { return std::fmaf(a, b, c); }
-
+#include "host_cuda_shim.h"
 #include "tcs_tile.cuh"
+
+// Run-time element access of a slot (the kernel indexes with compile-time constants).
+template <int E = 0>
+static T slot_value_rt(tcs::PipeSlot& s, int e) {
+  if constexpr (E + 1 < tcs::NEP) {
+    if (e != E) return slot_value_rt<E + 1>(s, e);
+  }
+  return tcs::slot_value<E>(s);
+}
 
 // Plane reader with the kernel's interface (pairs are just two scalar loads here).
 struct HostPlane {
@@ -52,34 +55,34 @@ extern "C" int pipe_sweep(const unsigned grid[3], unsigned left_offset, unsigned
       for (long long ms = R; ms < m_lim; ms += piece) {
         const long long me = (ms + piece < m_lim) ? ms + piece : m_lim;
         const long long np = me - ms + 2 * R;
-        T acc[NP2][NEP];
+        PipeSlot acc[NP2];
         // super-steps of `unroll` planes; slots re-aligned after each, as in tcs_pipe
         for (long long pi = 0; pi < np; ++pi) {
           const long long p = ms - R + pi;
           const T* base = in + x + (DIM == 3 ? y * xdim : 0) + p * plane;
           const HostPlane ld{base, xdim};
           const int t = (int)(pi % unroll);
-          auto slot = [&](auto kk) -> T(&)[NEP] {
+          auto slot = [&](auto kk) -> PipeSlot& {
             constexpr int k = decltype(kk)::value;
             return acc[((t - k) % NP2 + NP2) % NP2];
           };
           pipe_plane(ld, slot);
           const long long op = pi - 2 * R;
           if (op >= 0 && op < me - ms) {
-            T(&done)[NEP] = acc[((t - 2 * R) % NP2 + NP2) % NP2];
+            PipeSlot& done = acc[((t - 2 * R) % NP2 + NP2) % NP2];
             constexpr T c = T(1) / T(S);
             T* o = out + x + (DIM == 3 ? y * xdim : 0) + (ms + op) * plane;
             for (int ey = 0; ey < (DIM == 3 ? CY : 1); ++ey)
               for (int ex = 0; ex < CX; ++ex) {
                 const int e = ex + ey * CX;
-                o[ex + ey * xdim] = (COEFF == 0) ? done[e] * c : done[e];
+                const T v = slot_value_rt(done, e);
+                o[ex + ey * xdim] = (COEFF == 0) ? v * c : v;
               }
           }
           if (t == (int)unroll - 1 && unroll % NP2 != 0) {
-            T tmp[NP2][NEP];
+            PipeSlot tmp[NP2];
             std::memcpy(tmp, acc, sizeof(acc));
-            for (int m = 0; m < NP2; ++m)
-              for (int e = 0; e < NEP; ++e) acc[m][e] = tmp[(m + unroll) % NP2][e];
+            for (int m = 0; m < NP2; ++m) acc[m] = tmp[(m + unroll) % NP2];
           }
         }
       }

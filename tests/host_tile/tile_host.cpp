@@ -9,13 +9,7 @@
 #include <cmath>
 #include <cstring>
 
-#define __device__
-#define __host__
-#define __forceinline__ inline
-#define __constant__
-static inline double __fma_rn(double a, double b, double c) { return std::fma(a, b, c); }
-static inline float __fmaf_rn(float a, float b, float c) { return std::fmaf(a, b, c); }
-
+#include "host_cuda_shim.h"
 #include "tcs_tile.cuh"
 
 extern "C" int tile_sweep(const unsigned grid[3], unsigned left_offset, unsigned right_offset,

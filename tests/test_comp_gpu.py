@@ -86,3 +86,57 @@ def test_compensated_fp32_rejects_the_pipe_kernel(tcs):
     with pytest.raises(tcs.UnsupportedLaunch):
         st.update_grid(geom, x, x.clone(), tcs.Launch(block=(16, 4, 1), variant="pipe"))
     st.update_grid(geom, x, x.clone(), tcs.Launch(block=(16, 4, 1)))  # auto: march or direct
+
+
+PIPE_COMP_CASES = [
+    ((2, "Box", "Row", "Variable", 6, 4, 1, 1, "None", 0), (32, 1, 1), (301, 207, 1)),
+    ((2, "Box", "Row", "Jacobi", 3, 8, 1, 1, "Read", 16), (32, 1, 1), (400, 90, 1)),
+    ((3, "Box", "Row", "Variable", 2, 2, 2, 1, "Read", 16), (32, 4, 1), (90, 44, 30)),
+]
+
+
+@pytest.mark.parametrize("case", PIPE_COMP_CASES, ids=lambda c: "%dD_%s_%s_r%d_c%d" % (c[0][0], c[0][1], c[0][3], c[0][4], c[0][5]))
+def test_pipe_compensated_rows_within_bound(tcs, case):
+    """The pipelined kernel's compensated FP32 form (packed Box path, row partials combined by
+    two-sum): |f32c - exact| <= 3u|exact| + (2R + 2) u sum|mask||in| per point (u = 2^-24), and
+    better than plain FP32 on Variable stencils."""
+    import torch
+
+    cfg, block, sides = case
+    rng = np.random.default_rng(40 + cfg[4])
+    out = {}
+    S = G.spec_of(cfg).stencil_size
+    for prec in ("f32c", "f32"):
+        spec = G.spec_of(cfg, prec)
+        st = tcs.Stencil(spec)
+        geom = spec.geometry(*sides[:cfg[0]])
+        if prec == "f32c":
+            a = rng.uniform(-1, 1, geom.shape).astype(np.float32)
+            mask = rng.standard_normal(S) / S if cfg[3] == "Variable" else None
+        if mask is not None:
+            st.copy_mask(mask)
+        launch = tcs.Launch(block=block, variant="pipe")
+        assert st.plan(geom, launch).variant == "pipe"
+        x = torch.from_numpy(a).cuda()
+        y = x.clone()
+        st.sweeps(geom, x, y, 1, launch)
+        torch.cuda.synchronize()
+        assert st.device_status() == 0
+        out[prec] = y.cpu().numpy().astype(np.float64)
+    m32 = None if mask is None else mask.astype(np.float32).astype(np.float64)
+    exact = O.sweep(O.make_spec(*cfg), a.astype(np.float64), geom.right_offset, m32)
+    absm = None if m32 is None else np.abs(m32)
+    mag = O.sweep(O.make_spec(*cfg), np.abs(a.astype(np.float64)), geom.right_offset, absm)
+    if cfg[3] == "Jacobi":  # FP32 sweeps scale by fl32(1/S)
+        f = np.float64(np.float32(1.0 / S)) * S
+        exact, mag = exact * f, mag * f
+    sl = geom.interior_slices(cfg[4])
+    u = 2.0 ** -24
+    bound = 3 * u * np.abs(exact[sl]) + (2 * cfg[4] + 2) * u * mag[sl]
+    err = np.abs(out["f32c"][sl] - exact[sl])
+    assert np.all(err <= bound), float((err / bound).max())
+    if cfg[3] == "Variable":
+        assert err.max() < np.abs(out["f32"][sl] - exact[sl]).max()
+    outside = np.ones(geom.shape, dtype=bool)
+    outside[sl] = False
+    assert np.array_equal(out["f32c"][outside], a.astype(np.float64)[outside])

@@ -119,6 +119,75 @@ def test_pipe_arithmetic_matches_oracle_random(cfg, precision):
     assert np.array_equal(got, want)
 
 
+PAIR_CFGS = [
+    (2, "Box", "Row", "Variable", 6, 4, 1, 1, "None", 0),
+    (2, "Box", "Row", "Variable", 3, 8, 1, 1, "Read", 16),
+    (2, "Box", "Row", "Jacobi", 1, 2, 1, 1, "Write", 8),
+    (3, "Box", "Row", "Jacobi", 1, 2, 2, 1, "None", 0),
+    (3, "Box", "Row", "Variable", 2, 2, 1, 1, "Write", 16),
+    (3, "Box", "Row", "Variable", 1, 4, 2, 1, "Read", 8),
+]
+
+
+@pytest.mark.parametrize("cfg", PAIR_CFGS, ids=ref_configs.key)
+def test_pipe_packed_fp32_pairs_match_oracle(cfg):
+    """FP32 Box Row stencils with an even x coarsening take the packed-pair path (two outputs per
+    f32x2 instruction, lane by lane the scalar rounding): bit-identical to the float oracle."""
+    d, sh, o, c, r, cx, cy, cz, al, cl = cfg
+    spec = O.make_spec(*cfg)
+    g = O.geometry(spec, 23 + 2 * r + 3 * cx, 19 + 2 * r, 11 + 2 * r)
+    rng = np.random.default_rng(21)
+    shape = (g.grid[1], g.grid[0]) if d == 2 else (g.grid[2], g.grid[1], g.grid[0])
+    a = rng.uniform(-1, 1, shape).astype(np.float32)
+    mask = rng.standard_normal(O.stencil_size(spec)) if c == "Variable" else None
+    want = O.sweeps(spec, a, 3, g.right_offset, mask)
+    for piece, unroll in ((1 << 30, 1), (5, 2), (4, 3)):
+        got = host_tile.pipe_sweeps(cfg, a, g.grid, g.left_offset, g.right_offset, 3, mask, "f32", piece=piece,
+                                    unroll=unroll)
+        assert np.array_equal(got, want)
+
+
+COMP_PAIR_CFGS = [
+    (2, "Box", "Row", "Variable", 6, 4, 1, 1, "None", 0),
+    (2, "Box", "Row", "Jacobi", 3, 2, 1, 1, "None", 0),
+    (3, "Box", "Row", "Variable", 2, 2, 2, 1, "Read", 16),
+]
+
+
+@pytest.mark.parametrize("cfg", COMP_PAIR_CFGS, ids=ref_configs.key)
+def test_pipe_compensated_rows_within_bound(cfg):
+    """The pipelined kernel's compensated FP32 form (packed Box path): each footprint row's 2R+1
+    terms are summed with plain FMAs, the row partials with two-sum.  Per point, against the float64
+    oracle on the same FP32 inputs and FP32-rounded mask:
+        |f32c - exact| <= 3u |exact| + (2R + 2) u sum |mask| |in|,   u = 2^-24,
+    and plain FP32 (bound (S + 1) u sum |mask| |in|) does worse on the long stencil."""
+    d, sh, o, c, r, cx, cy, cz, al, cl = cfg
+    spec = O.make_spec(*cfg)
+    g = O.geometry(spec, 21 + 2 * r + 3 * cx, 17 + 2 * r, 9 + 2 * r)
+    rng = np.random.default_rng(31)
+    shape = (g.grid[1], g.grid[0]) if d == 2 else (g.grid[2], g.grid[1], g.grid[0])
+    a = rng.uniform(-1, 1, shape).astype(np.float32)
+    S = O.stencil_size(spec)
+    mask = rng.standard_normal(S) / S if c == "Variable" else None
+    got = host_tile.pipe_sweeps(cfg, a, g.grid, g.left_offset, g.right_offset, 1, mask, "f32c", piece=5,
+                                unroll=2).astype(np.float64)
+    plain = host_tile.pipe_sweeps(cfg, a, g.grid, g.left_offset, g.right_offset, 1, mask, "f32", piece=5,
+                                  unroll=2).astype(np.float64)
+    m32 = None if mask is None else mask.astype(np.float32).astype(np.float64)
+    exact = O.sweep(spec, a.astype(np.float64), g.right_offset, m32)
+    absm = None if m32 is None else np.abs(m32)
+    mag = O.sweep(spec, np.abs(a.astype(np.float64)), g.right_offset, absm)
+    u = 2.0 ** -24
+    if c == "Jacobi":  # the oracle scales by the double 1/S; the FP32 sweeps by fl32(1/S)
+        exact = exact * (np.float64(np.float32(1.0 / S)) * S)
+        mag = mag * (np.float64(np.float32(1.0 / S)) * S)
+    bound = 3 * u * np.abs(exact) + (2 * r + 2) * u * mag
+    err = np.abs(got - exact)
+    assert np.all(err <= bound), float((err / bound).max())
+    if c == "Variable":
+        assert err.max() < np.abs(plain - exact).max()
+
+
 PIPE_CASES = [
     (2, "Box", 1, (1, 1, 1), (32, 1, 1), (70, 23, 1), "None", 0),
     (2, "Box", 6, (2, 1, 1), (16, 1, 1), (80, 40, 1), "None", 0),

@@ -671,11 +671,18 @@ unsigned pipe_loader(const tcs_spec& s, unsigned long long xdim, const void* in)
   return pipe_loader_cp(s, xdim, in);
 }
 
+// The pipelined kernel's compensated FP32 form is the packed-pair Box path (tcs_tile.cuh):
+// Box neighbourhood, Row order (or 2D), even x coarsening.
+bool pipe_comp_ok(const tcs_spec& s) {
+  return s.neighbourhood == TCS_BOX && s.cx % 2 == 0 && (s.dimension == 2 || s.orientation == TCS_ROW);
+}
+
 int resolve_pipe(tcs_stencil* h, const TcsGeo& g, const tcs_launch* L, Resolved& out,
                  bool batch = false) {
   const tcs_spec& s = h->spec;
-  if (s.precision == TCS_F32C)
-    return fail(TCS_ERR_UNSUPPORTED, "compensated FP32 runs on the direct kernel only");
+  if (s.precision == TCS_F32C && !pipe_comp_ok(s))
+    return fail(TCS_ERR_UNSUPPORTED,
+                "compensated FP32 pipelined sweeps need a Box stencil in Row order with an even x coarsening");
   const unsigned R = (unsigned)s.range;
   const unsigned es = (unsigned)elem_size(s);
   const unsigned vec = 16u / es;
@@ -1488,6 +1495,8 @@ int precompile_pipe(const tcs_spec* spec, unsigned bx, unsigned by, unsigned chu
   if (s.dimension == 2) s.cz = 1;
   if (s.dimension == 2 && s.orientation == TCS_COLUMN)
     return fail(TCS_ERR_UNSUPPORTED, "2D Column orientation is not pipelined");
+  if (s.precision == TCS_F32C && !pipe_comp_ok(s))
+    return fail(TCS_ERR_UNSUPPORTED, "compensated FP32 pipelined sweeps need the packed Box path");
   const unsigned vec = 16u / (unsigned)elem_size(s);
   if (bx == 0 || (bx * (unsigned)s.cx) % vec != 0)
     return fail(TCS_ERR_UNSUPPORTED, "pipe: unsupported block");

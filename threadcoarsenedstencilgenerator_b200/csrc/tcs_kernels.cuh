@@ -509,6 +509,7 @@ constexpr int PLANE = PW * ROWS;     // elements per plane
 constexpr int CHUNK = CHP * PLANE;   // elements per ring slot
 constexpr int NP2 = 2 * R + 1;       // pipeline depth (output planes in flight)
 static_assert(!(DIM == 2 && ORIENT == 1), "2D Column orientation is not pipelined");
+static_assert(!COMP || PAIRS, "compensated pipelined sweeps take the packed Box path only");
 static_assert(CHP >= 1, "planes per chunk");
 static_assert(TXP % VEC == 0, "tile width must be a multiple of the 16-byte granule");
 // Columns whose element index is even for every thread: the thread origin sits at ring column
@@ -628,7 +629,7 @@ struct PipeState {
 // Every piece consumes all chunks it issues, so the loader may change from piece to piece.
 template <bool MIXED>
 __device__ __forceinline__ bool pipe_piece(const PipeGridView& G, tcs_u32 tile, tcs_u32 zs,
-                                           tcs_u32 ze, PipeState& st, T (&acc)[NP2][NEP]) {
+                                           tcs_u32 ze, PipeState& st, PipeSlot (&acc)[NP2]) {
   constexpr tcs_u32 NTHREADS = BX * BY;
   constexpr tcs_u32 CHUNK_BYTES = CHUNK * (tcs_u32)sizeof(T);
   const tcs_u32 nslot = st.nslot, tid = st.tid, bars = st.bars, gc = st.gc;
@@ -733,7 +734,7 @@ __device__ __forceinline__ bool pipe_piece(const PipeGridView& G, tcs_u32 tile, 
       const tcs_u32 pi = pbase + t;
       if (pi < np) {
         const PipeRing ld{pc + t * PLANE};
-        auto slot = [&](auto kk) -> T(&)[NEP] {
+        auto slot = [&](auto kk) -> PipeSlot& {
           constexpr int k = decltype(kk)::value;
           return acc[((t - k) % NP2 + NP2) % NP2];
         };
@@ -741,7 +742,7 @@ __device__ __forceinline__ bool pipe_piece(const PipeGridView& G, tcs_u32 tile, 
         const int op = (int)pi - 2 * R;
         if (lane_ok && op >= 0 && op < (int)nout) {
           constexpr T c = T(1) / T(S);
-          T(&done)[NEP] = acc[((t - 2 * R) % NP2 + NP2) % NP2];
+          PipeSlot& done = acc[((t - 2 * R) % NP2 + NP2) % NP2];
           T* orow = optr + (tcs_i64)t * plane_g;
           // Output x is R + leftOff + an even offset when CX is even: pairs are aligned when
           // R + LSHIFT is even (the shared-memory pair rule at gx = 0).
@@ -753,8 +754,8 @@ __device__ __forceinline__ bool pipe_piece(const PipeGridView& G, tcs_u32 tile, 
               T* o = orow + decltype(ex)::value + decltype(ey)::value * (tcs_i64)G.xdim;
               const T* so = G.src ? G.src + (o - G.out) : nullptr;
               if constexpr (pair) {
-                T v0 = (COEFF == 0) ? done[e] * c : done[e];
-                T v1 = (COEFF == 0) ? done[e + 1] * c : done[e + 1];
+                T v0 = (COEFF == 0) ? slot_value<e>(done) * c : slot_value<e>(done);
+                T v1 = (COEFF == 0) ? slot_value<e + 1>(done) * c : slot_value<e + 1>(done);
                 if (so) {
                   v0 = v0 + so[0];
                   v1 = v1 + so[1];
@@ -769,7 +770,7 @@ __device__ __forceinline__ bool pipe_piece(const PipeGridView& G, tcs_u32 tile, 
                   o[1] = v1;
                 }
               } else if constexpr (!tail) {
-                T v = (COEFF == 0) ? done[e] * c : done[e];
+                T v = (COEFF == 0) ? slot_value<e>(done) * c : slot_value<e>(done);
                 if (so) v = v + so[0];
                 *o = v;
               }
@@ -780,18 +781,9 @@ __device__ __forceinline__ bool pipe_piece(const PipeGridView& G, tcs_u32 tile, 
     });
     // Re-align the register slots with the next chunk: slot m takes what slot (m + CHP) held.
     if constexpr (CHP % NP2 != 0) {
-      T tmp[NP2][NEP];
-      static_for<0, NP2>([&](auto m) {
-        static_for<0, NEP>([&](auto e) {
-          tmp[decltype(m)::value][decltype(e)::value] = acc[decltype(m)::value][decltype(e)::value];
-        });
-      });
-      static_for<0, NP2>([&](auto m) {
-        static_for<0, NEP>([&](auto e) {
-          acc[decltype(m)::value][decltype(e)::value] =
-              tmp[(decltype(m)::value + CHP) % NP2][decltype(e)::value];
-        });
-      });
+      PipeSlot tmp[NP2];
+      static_for<0, NP2>([&](auto m) { tmp[decltype(m)::value] = acc[decltype(m)::value]; });
+      static_for<0, NP2>([&](auto m) { acc[decltype(m)::value] = tmp[(decltype(m)::value + CHP) % NP2]; });
     }
     optr += (tcs_i64)CHP * plane_g;
     if (++cur_slot == nslot) {
@@ -851,7 +843,7 @@ extern "C" __global__ void __launch_bounds__(TCS_BX * ((TCS_DIM == 3) ? TCS_BY :
   G.st_pair = (g.xdim % 2 == 0) && (reinterpret_cast<tcs_u64>(out) % (2 * sizeof(T)) == 0);
   if (G.use_tma && threadIdx.x == 0 && threadIdx.y == 0) tma_prefetch_map(&tmap);
   PipeState st = pipe_setup(g.nslot, G.use_tma);
-  T acc[NP2][NEP];
+  PipeSlot acc[NP2];
   const tcs_u64 w_begin = (tcs_u64)blockIdx.x * g.per_cta;
   const tcs_u64 w_end = min(w_begin + g.per_cta, g.total);
   for (tcs_u64 w = w_begin; w < w_end;) {
@@ -875,7 +867,7 @@ extern "C" __global__ void __launch_bounds__(TCS_BX * ((TCS_DIM == 3) ? TCS_BY :
                    const tcs_u64 total, const tcs_u64 per_cta, const tcs_u32 nslot) {
   using namespace tcs;
   PipeState st = pipe_setup(nslot, false);
-  T acc[NP2][NEP];
+  PipeSlot acc[NP2];
   const tcs_u64 w_begin = (tcs_u64)blockIdx.x * per_cta;
   const tcs_u64 w_end = min(w_begin + per_cta, total);
   tcs_u32 gi = 0;

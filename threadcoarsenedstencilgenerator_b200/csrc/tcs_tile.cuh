@@ -316,27 +316,143 @@ __device__ __forceinline__ void store(T* __restrict__ o, const Acc (&acc)[NE], t
 namespace tcs {
 constexpr int NEP = (DIM == 3) ? CX * CY : CX;  // outputs per thread and plane
 
-template <int GX, int GY, int DZ>
-__device__ __forceinline__ void apply_slot(T (&acc)[NEP], const T v) {
+// Packed FP32 arithmetic (sm_100 `fma.rn.f32x2`, `add`/`mul` likewise): one instruction applies a
+// term to two outputs, each lane rounded exactly as the scalar fmaf/add/mul, so results stay
+// bit-identical.  Used for FP32 Box stencils in Row order with an even x coarsening: the outputs
+// (2p, 2p+1) of a thread row receive the same term (rx, ry, rz) -- same mask coefficient -- from
+// the neighbouring input values (row[2p + rx + R], row[2p + 1 + rx + R]).
+#ifndef TCS_PAIRS
+#define TCS_PAIRS 1
+#endif
+constexpr bool PAIRS = (TCS_PAIRS != 0) && sizeof(T) == 4 && SHAPE == 0 && CX % 2 == 0 &&
+                       (DIM == 2 || ORIENT == 0);
+constexpr int NPAIR = (NEP / 2 > 0) ? NEP / 2 : 1;
+
+// The accumulators of one output plane of a thread: NEP scalars, or NEP/2 packed pairs (output
+// e = ex + ey*CX is lane e%2 of pair e/2).  The compensated form (FP32 grids, TCS_COMP) keeps, per
+// pair, the running sum `p` and the collected rounding errors `c`; the value is p + c.
+template <bool P, bool C>
+struct PipeSlotT {
+  T v[NEP];
+  template <int E>
+  __device__ __forceinline__ T& at() { return v[E]; }
+};
+template <>
+struct PipeSlotT<true, false> {
+  float2 p[NPAIR];
+  template <int E>
+  __device__ __forceinline__ float& at() {
+    if constexpr (E % 2 == 0)
+      return p[E / 2].x;
+    else
+      return p[E / 2].y;
+  }
+  template <int E>
+  __device__ __forceinline__ float value() const {
+    return (E % 2 == 0) ? p[E / 2].x : p[E / 2].y;
+  }
+};
+template <>
+struct PipeSlotT<true, true> {
+  float2 p[NPAIR], c[NPAIR];
+  template <int E>
+  __device__ __forceinline__ float value() const {
+    return (E % 2 == 0) ? p[E / 2].x + c[E / 2].x : p[E / 2].y + c[E / 2].y;
+  }
+};
+typedef PipeSlotT<PAIRS, PAIRS && COMP> PipeSlot;
+
+// Value of output e of a slot (the compensated sum where there is one).
+template <int E, class SL>
+__device__ __forceinline__ T slot_value(SL& s) {
+  if constexpr (PAIRS)
+    return s.template value<E>();
+  else
+    return s.template at<E>();
+}
+
+template <int GX, int GY, int DZ, class SL>
+__device__ __forceinline__ void apply_slot(SL& acc, const T v) {
   static_for<0, (DIM == 3) ? CY : 1>([&](auto ey) {
     static_for<0, CX>([&](auto ex) {
       constexpr int rx = GX - decltype(ex)::value;
       constexpr int ry = (DIM == 3) ? GY - decltype(ey)::value : DZ;
       constexpr int rz = (DIM == 3) ? DZ : 0;
       constexpr int e = decltype(ex)::value + decltype(ey)::value * CX;
+      T& a = acc.template at<e>();
       if constexpr (contributes(rx, ry, rz)) {
         if constexpr (is_first(rx, ry, rz)) {
-          acc[e] = v;
+          a = v;
         } else if constexpr (COEFF == 0) {
-          acc[e] = acc[e] + v;
+          a = a + v;
         } else if constexpr (is_second(rx, ry, rz)) {
-          acc[e] = fmat(acc[e], tcs_mask[first_mask_index()], v * tcs_mask[mask_index(rx, ry, rz)]);
+          a = fmat(a, tcs_mask[first_mask_index()], v * tcs_mask[mask_index(rx, ry, rz)]);
         } else {
-          acc[e] = fmat(v, tcs_mask[mask_index(rx, ry, rz)], acc[e]);
+          a = fmat(v, tcs_mask[mask_index(rx, ry, rz)], a);
         }
       }
     });
   });
+}
+
+// One term (rx, ry, rz) applied to a pair of outputs with the packed instructions; the same
+// first-term / second-term rules as apply_slot, lane by lane.
+template <int RX, int RY, int RZ>
+__device__ __forceinline__ void apply_pair(float2& a, const float2 v) {
+  if constexpr (is_first(RX, RY, RZ)) {
+    a = v;
+  } else if constexpr (COEFF == 0) {
+    a = __fadd2_rn(a, v);
+  } else {
+    const float m = tcs_mask[mask_index(RX, RY, RZ)];
+    if constexpr (is_second(RX, RY, RZ)) {
+      const float m0 = tcs_mask[first_mask_index()];
+      a = __ffma2_rn(a, make_float2(m0, m0), __fmul2_rn(v, make_float2(m, m)));
+    } else {
+      a = __ffma2_rn(v, make_float2(m, m), a);
+    }
+  }
+}
+
+// Compensated form: the terms of one footprint row of an output (2R+1 of them, rx ascending) are
+// summed with plain packed FMAs into a row partial q (q = v*m, then q = fma(v, m, q); Jacobi: sums
+// of the values); the row partial is then added to the running sum p with Knuth's two-sum and its
+// rounding error collected in c.  Error: |value - exact| <= u|exact| + gamma_{2R+1} sum|terms|
+// + O(u^2) (u = 2^-24), against gamma_S sum|terms| for the plain FP32 sweep.
+template <int RX, int RY, int RZ>
+__device__ __forceinline__ void row_term_pair(float2& q, const float2 v) {
+  if constexpr (RX == -R) {
+    if constexpr (COEFF == 0) {
+      q = v;
+    } else {
+      const float m = tcs_mask[mask_index(RX, RY, RZ)];
+      q = __fmul2_rn(v, make_float2(m, m));
+    }
+  } else if constexpr (COEFF == 0) {
+    q = __fadd2_rn(q, v);
+  } else {
+    const float m = tcs_mask[mask_index(RX, RY, RZ)];
+    q = __ffma2_rn(v, make_float2(m, m), q);
+  }
+}
+
+// Knuth's two-sum of (p, q), lane by lane: p <- fl(p + q), c += the exact rounding error.  The
+// differences are fma(x, -1, y) = fl(y - x), one rounding each, as the scalar subtractions.
+template <bool FIRST_ROW>
+__device__ __forceinline__ void two_sum_pair(float2& p, float2& c, const float2 q) {
+  if constexpr (FIRST_ROW) {
+    p = q;
+    c = make_float2(0.f, 0.f);
+  } else {
+    const float2 m1 = make_float2(-1.f, -1.f);
+    const float2 t = __fadd2_rn(p, q);
+    const float2 z = __ffma2_rn(p, m1, t);       // t - p
+    const float2 tz = __ffma2_rn(z, m1, t);      // t - z
+    const float2 e1 = __ffma2_rn(tz, m1, p);     // p - (t - z)
+    const float2 e2 = __ffma2_rn(z, m1, q);      // q - z
+    c = __fadd2_rn(c, __fadd2_rn(e1, e2));
+    p = t;
+  }
 }
 
 // Load the row segment gx in [GX0, GX0 + N) of in-plane row GY into registers.  The loader says
@@ -363,7 +479,66 @@ __device__ __forceinline__ void load_row(const LD& ld, T (&v)[N]) {
 // `slot(ic<k>)` returns the accumulators of the output at march-axis offset k - R.
 template <class LD, class SLOTS>
 __device__ __forceinline__ void pipe_plane(const LD& ld, SLOTS&& slot) {
-  if constexpr (SHAPE == 0) {
+  if constexpr (SHAPE == 0 && PAIRS && COMP) {
+    // Box, packed FP32, compensated: per input row and slot, the row partial of each output pair
+    // (rx ascending), then one two-sum into the slot's running sum.
+    constexpr int NY = (DIM == 3) ? 2 * R + CY : 1;
+    constexpr int OY = (DIM == 3) ? R : 0;
+    static_for<0, NY>([&](auto iy) {
+      constexpr int gy = decltype(iy)::value - OY;
+      T row[2 * R + CX];
+      load_row<gy, -R, 2 * R + CX>(ld, row);
+      static_for<0, 2 * R + 1>([&](auto k) {
+        constexpr int dz = decltype(k)::value - R;
+        auto& s = slot(k);
+        static_for<0, (DIM == 3) ? CY : 1>([&](auto ey) {
+          constexpr int ry = (DIM == 3) ? gy - decltype(ey)::value : dz;
+          constexpr int rz = (DIM == 3) ? dz : 0;
+          if constexpr (contributes(0, ry, rz)) {
+            static_for<0, CX / 2>([&](auto pp) {
+              constexpr int e = decltype(ey)::value * (CX / 2) + decltype(pp)::value;
+              float2 q;
+              static_for<0, 2 * R + 1>([&](auto rxi) {
+                constexpr int rx = decltype(rxi)::value - R;
+                constexpr int j = 2 * decltype(pp)::value + rx + R;
+                row_term_pair<rx, ry, rz>(q, make_float2(row[j], row[j + 1]));
+              });
+              // the first row of an output starts its sum (ry = rz = -R)
+              two_sum_pair<(ry == -R && (DIM == 2 || rz == -R))>(s.p[e], s.c[e], q);
+            });
+          }
+        });
+      });
+    });
+  } else if constexpr (SHAPE == 0 && PAIRS) {
+    // Box, packed FP32: per input row, every term rx feeds every slot and every output pair.  For a
+    // fixed output the terms still arrive row by row and, within a row, rx ascending.
+    constexpr int NY = (DIM == 3) ? 2 * R + CY : 1;
+    constexpr int OY = (DIM == 3) ? R : 0;
+    static_for<0, NY>([&](auto iy) {
+      constexpr int gy = decltype(iy)::value - OY;
+      T row[2 * R + CX];
+      load_row<gy, -R, 2 * R + CX>(ld, row);
+      static_for<0, 2 * R + 1>([&](auto rxi) {
+        constexpr int rx = decltype(rxi)::value - R;
+        static_for<0, 2 * R + 1>([&](auto k) {
+          constexpr int dz = decltype(k)::value - R;
+          auto& s = slot(k);
+          static_for<0, (DIM == 3) ? CY : 1>([&](auto ey) {
+            constexpr int ry = (DIM == 3) ? gy - decltype(ey)::value : dz;
+            constexpr int rz = (DIM == 3) ? dz : 0;
+            if constexpr (contributes(rx, ry, rz)) {
+              static_for<0, CX / 2>([&](auto pp) {
+                constexpr int j = 2 * decltype(pp)::value + rx + R;  // row index of lane 0's value
+                constexpr int e = decltype(ey)::value * (CX / 2) + decltype(pp)::value;
+                apply_pair<rx, ry, rz>(s.p[e], make_float2(row[j], row[j + 1]));
+              });
+            }
+          });
+        });
+      });
+    });
+  } else if constexpr (SHAPE == 0) {
     // Box: every in-plane footprint point feeds every slot, in the slice traversal order.
     constexpr int NY = (DIM == 3) ? 2 * R + CY : 1;
     constexpr int OY = (DIM == 3) ? R : 0;
