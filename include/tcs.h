@@ -232,6 +232,10 @@ int tcs_precompile(const tcs_spec* spec, char* cubin_path, unsigned path_cap);
 int tcs_precompile_pipe(const tcs_spec* spec, unsigned bx, unsigned by, unsigned chunk,
                         char* cubin_path, unsigned path_cap);
 
+/* Same with an epilogue: 1 = the FP64 defect sweep, 2 = the FP32 accumulating sweep. */
+int tcs_precompile_pipe_epilogue(const tcs_spec* spec, unsigned bx, unsigned by, unsigned chunk, unsigned epi,
+                                 char* cubin_path, unsigned path_cap);
+
 /* ---- Mixed-precision helpers (FP64 defect correction of FP32 sweeps) ----
  * All act on the interior of buffers laid out like the sweep buffers (gridSize, rightOffset).
  * They are additions of this engine; the reference computes in FP64 only. */
@@ -241,6 +245,24 @@ int tcs_precompile_pipe(const tcs_spec* spec, unsigned bx, unsigned by, unsigned
 int tcs_update_grid_source(tcs_stencil* h, const unsigned grid[3], unsigned right_offset,
                            const tcs_launch* launch, const void* in, const void* src, void* out,
                            void* stream);
+
+/* Fused defect-correction sweeps on the pipelined kernel (variant TCS_VARIANT_AUTO or
+ * TCS_VARIANT_PIPE; grids of whole coarsening tiles; TCS_ERR_UNSUPPORTED otherwise).
+ * tcs_defect_sweep (FP64 handle): one sweep of x whose epilogue writes the defect
+ * r = fl32(S(x) - x) on the interior and, when norms != NULL, the norms {max |S(x) - x|,
+ * ||S(x) - x||_2} in FP64 (synchronises `stream`).  S(x) itself is never stored.  r is
+ * bit-identical to tcs_update_grid into a buffer sx followed by tcs_residual(x, sx); the 2-norm is
+ * summed per thread and per CTA, so its last bits may differ from tcs_residual's.  The per-CTA
+ * partials live in the handle's scratch memory.
+ * tcs_update_grid_accumulate (FP32 handle): x += (double)(S(in) + src) on the interior, with x the
+ * FP64 state (src may be NULL): the last correction sweep of a period and the accumulation into
+ * the state in one pass, bit-identical to tcs_update_grid_source into e followed by
+ * tcs_accumulate(x, e).  The current device must be the handle's. */
+int tcs_defect_sweep(tcs_stencil* h, const unsigned grid[3], unsigned right_offset, const tcs_launch* launch,
+                     const void* x, float* r, double norms[2], void* stream);
+int tcs_update_grid_accumulate(tcs_stencil* h, const unsigned grid[3], unsigned right_offset,
+                               const tcs_launch* launch, const void* in, const void* src, double* x,
+                               void* stream);
 
 /* FP64 defect r = fl32(sx - x) (sx = one FP64 sweep of x) and, when norms != NULL, the global
  * residual norms {max |sx - x|, ||sx - x||_2} computed on the GPU in FP64 (synchronises

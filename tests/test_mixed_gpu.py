@@ -124,3 +124,89 @@ def test_defect_corrected_fp32_tracks_fp64(tcs, cfg, n, period):
     s32 = dc.s64.compare(geom, res32, b, "f32")
     assert s32["max_rel"] < 1e-3
     assert dc.s64.device_status() == 0 and dc.s32.device_status() == 0
+
+
+FUSED_CASES = [
+    ((2, "Box", "Row", "Variable", 6, 4, 1, 1, "None", 0), (32, 1, 1), (300, 90, 1)),
+    ((3, "Star", "Row", "Variable", 2, 2, 2, 1, "Read", 16), (16, 4, 1), (70, 42, 30)),
+    ((3, "Box", "Row", "Jacobi", 1, 2, 1, 1, "None", 0), (32, 2, 1), (66, 20, 19)),
+]
+
+
+@pytest.mark.parametrize("case", FUSED_CASES, ids=lambda c: "%dD_%s_%s_r%d" % (c[0][0], c[0][1], c[0][3], c[0][4]))
+def test_fused_defect_and_accumulate_sweeps(tcs, case):
+    """tcs_defect_sweep == one FP64 sweep + tcs_residual (r bit for bit, max norm exact, 2-norm to
+    1e-12); tcs_update_grid_accumulate == tcs_update_grid_source + tcs_accumulate (bit for bit)."""
+    import torch
+
+    cfg, block, sides = case
+    s64 = tcs.Stencil(G.spec_of(cfg, "f64"))
+    s32 = tcs.Stencil(G.spec_of(cfg, "f32"))
+    geom = s64.spec.geometry(*sides[:cfg[0]])
+    rng = np.random.default_rng(17)
+    mask = rng.standard_normal(s64.spec.stencil_size) / s64.spec.stencil_size if cfg[3] == "Variable" else None
+    if mask is not None:
+        s64.copy_mask(mask)
+        s32.copy_mask(mask)
+    launch = tcs.Launch(block=block, variant="pipe")
+    x = torch.from_numpy(rng.uniform(-1, 1, geom.shape)).cuda()
+    sx = x.clone()
+    r_ref = torch.zeros(geom.shape, dtype=torch.float32, device="cuda")
+    r = torch.full(geom.shape, 0.0, dtype=torch.float32, device="cuda")
+    s64.update_grid(geom, x, sx, launch)
+    n_ref = s64.residual(geom, x, sx, r_ref)
+    n_fused = s64.defect_sweep(geom, x, r, launch)
+    torch.cuda.synchronize()
+    assert torch.equal(r, r_ref)
+    assert n_fused[0] == n_ref[0]
+    assert abs(n_fused[1] - n_ref[1]) <= 1e-12 * n_ref[1]
+    # accumulate: x2 += S(e) + r  against  e1 = S(e) + r; x1 += e1
+    e = torch.from_numpy(rng.standard_normal(geom.shape).astype(np.float32) * 1e-3).cuda()
+    sl = geom.interior_slices(cfg[4])
+    outside = torch.ones(geom.shape, dtype=torch.bool)
+    outside[sl] = False
+    e[outside.cuda()] = 0
+    x1, x2 = x.clone(), x.clone()
+    e1 = torch.zeros_like(e)
+    s32.update_grid_source(geom, e, r, e1, launch)
+    s64.accumulate(geom, x1, e1)
+    s32.update_grid_accumulate(geom, e, r, x2, launch)
+    # the same buffer as input and source (the first correction step of a period of two)
+    x3, x4 = x.clone(), x.clone()
+    e2 = torch.zeros_like(e)
+    s32.update_grid_source(geom, r, r, e2, launch)
+    s64.accumulate(geom, x3, e2)
+    s32.update_grid_accumulate(geom, r, r, x4, launch)
+    torch.cuda.synchronize()
+    assert s64.device_status() == 0 and s32.device_status() == 0
+    assert torch.equal(x1, x2)
+    assert torch.equal(x3, x4)
+
+
+@pytest.mark.parametrize("tensor_cores", [False, True])
+def test_fused_defect_correction_equals_unfused(tcs, tensor_cores):
+    """The fused period (defect sweep, first correction step read from r, accumulating last step)
+    gives the unfused period's state bit for bit."""
+    import torch
+
+    from threadcoarsenedstencilgenerator_b200.mixed import DefectCorrectedSweeps
+
+    cfg = (2, "Box", "Row", "Variable", 6, 4, 1, 1, "None", 0)
+    spec = G.spec_of(cfg)
+    geom = spec.geometry(520, 300)
+    rng = np.random.default_rng(23)
+    mask = rng.standard_normal(spec.stencil_size) / spec.stencil_size
+    a = rng.uniform(-1, 1, geom.shape)
+    launch = tcs.Launch(block=(32, 1, 1), variant="pipe")
+    out = []
+    for fused in (True, False):
+        dc = DefectCorrectedSweeps(spec, launch, mask=mask, tensor_cores=tensor_cores, fused=fused)
+        x = torch.from_numpy(a).cuda()
+        x, res = dc.run(geom, x, 45, 20)
+        torch.cuda.synchronize()
+        assert dc.fused == fused
+        out.append((x.cpu(), res))
+    assert torch.equal(out[0][0], out[1][0])
+    assert out[0][1].fp64_sweeps == out[1][1].fp64_sweeps == 3
+    for (m0, l0), (m1, l1) in zip(out[0][1].residual_history, out[1][1].residual_history):
+        assert m0 == m1 and abs(l0 - l1) <= 1e-12 * l1

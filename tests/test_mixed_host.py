@@ -57,9 +57,26 @@ class FakeStencil:
         sl = self._interior(geom)
         x.numpy()[sl] += e.numpy()[sl].astype(np.float64)
 
+    # the fused sweeps: the same arithmetic as the unfused pairs of calls
+    def defect_sweep(self, geom, x, r, launch=None, stream=None):
+        FakeStencil.log.append(("f64 sweep", self.spec.precision))
+        sx = O.sweep(self.ospec, x.numpy(), 0, self.mask)
+        d = sx - x.numpy()
+        sl = self._interior(geom)
+        r.numpy()[sl] = d[sl].astype(np.float32)
+        return float(np.abs(d[sl]).max()), float(np.sqrt((d[sl] ** 2).sum()))
 
-@pytest.mark.parametrize("n, period", [(45, 20), (20, 20), (7, 3), (1, 5)])
-def test_defect_correction_loop_tracks_fp64(monkeypatch, n, period):
+    def update_grid_accumulate(self, geom, a, r, x, launch=None, stream=None):
+        import torch
+
+        e = torch.zeros(a.shape, dtype=torch.float32)
+        self.update_grid_source(geom, a, r, e)
+        self.accumulate(geom, x, e)
+
+
+@pytest.mark.parametrize("fused", [True, False])
+@pytest.mark.parametrize("n, period", [(45, 20), (20, 20), (7, 3), (1, 5), (4, 2)])
+def test_defect_correction_loop_tracks_fp64(monkeypatch, n, period, fused):
     import torch
 
     monkeypatch.setattr(mixed, "Stencil", FakeStencil)
@@ -70,9 +87,14 @@ def test_defect_correction_loop_tracks_fp64(monkeypatch, n, period):
     mask = rng.random(spec.stencil_size)
     mask /= mask.sum()  # a smoothing stencil: the state settles, the corrections shrink
     a = rng.random(geom.shape)
-    dc = mixed.DefectCorrectedSweeps(spec, mask=mask)
+    dc = mixed.DefectCorrectedSweeps(spec, mask=mask, fused=fused)
     x = torch.from_numpy(a.copy())
     x, res = dc.run(geom, x, n, period=period)
+    # the fused period gives the unfused period's bits
+    FakeStencil.log = []
+    other = mixed.DefectCorrectedSweeps(spec, mask=mask, fused=not fused)
+    y, _ = other.run(geom, torch.from_numpy(a.copy()), n, period=period)
+    assert torch.equal(x, y)
     want = O.sweeps(O.make_spec(*CFG), a, n, 0, mask)
     periods = -(-n // period)
     assert res.fp64_sweeps == periods and res.fp32_sweeps == n and len(res.residual_history) == periods

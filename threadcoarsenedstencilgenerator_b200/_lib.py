@@ -134,6 +134,9 @@ SIGNATURES = {
     "tcs_update_grid_source": [_vp, U3, _u, _P(CLaunch), _vp, _vp, _vp, _vp],
     "tcs_residual": [_vp, U3, _u, _vp, _vp, _vp, _P(ctypes.c_double), _vp],
     "tcs_residual_static": [_vp, U3, _u, _vp, _vp, _vp, _P(ctypes.c_double), _u, _vp],
+    "tcs_defect_sweep": [_vp, U3, _u, _P(CLaunch), _vp, _vp, _P(ctypes.c_double), _vp],
+    "tcs_update_grid_accumulate": [_vp, U3, _u, _P(CLaunch), _vp, _vp, _vp, _vp],
+    "tcs_precompile_pipe_epilogue": [_P(CSpec), _u, _u, _u, _u, ctypes.c_char_p, _u],
     "tcs_scratch_bytes": [_vp, _P(ctypes.c_ulonglong)],
     "tcs_benchmark_durations": [_vp, _vp, _u, _P(_u)],
     "tcs_accumulate": [_vp, U3, _u, _vp, _vp, _vp],

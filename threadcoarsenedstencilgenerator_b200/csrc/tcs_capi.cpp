@@ -216,8 +216,9 @@ std::string cache_dir() {
 struct PipeKey {
   unsigned bx, by, ch, lshift;
   unsigned batch = 0;
+  unsigned epi = 0;  // epilogue mode (tcs_kernels.cuh, TCS_EPI): 0 plain, 1 FP64 defect, 2 FP32 accumulate
   bool operator==(const PipeKey& o) const {
-    return bx == o.bx && by == o.by && ch == o.ch && lshift == o.lshift && batch == o.batch;
+    return bx == o.bx && by == o.by && ch == o.ch && lshift == o.lshift && batch == o.batch && epi == o.epi;
   }
 };
 
@@ -227,6 +228,7 @@ std::string instance_macros(const tcs_spec& s, const PipeKey* pk) {
     m << "#define TCS_PIPE 1\n#define TCS_BX " << pk->bx << "\n#define TCS_BY " << pk->by
       << "\n#define TCS_CH " << pk->ch << "\n#define TCS_LSHIFT " << pk->lshift << "\n";
   if (pk && pk->batch) m << "#define TCS_BATCH 1\n";
+  if (pk && pk->epi) m << "#define TCS_EPI " << pk->epi << "\n";
   m << "#define TCS_T " << (s.precision == TCS_F64 ? "double" : "float") << "\n"
     << "#define TCS_COMP " << (s.precision == TCS_F32C ? 1 : 0) << "\n"
     << "#define TCS_DIM " << s.dimension << "\n"
@@ -678,7 +680,7 @@ bool pipe_comp_ok(const tcs_spec& s) {
 }
 
 int resolve_pipe(tcs_stencil* h, const TcsGeo& g, const tcs_launch* L, Resolved& out,
-                 bool batch = false) {
+                 bool batch = false, unsigned epi = 0) {
   const tcs_spec& s = h->spec;
   if (s.precision == TCS_F32C && !pipe_comp_ok(s))
     return fail(TCS_ERR_UNSUPPORTED,
@@ -706,7 +708,7 @@ int resolve_pipe(tcs_stencil* h, const TcsGeo& g, const tcs_launch* L, Resolved&
     return fail(TCS_ERR_UNSUPPORTED, "pipe: tile exceeds the 256-element TMA box limit");
   const bool no_tma = W > 256;
   const unsigned chunk_bytes = ch * rows * W * es;
-  PipeKey key{L->block[0], s.dimension == 3 ? L->block[1] : 1u, ch, lshift, batch ? 1u : 0u};
+  PipeKey key{L->block[0], s.dimension == 3 ? L->block[1] : 1u, ch, lshift, batch ? 1u : 0u, epi};
   PipeMod* pm = nullptr;
   int rc = pipe_module(h, key, &pm);
   if (rc) return rc;
@@ -905,6 +907,16 @@ int fringe_module(tcs_stencil* h) {
   return upload_mask(h, h->fringe_mask);
 }
 
+// Does a sweep of this geometry leave partial coarsening tiles to the coarsening-1 fringe kernel?
+bool has_fringe(const tcs_stencil* h, const TcsGeo& g) {
+  const tcs_spec& s = h->spec;
+  const bool d3 = s.dimension == 3;
+  const unsigned R = (unsigned)s.range;
+  const unsigned cz = d3 ? (unsigned)s.cz : 1u;
+  const unsigned ex = g.x_lim > g.x0 ? g.x_lim - g.x0 : 0, ey = g.y_lim - R, ez = d3 ? g.z_lim - R : 0;
+  return ex % (unsigned)s.cx != 0 || ey % (unsigned)s.cy != 0 || (d3 && ez % cz != 0);
+}
+
 int launch_fringe(tcs_stencil* h, const TcsGeo& g, const void* in, void* out, const void* src, CUstream st) {
   const tcs_spec& s = h->spec;
   const bool d3 = s.dimension == 3;
@@ -969,8 +981,8 @@ int launch_resolved(tcs_stencil* h, const Resolved& r, const void* in, void* out
       if (rc) return rc;
       pmap = *map;
     }
-    CUdeviceptr pin = (CUdeviceptr)in, pout = (CUdeviceptr)out;
-    void* args[] = {&pmap, &pin, &pout, &psrc, &pg};
+    CUdeviceptr pin = (CUdeviceptr)in, pout = (CUdeviceptr)out, paux = 0, ppart = 0;
+    void* args[] = {&pmap, &pin, &pout, &psrc, &pg, &paux, &ppart};
     TCS_CU(g_drv.LaunchKernel(r.pipe->f, r.grid[0], 1, 1, r.block[0], r.block[1], 1, r.smem, st,
                               args, nullptr));
     return launch_fringe(h, r.geo, in, out, src, st);
@@ -1488,7 +1500,7 @@ int tcs_precompile(const tcs_spec* spec, char* cubin_path, unsigned path_cap) {
 namespace {
 
 int precompile_pipe(const tcs_spec* spec, unsigned bx, unsigned by, unsigned chunk, bool batch,
-                    char* cubin_path, unsigned path_cap) {
+                    char* cubin_path, unsigned path_cap, unsigned epi = 0) {
   int rc = validate(spec);
   if (rc) return rc;
   tcs_spec s = *spec;
@@ -1501,7 +1513,9 @@ int precompile_pipe(const tcs_spec* spec, unsigned bx, unsigned by, unsigned chu
   if (bx == 0 || (bx * (unsigned)s.cx) % vec != 0)
     return fail(TCS_ERR_UNSUPPORTED, "pipe: unsupported block");
   if (chunk == 0) chunk = pipe_auto_chunk(s, bx, by);
-  PipeKey key{bx, s.dimension == 3 ? by : 1u, chunk, left_offset_of(s) % vec, batch ? 1u : 0u};
+  if (epi > 2 || (epi == 1 && s.precision != TCS_F64) || (epi == 2 && s.precision != TCS_F32) || (epi && batch))
+    return fail(TCS_ERR_UNSUPPORTED, "pipe: epilogue not available for this precision");
+  PipeKey key{bx, s.dimension == 3 ? by : 1u, chunk, left_offset_of(s) % vec, batch ? 1u : 0u, epi};
   std::vector<char> cubin;
   std::string path;
   rc = instantiate(s, &key, cubin, &path);
@@ -1544,20 +1558,6 @@ int ensure_scratch(tcs_stencil* h, size_t need) {
   return TCS_OK;
 }
 
-}  // namespace
-
-extern "C" {
-
-int tcs_precompile_pipe(const tcs_spec* spec, unsigned bx, unsigned by, unsigned chunk,
-                        char* cubin_path, unsigned path_cap) {
-  return precompile_pipe(spec, bx, by, chunk, false, cubin_path, path_cap);
-}
-
-int tcs_precompile_batch(const tcs_spec* spec, unsigned bx, unsigned by, unsigned chunk,
-                         char* cubin_path, unsigned path_cap) {
-  return precompile_pipe(spec, bx, by, chunk, true, cubin_path, path_cap);
-}
-
 // The residual entry points launch on the calling thread's current device: it must be the device
 // the handle (and the buffers) belong to.
 int check_current_device(const tcs_stencil* h) {
@@ -1567,6 +1567,25 @@ int check_current_device(const tcs_stencil* h) {
     return fail(TCS_ERR_INVALID_VALUE, "current device " + std::to_string(dev) + " is not the handle's device " +
                                            std::to_string(h->device));
   return TCS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int tcs_precompile_pipe(const tcs_spec* spec, unsigned bx, unsigned by, unsigned chunk,
+                        char* cubin_path, unsigned path_cap) {
+  return precompile_pipe(spec, bx, by, chunk, false, cubin_path, path_cap);
+}
+
+int tcs_precompile_pipe_epilogue(const tcs_spec* spec, unsigned bx, unsigned by, unsigned chunk, unsigned epi,
+                                 char* cubin_path, unsigned path_cap) {
+  return precompile_pipe(spec, bx, by, chunk, false, cubin_path, path_cap, epi);
+}
+
+int tcs_precompile_batch(const tcs_spec* spec, unsigned bx, unsigned by, unsigned chunk,
+                         char* cubin_path, unsigned path_cap) {
+  return precompile_pipe(spec, bx, by, chunk, true, cubin_path, path_cap);
 }
 
 int tcs_residual(tcs_stencil* h, const unsigned grid[3], unsigned right_offset, const double* x,
@@ -1639,6 +1658,90 @@ int tcs_scratch_bytes(tcs_stencil* h, unsigned long long* bytes) {
   if (!h || !bytes) return fail(TCS_ERR_INVALID_VALUE, "NULL argument");
   *bytes = (unsigned long long)h->scratch_len * sizeof(double);
   return TCS_OK;
+}
+
+// ---- fused defect-correction sweeps (pipe kernel epilogues 1 and 2) ---------------------------
+}  // extern "C"
+
+namespace {
+
+// Resolve a launch of the pipelined kernel with epilogue `epi`; the fused sweeps run on the pipe
+// kernel only and on geometries without a coarsening fringe.
+int resolve_epi(tcs_stencil* h, const unsigned grid[3], unsigned right_offset, const tcs_launch* launch,
+                unsigned epi, Resolved& r) {
+  if (!h || !launch) return fail(TCS_ERR_INVALID_VALUE, "NULL handle or launch");
+  int rc = check_current_device(h);
+  if (rc) return rc;
+  TcsGeo g;
+  rc = make_geo(h, grid, right_offset, g);
+  if (rc) return rc;
+  rc = check_block(h, launch->block);
+  if (rc) return rc;
+  if (launch->variant != TCS_VARIANT_AUTO && launch->variant != TCS_VARIANT_PIPE)
+    return fail(TCS_ERR_UNSUPPORTED, "fused defect-correction sweeps run on the pipelined kernel");
+  if (has_fringe(h, g))
+    return fail(TCS_ERR_UNSUPPORTED, "fused defect-correction sweeps need a grid of whole coarsening tiles");
+  return resolve_pipe(h, g, launch, r, false, epi);
+}
+
+int launch_epi(tcs_stencil* h, const Resolved& r, const void* in, const void* src, void* aux, double* partials,
+               CUstream st) {
+  TcsPipeGeo pg = r.pgeo;
+  pg.loader = r.no_tma ? pipe_loader_cp(h->spec, pg.xdim, in) : pipe_loader(h->spec, pg.xdim, in);
+  alignas(64) CUtensorMap pmap;
+  std::memset(&pmap, 0, sizeof(pmap));
+  if (pg.loader == 0) {
+    CUtensorMap* map = nullptr;
+    int rc = tensor_map(h, in, r, &map);
+    if (rc) return rc;
+    pmap = *map;
+  }
+  // `out` only anchors the kernel's output offsets: epilogues 1 and 2 store through `aux`
+  CUdeviceptr pin = (CUdeviceptr)in, pout = (CUdeviceptr)in, psrc = (CUdeviceptr)src, paux = (CUdeviceptr)aux,
+              ppart = (CUdeviceptr)partials;
+  void* args[] = {&pmap, &pin, &pout, &psrc, &pg, &paux, &ppart};
+  TCS_CU(g_drv.LaunchKernel(r.pipe->f, r.grid[0], 1, 1, r.block[0], r.block[1], 1, r.smem, st, args, nullptr));
+  return TCS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int tcs_defect_sweep(tcs_stencil* h, const unsigned grid[3], unsigned right_offset, const tcs_launch* launch,
+                     const void* x, float* r, double norms[2], void* stream) {
+  if (!h || !x || !r) return fail(TCS_ERR_INVALID_VALUE, "NULL argument");
+  if (h->spec.precision != TCS_F64) return fail(TCS_ERR_INVALID_VALUE, "the defect sweep needs an FP64 handle");
+  Resolved rs;
+  int rc = resolve_epi(h, grid, right_offset, launch, 1, rs);
+  if (rc) return rc;
+  const unsigned nb = rs.grid[0];
+  rc = ensure_scratch(h, 2ull * nb + 8);
+  if (rc) return rc;
+  double* res = h->scratch + 2ull * nb;
+  rc = launch_epi(h, rs, x, x, r, h->scratch, (CUstream)stream);
+  if (rc) return rc;
+  const int e = tcs_field_launch_finish(h->scratch, (int)nb, 2, 1u, res, (cudaStream_t)stream);
+  if (e != 0) return fail(TCS_ERR_CUDA, std::string("finish kernel: ") + cudaGetErrorString((cudaError_t)e));
+  if (norms) {
+    double host[2];
+    TCS_RT(cudaMemcpyAsync(host, res, sizeof(host), cudaMemcpyDeviceToHost, (cudaStream_t)stream));
+    TCS_RT(cudaStreamSynchronize((cudaStream_t)stream));
+    norms[0] = host[0];
+    norms[1] = std::sqrt(host[1]);
+  }
+  return TCS_OK;
+}
+
+int tcs_update_grid_accumulate(tcs_stencil* h, const unsigned grid[3], unsigned right_offset,
+                               const tcs_launch* launch, const void* in, const void* src, double* x,
+                               void* stream) {
+  if (!h || !in || !x) return fail(TCS_ERR_INVALID_VALUE, "NULL argument");
+  if (h->spec.precision != TCS_F32) return fail(TCS_ERR_INVALID_VALUE, "the accumulating sweep needs an FP32 handle");
+  Resolved rs;
+  int rc = resolve_epi(h, grid, right_offset, launch, 2, rs);
+  if (rc) return rc;
+  return launch_epi(h, rs, in, src, x, nullptr, (CUstream)stream);
 }
 
 int tcs_accumulate(tcs_stencil* h, const unsigned grid[3], unsigned right_offset, double* x,

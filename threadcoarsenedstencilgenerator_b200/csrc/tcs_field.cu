@@ -130,6 +130,12 @@ extern "C" int tcs_field_launch_defect(const double* x, const double* sx, float*
   return (int)cudaGetLastError();
 }
 
+extern "C" int tcs_field_launch_finish(const double* partial, int nblocks, int w, unsigned max_mask,
+                                       double* result, cudaStream_t st) {
+  tcs_k_finish<<<1, kThreads, 0, st>>>(partial, nblocks, w, max_mask, result);
+  return (int)cudaGetLastError();
+}
+
 extern "C" int tcs_field_launch_compare(const void* a, int a_f32, const double* b, TcsFieldGeo g,
                                         double* scratch, int nblocks, double* result4,
                                         cudaStream_t st) {

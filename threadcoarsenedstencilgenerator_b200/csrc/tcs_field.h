@@ -34,6 +34,10 @@ int tcs_field_launch_defect(const double* x, const double* sx, float* r, TcsFiel
 int tcs_field_launch_compare(const void* a, int a_f32, const double* b, TcsFieldGeo g,
                              double* scratch, int nblocks, double* result4, cudaStream_t st);
 int tcs_field_launch_add(double* x, const float* e, TcsFieldGeo g, int nblocks, cudaStream_t st);
+// Reduce nblocks per-block partials of width w into result (one block; slot k is a maximum when bit
+// k of max_mask is set, a sum otherwise).
+int tcs_field_launch_finish(const double* partial, int nblocks, int w, unsigned max_mask, double* result,
+                            cudaStream_t st);
 // Failure-detection self-test: a bounded wait on a barrier nothing arrives at (at most `limit`
 // clock cycles), which then sets bit 0 (value 1) of `status`.  Returns a cudaError_t value.
 int tcs_field_launch_wait_probe(unsigned* status, long long limit, cudaStream_t st);

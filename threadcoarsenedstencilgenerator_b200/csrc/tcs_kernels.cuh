@@ -491,7 +491,21 @@ extern "C" __global__ void tcs_init(T* __restrict__ a, const tcs_u64 xdim, const
 // still accumulates in exactly the reference order) and completes output p-R.  Each input element
 // is read from HBM once and from shared memory once per thread that needs it; with the plane loop
 // unrolled by 2R+1 every register slot and every shared-memory offset is a compile-time constant.
+#ifndef TCS_EPI
+#define TCS_EPI 0
+#endif
 namespace tcs {
+// Epilogue of the pipelined sweep (what happens to an output value v once it is complete):
+//   0  out = v (+ src)                                      every ordinary sweep
+//   1  (FP64) r = fl32(v - x) with x = src, into the float array `aux`, and the running norms
+//      max |v - x|, sum (v - x)^2 per thread, reduced per CTA into `partials`: the defect of a
+//      defect-correction period without writing S(x) (r bit-identical to a sweep followed by
+//      tcs_residual)
+//   2  (FP32) x64 += (double)(v (+ src)) with x64 the double array `aux`: the last correction
+//      sweep of a period fused with the accumulation into the FP64 state
+constexpr int EPI = TCS_EPI;
+static_assert(EPI == 0 || (EPI == 1 && sizeof(T) == 8) || (EPI == 2 && sizeof(T) == 4),
+              "epilogue 1 needs FP64 sweeps, epilogue 2 FP32 sweeps");
 constexpr int BX = TCS_BX;
 constexpr int BY = (DIM == 3) ? TCS_BY : 1;
 constexpr int CHP = TCS_CH;          // planes per chunk
@@ -584,6 +598,7 @@ struct PipeGridView {
   bool use_tma;
   bool cp_pair;  // cp.async loader moves two elements per copy (FP32, even pitch, 8-byte base)
   bool st_pair;  // output pairs stored with one access (even pitch, pair-aligned base)
+  void* aux;     // epilogues 1 and 2: the float defect array / the double state (same layout)
 };
 
 // cp.async fill of one ring chunk: CHP planes of ROWS rows (3D) or CHP rows (2D), PW elements
@@ -620,6 +635,7 @@ __device__ __forceinline__ void pipe_copy_chunk(const PipeGridView& G, tcs_u32 d
 struct PipeState {
   tcs_u32 bars, ring_s, nslot, tid, gc;
   T* ring;
+  double nmax, nsum;  // epilogue 1: this thread's running defect norms
 };
 
 // Sweep one piece: tile `tile` of grid `G`, output planes [R + zs, R + ze) along the march axis.
@@ -733,6 +749,21 @@ __device__ __forceinline__ bool pipe_piece(const PipeGridView& G, tcs_u32 tile, 
       constexpr int t = decltype(tt)::value;
       const tcs_u32 pi = pbase + t;
       if (pi < np) {
+        // A source term is read from global memory when its output row is stored: fetch the rows
+        // of the output completed PF planes later into L1 now, so that the store does not wait
+        // for the latency of DRAM or L2.
+        constexpr int PF = 2;
+        if (G.src && lane_ok) {
+          const int opf = (int)pi - 2 * R + PF;
+          if (opf >= 0 && opf < (int)nout) {
+            const T* sp = G.src + ((optr - G.out) + (tcs_i64)(t + PF) * plane_g);
+            static_for<0, (DIM == 3) ? CY : 1>([&](auto ey) {
+              const T* q = sp + decltype(ey)::value * (tcs_i64)G.xdim;
+              asm volatile("prefetch.global.L1 [%0];" ::"l"(q));
+              if constexpr (CX * sizeof(T) > 16) asm volatile("prefetch.global.L1 [%0];" ::"l"(q + CX - 1));
+            });
+          }
+        }
         const PipeRing ld{pc + t * PLANE};
         auto slot = [&](auto kk) -> PipeSlot& {
           constexpr int k = decltype(kk)::value;
@@ -740,7 +771,29 @@ __device__ __forceinline__ bool pipe_piece(const PipeGridView& G, tcs_u32 tile, 
         };
         pipe_plane(ld, slot);
         const int op = (int)pi - 2 * R;
-        if (lane_ok && op >= 0 && op < (int)nout) {
+        if (EPI != 0 && lane_ok && op >= 0 && op < (int)nout) {
+          constexpr T c = T(1) / T(S);
+          PipeSlot& done = acc[((t - 2 * R) % NP2 + NP2) % NP2];
+          const tcs_i64 rowoff = (optr - G.out) + (tcs_i64)t * plane_g;
+          static_for<0, (DIM == 3) ? CY : 1>([&](auto ey) {
+            static_for<0, CX>([&](auto ex) {
+              constexpr int e = decltype(ex)::value + decltype(ey)::value * CX;
+              const tcs_i64 off = rowoff + decltype(ex)::value + decltype(ey)::value * (tcs_i64)G.xdim;
+              T v = (COEFF == 0) ? slot_value<e>(done) * c : slot_value<e>(done);
+              if constexpr (EPI == 1) {
+                const double d = (double)v - (double)G.src[off];
+                static_cast<float*>(G.aux)[off] = (float)d;
+                st.nmax = fmax(st.nmax, fabs(d));
+                st.nsum = fma(d, d, st.nsum);
+              } else {
+                if (G.src) v = v + G.src[off];
+                double* xg = static_cast<double*>(G.aux);
+                xg[off] = xg[off] + (double)v;
+              }
+            });
+          });
+        }
+        if (EPI == 0 && lane_ok && op >= 0 && op < (int)nout) {
           constexpr T c = T(1) / T(S);
           PipeSlot& done = acc[((t - 2 * R) % NP2 + NP2) % NP2];
           T* orow = optr + (tcs_i64)t * plane_g;
@@ -808,6 +861,8 @@ __device__ __forceinline__ PipeState pipe_setup(tcs_u32 nslot, bool single_arriv
   st.ring_s = (st.bars + bar_bytes + 127u) & ~127u;
   st.ring = reinterpret_cast<T*>(tcs_smem + (st.ring_s - st.bars));
   st.gc = 0;
+  st.nmax = 0.0;
+  st.nsum = 0.0;
   if (st.tid == 0) {
     for (tcs_u32 i = 0; i < nslot; ++i) mbar_init(st.bars + 8u * i, single_arrival ? 1u : BX * BY);
     fence_barrier_init();
@@ -821,9 +876,11 @@ __device__ __forceinline__ PipeState pipe_setup(tcs_u32 nslot, bool single_arriv
 #ifndef TCS_BATCH
 extern "C" __global__ void __launch_bounds__(TCS_BX * ((TCS_DIM == 3) ? TCS_BY : 1))
     tcs_pipe(const __grid_constant__ TcsTmaMap tmap, const T* __restrict__ in,
-             T* __restrict__ out, const T* __restrict__ src, const TcsPipeGeo g) {
+             T* __restrict__ out, const T* __restrict__ src, const TcsPipeGeo g, void* aux,
+             double* __restrict__ partials) {
   using namespace tcs;
   PipeGridView G;
+  G.aux = aux;
   G.map = &tmap;
   G.in = in;
   G.out = out;
@@ -853,6 +910,35 @@ extern "C" __global__ void __launch_bounds__(TCS_BX * ((TCS_DIM == 3) ? TCS_BY :
     w += ze - zs;
     if (!pipe_piece<false>(G, tile, zs, ze, st, acc)) return;
   }
+  if constexpr (EPI == 1) {
+    // this CTA's defect norms: shuffles within each warp, then one value per warp in shared memory
+    __shared__ double red[2][32];
+    double mx = st.nmax, ss = st.nsum;
+    constexpr tcs_u32 NT = BX * BY;
+    const tcs_u32 lane = st.tid & 31u, width = min(32u, NT - (st.tid & ~31u));  // lanes of this warp
+    const unsigned lanes = width == 32u ? 0xffffffffu : ((1u << width) - 1u);
+    for (tcs_u32 o = 16; o > 0; o >>= 1) {
+      const double m2 = __shfl_down_sync(lanes, mx, o), s2 = __shfl_down_sync(lanes, ss, o);
+      if (lane + o < width) {
+        mx = fmax(mx, m2);
+        ss += s2;
+      }
+    }
+    const tcs_u32 warp = st.tid >> 5, nwarps = (NT + 31) / 32;
+    if (lane == 0) {
+      red[0][warp] = mx;
+      red[1][warp] = ss;
+    }
+    __syncthreads();
+    if (st.tid == 0) {
+      for (tcs_u32 k = 1; k < nwarps; ++k) {
+        mx = fmax(mx, red[0][k]);
+        ss += red[1][k];
+      }
+      partials[2 * blockIdx.x] = mx;
+      partials[2 * blockIdx.x + 1] = ss;
+    }
+  }
 }
 #endif  // !TCS_BATCH
 
@@ -866,6 +952,7 @@ extern "C" __global__ void __launch_bounds__(TCS_BX * ((TCS_DIM == 3) ? TCS_BY :
     tcs_pipe_batch(const TcsBatchGrid* __restrict__ grids, const tcs_u32 ngrids,
                    const tcs_u64 total, const tcs_u64 per_cta, const tcs_u32 nslot) {
   using namespace tcs;
+  static_assert(EPI == 0, "batched sweeps store plain outputs");
   PipeState st = pipe_setup(nslot, false);
   PipeSlot acc[NP2];
   const tcs_u64 w_begin = (tcs_u64)blockIdx.x * per_cta;
@@ -898,6 +985,7 @@ extern "C" __global__ void __launch_bounds__(TCS_BX * ((TCS_DIM == 3) ? TCS_BY :
     G.use_tma = (B.loader == 0);
     G.cp_pair = (B.loader == 2);
     G.st_pair = (B.xdim % 2 == 0) && (reinterpret_cast<tcs_u64>(B.out) % (2 * sizeof(T)) == 0);
+    G.aux = nullptr;
     const tcs_u64 local = w - B.first;
     const tcs_u32 tile = (tcs_u32)(local / B.m);
     const tcs_u32 zs = (tcs_u32)(local % B.m);

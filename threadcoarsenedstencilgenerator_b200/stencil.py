@@ -185,6 +185,25 @@ class Stencil:
                                                     ctypes.byref(launch.to_c()), _ptr(src), _ptr(source),
                                                     _ptr(dst), _stream(stream)))
 
+    def defect_sweep(self, geom: Geometry, x, r, launch: Launch | None = None, stream=None, norms: bool = True):
+        """One FP64 sweep of x whose epilogue writes r = fl32(S(x) - x) (S(x) is not stored);
+        returns (max |S(x) - x|, ||S(x) - x||_2) when norms.  Pipelined kernel only."""
+        launch = launch or Launch()
+        out = (ctypes.c_double * 2)()
+        _lib.check(self._lib.tcs_defect_sweep(self._h, _lib.U3(*geom.grid), geom.right_offset,
+                                              ctypes.byref(launch.to_c()), _ptr(x), _ptr(r), out if norms else None,
+                                              _stream(stream)))
+        return (out[0], out[1]) if norms else None
+
+    def update_grid_accumulate(self, geom: Geometry, src, source, x, launch: Launch | None = None,
+                               stream=None) -> None:
+        """One FP32 sweep added to the FP64 state: x += S(src) + source (source may be None)."""
+        launch = launch or Launch()
+        _lib.check(self._lib.tcs_update_grid_accumulate(self._h, _lib.U3(*geom.grid), geom.right_offset,
+                                                        ctypes.byref(launch.to_c()), _ptr(src),
+                                                        None if source is None else _ptr(source), _ptr(x),
+                                                        _stream(stream)))
+
     def sweeps_tb2(self, geom: Geometry, a, b, n: int, stream=None):
         """n ping-pong sweeps starting from a with temporal blocking (2D: two sweeps per pass over
         HBM, bit-identical to n ordinary sweeps); returns the buffer holding the result."""
@@ -277,6 +296,15 @@ def precompile_pipe(spec: StencilSpec, block, chunk: int) -> str:
     buf = ctypes.create_string_buffer(1024)
     b = tuple(block) + (1,) * (3 - len(block))
     _lib.check(_lib.load().tcs_precompile_pipe(ctypes.byref(spec.to_c()), b[0], b[1], int(chunk), buf, 1024))
+    return buf.value.decode()
+
+
+def precompile_pipe_epilogue(spec: StencilSpec, block, chunk: int, epi: int) -> str:
+    """Instantiate the pipelined sweep with epilogue 1 (FP64 defect) or 2 (FP32 accumulate)."""
+    buf = ctypes.create_string_buffer(1024)
+    b = tuple(block) + (1,) * (3 - len(block))
+    _lib.check(_lib.load().tcs_precompile_pipe_epilogue(ctypes.byref(spec.to_c()), b[0], b[1], int(chunk), int(epi),
+                                                        buf, 1024))
     return buf.value.decode()
 
 
