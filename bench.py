@@ -33,6 +33,8 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 FALLBACK_HBM_GBS = 6650.0
+# Nominal FP64 FMA peak: 148 SMs x 64 FMA/clk x 2 flops x 1.965 GHz.
+FP64_PEAK_FLOPS = 148 * 64 * 2 * 1.965e9
 
 
 def _peaks():
@@ -376,13 +378,123 @@ def run_ours(args) -> dict | None:
     }
     if temporal:
         line["temporal_blocking"] = temporal
+    if world == 1 and not args.no_extras:
+        del x, y, dev, outs, host, jobs_in, jobs_out
+        line["configs"] = run_extras(args)
     return line
 
 
+def run_config1(steps: int = 20, warmup: int = 3) -> dict:
+    """2D Box Jacobi r1 (9-point mean) FP64 on 4096^2: the tuned single-sweep kernel and the
+    two-sweeps-per-pass kernel (temporal blocking), each timed with CUDA events and checked against
+    the oracle after the sweeps it ran."""
+    import numpy as np
+    import torch
+
+    import oracle as O
+    import threadcoarsenedstencilgenerator_b200 as tcs
+    from threadcoarsenedstencilgenerator_b200.workloads import WORKLOADS
+
+    w = WORKLOADS["2d_box_jacobi_r1_4096"]
+    spec = w.tuned_spec()
+    launch = w.tuned_launch()
+    geom = spec.geometry(*w.grid)
+    st = tcs.Stencil(spec)
+    a = w.make_input(geom)
+    stream = torch.cuda.current_stream()
+    peak, peak_kind = _peaks()
+    ospec = O.make_spec(spec.dimension, spec.neighbourhood, spec.orientation, spec.coefficients, spec.range,
+                        spec.cx, spec.cy, spec.cz, spec.alignment, spec.cl_size)
+    out = {"workload": w.name, "coarsening": list(spec.coarsening), "block": list(launch.block),
+           "variant": st.plan(geom, launch).variant}
+    nt = steps + (steps % 2)
+    for name, run in (("single_sweep", lambda u, v, k: st.sweeps(geom, u, v, k, launch, stream)),
+                      ("temporal_blocking", lambda u, v, k: st.sweeps_tb2(geom, u, v, k, stream))):
+        x = torch.from_numpy(a).cuda()
+        y = x.clone()
+        run(x, y, 2 * warmup)
+        torch.cuda.synchronize()
+        x.copy_(torch.from_numpy(a))
+        y.copy_(x)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        res = run(x, y, nt)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        if st.device_status() != 0:
+            raise RuntimeError("device status word set during %s" % name)
+        ms = e0.elapsed_time(e1)
+        glups = geom.interior_points * nt / (ms / 1e3) / 1e9
+        want = O.sweeps(ospec, a, nt, geom.right_offset, None, cpu_threads=0)
+        bytes_per_lup = 16 if name == "single_sweep" else 8  # two sweeps per pass: 16 B per two updates
+        achieved = glups * bytes_per_lup
+        out[name] = {"glups": glups, "sweeps": nt, "ms_per_sweep": ms / nt,
+                     "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                                  "frac": achieved / peak, "peak_source": peak_kind,
+                                  "algorithmic_bytes_per_lup": bytes_per_lup},
+                     "parity": bool(np.array_equal(res.cpu().numpy(), want))}
+        del x, y
+    out["temporal_vs_single"] = out["temporal_blocking"]["glups"] / out["single_sweep"]["glups"]
+    out["roofline_note"] = ("single sweep: 16 B per lattice update (read + write); temporal blocking: 16 B per "
+                            "two updates, so its HBM fraction counts 8 B per update")
+    st.close()
+    torch.cuda.empty_cache()
+    return out
+
+
+def run_extras(args) -> dict:
+    """The other configurations of the workload list, each a compact record (single GPU): 2D Box
+    Jacobi r1 (single sweep and temporal blocking), the 2D Box Variable r6 precision table, the
+    batched uneven grids, and the learned autotuner live on held-out parameter sets."""
+    import argparse as _ap
+
+    import torch
+
+    out = {}
+    torch.cuda.empty_cache()
+    out["config1_2d_box_jacobi_r1_4096"] = run_config1()
+    torch.cuda.empty_cache()
+    prec = run_precision(_ap.Namespace(workload="2d_box_var_r6_16384x8192", sweeps=200, period=20))
+    out["config3_2d_box_var_r6_16384x8192"] = {"config": prec["config"], "precision": prec["precision"]}
+    torch.cuda.empty_cache()
+    b = run_batch(_ap.Namespace(workload="batch_3d_star_jacobi_r2_64", steps=5, warmup=3, e2e_steps=1,
+                                no_cpu_baseline=True, gpus=1))
+    out["config4_batch_3d_star_jacobi_r2_64"] = {"value": b["value"], "unit": b["unit"], "config": b["config"],
+                                                 "roofline": b["roofline"], "batch": b["batch"]}
+    torch.cuda.empty_cache()
+    out["config5_autotune_live"] = run_autotune_live(3)
+    return out
+
+
+def run_autotune_live(n_sets: int) -> dict:
+    """The learned tuner against the exhaustive sweep on the first n held-out parameter sets of the
+    committed corpus (model top-5 timed, fallback rules as in production)."""
+    from threadcoarsenedstencilgenerator_b200 import autotune as A
+
+    cfg, X, y = A.load_corpus()
+    hold, _ = A.split(cfg)
+    m = A.CostModel.load()
+    rows = []
+    r = A.live(m, hold[:n_sets], log=lambda line: rows.append(line))
+    m.close()
+    return {**r, "sets": [json.loads(q) for q in rows]}
+
+
 def run_precision(args) -> dict | None:
-    """FP64 vs FP32 vs FP32 with FP64 defect correction on one workload (single GPU): each runs the
-    workload's full sweep count from the same input; errors are measured on the GPU against the
-    FP64 result (the engine's FP64 sweep is bit-identical to the reference kernel)."""
+    """FP64 against the reduced-precision forms on one workload (single GPU), each from the same
+    input for the workload's sweep count: plain FP32, compensated FP32, FP32 with FP64 defect
+    correction every `period` sweeps, and (2D Box) the tensor-core sweep alone and with the same
+    defect correction.  Errors are measured on the GPU against the engine's FP64 result (which is
+    bit-identical to the reference kernel), three ways:
+
+      per_sweep  one sweep of each raw form from the same input against one FP64 sweep -- the
+                 accuracy of a single reduced-precision sweep;
+      periods    the defect-corrected iterates against the FP64 iterate at every period boundary
+                 (sweeps 20, 40, ...), including the boundaries before the iteration settles;
+      final      after all sweeps.
+
+    Relative errors: max_rel = max|a - b| / max|b|, rms_rel = ||a - b||_2 / ||b||_2 over the
+    interior."""
     import numpy as np
     import torch
 
@@ -397,128 +509,156 @@ def run_precision(args) -> dict | None:
     geom = spec.geometry(*w.grid)
     mask = w.make_mask()
     n = args.sweeps or w.sweeps
+    period = args.period
     a = w.make_input(geom)
+    a32 = a.astype(np.float32)
     points = geom.interior_points
     stream = torch.cuda.current_stream()
     ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
+
+    def timed(fn):
+        e0, e1 = ev(), ev()
+        e0.record(stream)
+        out = fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return out, e0.elapsed_time(e1)
+
+    def err(d):
+        return {"max_rel": d["max_rel"], "rms_rel": d["rms_rel"]}
 
     # FP32 has a tuned shape of its own; it sweeps the FP64 geometry (partial coarsening tiles go
     # to the coarsening-1 fringe kernel, so the values do not depend on the shape)
     spec32 = w.tuned_spec("f32")
     launch32 = w.tuned_launch("f32")
     dc = DefectCorrectedSweeps(spec, launch, launch32=launch32, mask=mask, coarsening32=spec32.coarsening)
-    # FP64
-    x = torch.from_numpy(a).cuda()
-    y = x.clone()
-    dc.s64.sweeps(geom, x, y, 3, launch)
-    x.copy_(torch.from_numpy(a))
-    y.copy_(x)
-    e0, e1 = ev(), ev()
-    e0.record(stream)
-    ref = dc.s64.sweeps(geom, x, y, n, launch, stream)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    t64 = e0.elapsed_time(e1)
-    # plain FP32
-    x32 = torch.from_numpy(a.astype(np.float32)).cuda()
-    y32 = x32.clone()
-    dc.s32.sweeps(geom, x32, y32, 3, launch32)
-    x32.copy_(torch.from_numpy(a.astype(np.float32)))
-    y32.copy_(x32)
-    e0, e1 = ev(), ev()
-    e0.record(stream)
-    r32 = dc.s32.sweeps(geom, x32, y32, n, launch32, stream)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    t32 = e0.elapsed_time(e1)
-    s32 = dc.s64.compare(geom, r32, ref, "f32")
-    del x32, y32
-    # FP32 with compensated (two-sum) accumulation: direct or march kernel (block of the tuned launch)
-    s32c = tcs.Stencil(spec.replace(precision="f32c"))
+    s64, s32 = dc.s64, dc.s32
+    s32c = tcs.Stencil(spec32.replace(precision="f32c"))
     if mask is not None:
         s32c.copy_mask(mask)
-    lc = tcs.Launch(block=(128, 1, 1) if spec.dimension == 2 else (32, 4, 1), variant="auto")
-    x32 = torch.from_numpy(a.astype(np.float32)).cuda()
+    tc_ok = spec.dimension == 2 and spec.neighbourhood == "Box" and spec.range <= 8
+    dtc = DefectCorrectedSweeps(spec, launch, mask=mask, tensor_cores=True) if tc_ok else None
+
+    x = torch.from_numpy(a).cuda()
+    y = x.clone()
+    x32 = torch.from_numpy(a32).cuda()
     y32 = x32.clone()
-    s32c.sweeps(geom, x32, y32, 3, lc)
-    x32.copy_(torch.from_numpy(a.astype(np.float32)))
-    y32.copy_(x32)
-    e0, e1 = ev(), ev()
-    e0.record(stream)
-    r32c = s32c.sweeps(geom, x32, y32, n, lc, stream)
-    e1.record(stream)
+
+    # ---- per-sweep accuracy: one sweep of every form from the same input ----------------------
+    s64.update_grid(geom, x, y, launch)
+    per_sweep = {}
+    s32.update_grid(geom, x32, y32, launch32)
+    per_sweep["f32"] = err(s64.compare(geom, y32, y, "f32"))
+    s32c.update_grid(geom, x32, y32, launch32)
+    per_sweep["f32_compensated"] = err(s64.compare(geom, y32, y, "f32"))
+    if dtc:
+        dtc.s32.tc_update_grid(geom, x32, y32)
+        per_sweep["tensor_cores"] = err(s64.compare(geom, y32, y, "f32"))
     torch.cuda.synchronize()
-    t32c = e0.elapsed_time(e1)
-    s32c_err = dc.s64.compare(geom, r32c, ref, "f32")
-    p32c = s32c.plan(geom, lc)
-    del x32, y32
-    # FP32 + FP64 defect correction
-    xm = torch.from_numpy(a).cuda()
-    work = {"sx": xm.clone(), "r": torch.zeros(geom.shape, dtype=torch.float32, device="cuda"),
+
+    def reset():
+        x.copy_(torch.from_numpy(a))
+        y.copy_(x)
+        x32.copy_(torch.from_numpy(a32))
+        y32.copy_(x32)
+
+    # ---- throughput and final error over n sweeps ---------------------------------------------
+    reset()
+    s64.sweeps(geom, x, y, 3, launch)  # warm-up
+    reset()
+    ref, t64 = timed(lambda: s64.sweeps(geom, x, y, n, launch, stream))
+    ref_final = ref.clone()
+    forms = {}
+    s32.sweeps(geom, x32, y32, 3, launch32)
+    reset()
+    r, t = timed(lambda: s32.sweeps(geom, x32, y32, n, launch32, stream))
+    forms["f32"] = {"ms": t, **err(s64.compare(geom, r, ref_final, "f32")), "variant": s32.plan(geom, launch32).variant}
+    s32c.sweeps(geom, x32, y32, 3, launch32)
+    reset()
+    r, t = timed(lambda: s32c.sweeps(geom, x32, y32, n, launch32, stream))
+    forms["f32_compensated"] = {"ms": t, **err(s64.compare(geom, r, ref_final, "f32")),
+                                "variant": s32c.plan(geom, launch32).variant}
+    work = {"sx": torch.empty_like(x), "r": torch.zeros(geom.shape, dtype=torch.float32, device="cuda"),
             "e0": torch.zeros(geom.shape, dtype=torch.float32, device="cuda"),
             "e1": torch.zeros(geom.shape, dtype=torch.float32, device="cuda")}
-    e0, e1 = ev(), ev()
-    e0.record(stream)
-    xm, res = dc.run(geom, xm, n, args.period, stream, work)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    tmix = e0.elapsed_time(e1)
-    smix = dc.s64.compare(geom, xm, ref, "f64")
-    tc = None
-    if spec.dimension == 2 and spec.neighbourhood == "Box" and spec.range <= 8:
-        # the same defect-corrected iteration with the FP32 sweeps on the tensor cores
-        dtc = DefectCorrectedSweeps(spec, launch, mask=mask, tensor_cores=True)
+    xm = torch.from_numpy(a).cuda()
+    dc.run(geom, xm, 2, period, stream, work)  # warm-up
+    xm.copy_(torch.from_numpy(a))
+    (xm, res), t = timed(lambda: dc.run(geom, xm, n, period, stream, work))
+    forms["f32_defect_corrected"] = {"ms": t, **err(s64.compare(geom, xm, ref_final, "f64")),
+                                     "fp64_sweeps": res.fp64_sweeps, "fp32_sweeps": res.fp32_sweeps,
+                                     "fused": dc.fused}
+    xt = None
+    if dtc:
         xt = torch.from_numpy(a).cuda()
-        dtc.run(geom, xt, 2, args.period, stream, work)  # warm-up (Toeplitz operands, tensor maps)
+        dtc.run(geom, xt, 2, period, stream, work)  # warm-up (Toeplitz operands, tensor maps)
         xt.copy_(torch.from_numpy(a))
-        e0, e1 = ev(), ev()
-        e0.record(stream)
-        xt, rtc = dtc.run(geom, xt, n, args.period, stream, work)
-        e1.record(stream)
-        torch.cuda.synchronize()
-        ttc = e0.elapsed_time(e1)
-        stc = dc.s64.compare(geom, xt, ref, "f64")
-        # raw FP32 tensor-core sweeps (no correction) for the kernel rate
-        x32 = torch.from_numpy(a.astype(np.float32)).cuda()
-        y32 = x32.clone()
-        dtc.s32.tc_update_grid(geom, x32, y32)
-        e0, e1 = ev(), ev()
-        e0.record(stream)
-        for i in range(20):
-            (dtc.s32.tc_update_grid(geom, x32, y32) if i % 2 == 0 else dtc.s32.tc_update_grid(geom, y32, x32))
-        e1.record(stream)
-        torch.cuda.synchronize()
-        tsweep = e0.elapsed_time(e1) / 20
+        (xt, rtc), t = timed(lambda: dtc.run(geom, xt, n, period, stream, work))
+        forms["tensor_cores_defect_corrected"] = {"ms": t, **err(s64.compare(geom, xt, ref_final, "f64"))}
+        xs = torch.from_numpy(a32).cuda()
+        ys = xs.clone()
+        dtc.s32.tc_update_grid(geom, xs, ys)
+
+        def tc_sweeps():
+            u, v = xs, ys
+            for _ in range(n):
+                dtc.s32.tc_update_grid(geom, u, v)
+                u, v = v, u
+            return u
+
+        r, t = timed(tc_sweeps)
+        forms["tensor_cores"] = {"ms": t, **err(s64.compare(geom, r, ref_final, "f32"))}
         if dtc.s32.device_status() != 0:
             raise RuntimeError("device status word set during the tensor-core sweeps")
-        tc = {"glups": None, "ms": ttc, "max_rel": stc["max_rel"], "rms_rel": stc["rms_rel"],
-              "fp64_sweeps": rtc.fp64_sweeps, "fp32_sweeps": rtc.fp32_sweeps, "sweep_ms": tsweep}
-        del x32, y32, xt
+        del xs, ys
+
+    # ---- defect-corrected iterates at every period boundary -----------------------------------
+    periods = {"f32_defect_corrected": []}
+    if dtc:
+        periods["tensor_cores_defect_corrected"] = []
+    reset()
+    xm.copy_(torch.from_numpy(a))
+    if xt is not None:
+        xt.copy_(torch.from_numpy(a))
+    done = 0
+    cur = x
+    while done < n:
+        k = min(period, n - done)
+        nxt = y if cur is x else x
+        cur = s64.sweeps(geom, cur, nxt, k, launch, stream)
+        dc.run(geom, xm, k, period, stream, work)
+        periods["f32_defect_corrected"].append({"sweep": done + k, **err(s64.compare(geom, xm, cur, "f64"))})
+        if xt is not None:
+            dtc.run(geom, xt, k, period, stream, work)
+            periods["tensor_cores_defect_corrected"].append({"sweep": done + k,
+                                                             **err(s64.compare(geom, xt, cur, "f64"))})
+        done += k
+    for name, rows in periods.items():
+        forms[name]["max_rel_over_periods"] = max(q["max_rel"] for q in rows)
+
     glups = lambda ms: points * n / (ms / 1e3) / 1e9  # noqa: E731
+    for f in forms.values():
+        f["glups"] = glups(f["ms"])
+        f["speedup_vs_f64"] = t64 / f["ms"]
+    # FP64 is bound by the FP64 pipe on long stencils: 2S-1 flops per point (cuda/benchmark.cpp:76-81)
+    flops = spec.flops_per_update * points * n / (t64 / 1e3)
     return {
-        "metric": "GLup/s (%s, %d sweeps, FP32 sweeps with FP64 defect correction every %d)" % (w.name, n, args.period),
-        "value": glups(tmix), "unit": "GLup/s", "n_gpus": 1, "steps": n, "warmup": 3,
-        "ms_per_step": tmix / n, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32+f64", "data": "synthetic (numpy default_rng seed %d)" % w.seed,
+        "metric": "GLup/s (%s, %d sweeps, FP32 sweeps with FP64 defect correction every %d)" % (w.name, n, period),
+        "value": glups(forms["f32_defect_corrected"]["ms"]), "unit": "GLup/s", "n_gpus": 1, "steps": n, "warmup": 3,
+        "ms_per_step": forms["f32_defect_corrected"]["ms"] / n, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic (numpy default_rng seed %d)" % w.seed,
         "config": {"workload": w.name, "grid": list(w.grid[:spec.dimension]), "coarsening": list(spec.coarsening),
-                   "block": list(launch.block), "variant": launch.variant, "period": args.period,
+                   "block": list(launch.block), "variant": launch.variant, "period": period,
                    "f32_coarsening": list(dc.spec32.coarsening), "f32_block": list(launch32.block),
                    "f32_chunk": launch32.chunk},
         "precision": {
-            "f64": {"glups": glups(t64), "ms": t64},
-            "f32": {"glups": glups(t32), "ms": t32, "max_rel": s32["max_rel"], "rms_rel": s32["rms_rel"]},
-            "f32_compensated": {"glups": glups(t32c), "ms": t32c, "max_rel": s32c_err["max_rel"],
-                                "rms_rel": s32c_err["rms_rel"], "variant": p32c.variant, "block": list(p32c.block)},
-            "f32_defect_corrected": {"glups": glups(tmix), "ms": tmix, "max_rel": smix["max_rel"],
-                                     "rms_rel": smix["rms_rel"], "fp64_sweeps": res.fp64_sweeps,
-                                     "fp32_sweeps": res.fp32_sweeps,
-                                     "final_residual_max": res.residual_history[-1][0]},
-            "speedup_vs_f64": t64 / tmix,
-            "tensor_core_defect_corrected": tc and {**tc, "glups": glups(tc["ms"]),
-                                                     "sweep_glups": points / (tc["sweep_ms"] / 1e3) / 1e9,
-                                                     "speedup_vs_f64": t64 / tc["ms"]},
+            "f64": {"glups": glups(t64), "ms": t64, "tflops": flops / 1e12,
+                    "fp64_pipe_frac_nominal": flops / FP64_PEAK_FLOPS},
+            **forms,
+            "per_sweep": per_sweep,
+            "periods": periods,
             "error_definition": "max_rel = max|a-b| / max|b|, rms_rel = ||a-b||_2 / ||b||_2 over the interior, "
-                                "b = FP64 result after the same sweeps",
+                                "b = FP64 result after the same sweeps from the same input",
         },
     }
 
@@ -895,6 +1035,8 @@ def main(argv=None) -> int:
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--e2e-steps", type=int, default=6)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="headline workload only (skip the other configurations' records)")
     ap.add_argument("--precision", default="f64", choices=["f64", "mixed"],
                     help="mixed: FP64 vs FP32 vs FP32 with FP64 defect correction on the workload")
     ap.add_argument("--sweeps", type=int, default=0, help="precision mode: sweeps (default: the workload's)")
