@@ -75,3 +75,25 @@ def pipe_sweeps(cfg, a: np.ndarray, grid, left_offset, right_offset, n: int, mas
                        ctypes.c_uint(unroll))
         x, y = y, x
     return x
+
+
+def tb3_passes(cfg, a: np.ndarray, grid, left_offset, right_offset, n: int, mask=None, precision="f64",
+               block=(8, 8), piece: int = 1 << 30, unroll: int = 2):
+    """n passes (2n sweeps) through the host build of the 3D two-sweep kernel's control flow,
+    compiled with the kernel's own thread tile (2 x 2 for even ranges, 1 x 1 for odd ones)."""
+    d, sh, o, c, r, cx, cy, cz, al, cl = cfg
+    C = 2 if r % 2 == 0 else 1
+    lib = build((d, sh, o, c, r, C, C, 1, al, cl), precision, "tb3_host.cpp")
+    x = np.ascontiguousarray(a).copy()
+    y = x.copy()
+    m = np.ascontiguousarray(np.zeros(1) if mask is None else np.asarray(mask, dtype=np.float64))
+    u3 = ctypes.c_uint * 3
+    for _ in range(n):
+        rc = lib.tb3_pass(u3(*grid), ctypes.c_uint(left_offset), ctypes.c_uint(right_offset),
+                          ctypes.c_int(0 if al == "None" else 1), x.ctypes.data_as(ctypes.c_void_p),
+                          y.ctypes.data_as(ctypes.c_void_p), m.ctypes.data_as(ctypes.c_void_p),
+                          ctypes.c_uint(block[0]), ctypes.c_uint(block[1]), ctypes.c_uint(piece),
+                          ctypes.c_uint(unroll))
+        assert rc == 0
+        x, y = y, x
+    return x

@@ -1,0 +1,37 @@
+"""The 3D two-sweep kernel's control flow on the CPU (tests/host_tile/tb3_host.cpp): one pass
+equals two oracle sweeps bit for bit -- extended and output tiles, ragged last tiles, the border
+copy into the plane buffer, pieces that restart both pipelines, the slot rotation at chunk ends."""
+
+import numpy as np
+import pytest
+
+import host_tile
+import oracle as O
+
+CASES = [
+    # (cfg, grid, block (threads), piece, unroll)
+    ((3, "Star", "Row", "Jacobi", 2, 2, 2, 2, "None", 0), (37, 29, 23), (8, 6), 7, 2),
+    ((3, "Star", "Row", "Variable", 2, 1, 1, 1, "Read", 16), (45, 26, 19), (16, 4), 1 << 30, 3),
+    ((3, "Box", "Row", "Jacobi", 1, 1, 1, 1, "None", 0), (29, 23, 17), (8, 8), 5, 2),
+    ((3, "Box", "Column", "Variable", 1, 2, 1, 1, "Write", 8), (33, 20, 15), (6, 5), 4, 1),
+    ((3, "Star", "Column", "Variable", 3, 1, 1, 1, "Write", 8), (41, 30, 22), (12, 10), 6, 2),
+    ((3, "Star", "Row", "Variable", 4, 2, 2, 1, "Read", 16), (52, 40, 26), (10, 8), 9, 3),
+    ((3, "Box", "Row", "Variable", 2, 2, 2, 1, "None", 0), (31, 27, 16), (6, 6), 1 << 30, 2),
+]
+
+
+@pytest.mark.parametrize("precision", ["f64", "f32"])
+@pytest.mark.parametrize("case", CASES, ids=lambda c: "%s_%s_%s_r%d_b%dx%d" % (c[0][1], c[0][2], c[0][3], c[0][4],
+                                                                             c[2][0], c[2][1]))
+def test_two_sweep_pass_equals_two_sweeps(case, precision):
+    cfg, n, block, piece, unroll = case
+    spec = O.make_spec(*cfg)
+    g = O.geometry(spec, *n)
+    rng = np.random.default_rng(61)
+    dt = np.float64 if precision == "f64" else np.float32
+    a = rng.uniform(-1, 1, (g.grid[2], g.grid[1], g.grid[0])).astype(dt)
+    mask = rng.standard_normal(O.stencil_size(spec)) if cfg[3] == "Variable" else None
+    want = O.sweeps(spec, a, 4, g.right_offset, mask)
+    got = host_tile.tb3_passes(cfg, a, g.grid, g.left_offset, g.right_offset, 2, mask, precision, block, piece,
+                               unroll)
+    assert np.array_equal(got, want)

@@ -137,6 +137,9 @@ SIGNATURES = {
     "tcs_defect_sweep": [_vp, U3, _u, _P(CLaunch), _vp, _vp, _P(ctypes.c_double), _vp],
     "tcs_update_grid_accumulate": [_vp, U3, _u, _P(CLaunch), _vp, _vp, _vp, _vp],
     "tcs_precompile_pipe_epilogue": [_P(CSpec), _u, _u, _u, _u, ctypes.c_char_p, _u],
+    "tcs_sweeps_tb3": [_vp, U3, _u, _P(CLaunch), _vp, _vp, _u, _vp, _P(ctypes.c_int)],
+    "tcs_plan_tb3": [_vp, U3, _u, _P(CLaunch), _P(CPlan)],
+    "tcs_precompile_tb3": [_P(CSpec), _u, _u, _u, ctypes.c_char_p, _u],
     "tcs_scratch_bytes": [_vp, _P(ctypes.c_ulonglong)],
     "tcs_benchmark_durations": [_vp, _vp, _u, _P(_u)],
     "tcs_accumulate": [_vp, U3, _u, _vp, _vp, _vp],

@@ -217,8 +217,10 @@ struct PipeKey {
   unsigned bx, by, ch, lshift;
   unsigned batch = 0;
   unsigned epi = 0;  // epilogue mode (tcs_kernels.cuh, TCS_EPI): 0 plain, 1 FP64 defect, 2 FP32 accumulate
+  unsigned tb3 = 0;  // tcs_tb3 (two sweeps per pass, 3D) with thread tiles tb3 x tb3; 0: tcs_pipe
   bool operator==(const PipeKey& o) const {
-    return bx == o.bx && by == o.by && ch == o.ch && lshift == o.lshift && batch == o.batch && epi == o.epi;
+    return bx == o.bx && by == o.by && ch == o.ch && lshift == o.lshift && batch == o.batch && epi == o.epi &&
+           tb3 == o.tb3;
   }
 };
 
@@ -229,6 +231,11 @@ std::string instance_macros(const tcs_spec& s, const PipeKey* pk) {
       << "\n#define TCS_CH " << pk->ch << "\n#define TCS_LSHIFT " << pk->lshift << "\n";
   if (pk && pk->batch) m << "#define TCS_BATCH 1\n";
   if (pk && pk->epi) m << "#define TCS_EPI " << pk->epi << "\n";
+  if (pk && pk->tb3) m << "#define TCS_TB3 1\n";
+  // the two-sweep kernel has thread tiles of its own (tb3 x tb3 x 1); the term order of every
+  // output does not depend on them
+  const int cx = (pk && pk->tb3) ? (int)pk->tb3 : s.cx, cy = (pk && pk->tb3) ? (int)pk->tb3 : s.cy;
+  const int cz = (pk && pk->tb3) ? 1 : (s.dimension == 3 ? s.cz : 1);
   m << "#define TCS_T " << (s.precision == TCS_F64 ? "double" : "float") << "\n"
     << "#define TCS_COMP " << (s.precision == TCS_F32C ? 1 : 0) << "\n"
     << "#define TCS_DIM " << s.dimension << "\n"
@@ -236,9 +243,9 @@ std::string instance_macros(const tcs_spec& s, const PipeKey* pk) {
     << "#define TCS_ORIENT " << s.orientation << "\n"
     << "#define TCS_COEFF " << s.coefficients << "\n"
     << "#define TCS_R " << s.range << "\n"
-    << "#define TCS_CX " << s.cx << "\n"
-    << "#define TCS_CY " << s.cy << "\n"
-    << "#define TCS_CZ " << (s.dimension == 3 ? s.cz : 1) << "\n";
+    << "#define TCS_CX " << cx << "\n"
+    << "#define TCS_CY " << cy << "\n"
+    << "#define TCS_CZ " << cz << "\n";
   return m.str();
 }
 
@@ -599,7 +606,8 @@ int pipe_module(tcs_stencil* h, const PipeKey& key, PipeMod** out) {
     return fail(TCS_ERR_CUDA, "cuModuleLoadData (pipe): " + cu_msg(cr));
   }
   size_t bytes = 0;
-  if ((cr = g_drv.ModuleGetFunction(&pm->f, pm->mod, key.batch ? "tcs_pipe_batch" : "tcs_pipe")) !=
+  if ((cr = g_drv.ModuleGetFunction(&pm->f, pm->mod,
+                                    key.batch ? "tcs_pipe_batch" : (key.tb3 ? "tcs_tb3" : "tcs_pipe"))) !=
           CUDA_SUCCESS ||
       (cr = g_drv.ModuleGetGlobal(&pm->mask_ptr, &pm->mask_bytes, pm->mod, "tcs_mask")) != CUDA_SUCCESS ||
       (cr = g_drv.ModuleGetGlobal(&pm->status_ptr, &bytes, pm->mod, "tcs_status")) != CUDA_SUCCESS) {
@@ -815,6 +823,124 @@ int resolve_pipe(tcs_stencil* h, const TcsGeo& g, const tcs_launch* L, Resolved&
   return TCS_OK;
 }
 
+// The two-sweep kernel tcs_tb3 (3D): thread tiles C x C with C = 2 for even ranges and 1 for odd
+// ones (C divides R, so a thread tile lies wholly inside or outside the output tile); by default
+// an extended tile of 64 x 32 columns (C = 2: 32 x 16 threads) or 32 x 32 (C = 1: 32 x 32
+// threads), whose inner (EX - 2R) x (EY - 2R) columns are the output tile.  `L` (may be NULL)
+// gives the block (bx, by) and the planes per ring chunk.
+int resolve_tb3(tcs_stencil* h, const TcsGeo& g, const tcs_launch* L, Resolved& out) {
+  const tcs_spec& s = h->spec;
+  if (s.dimension != 3) return fail(TCS_ERR_UNSUPPORTED, "tb3: 3D stencils only");
+  if (s.precision == TCS_F32C) return fail(TCS_ERR_UNSUPPORTED, "tb3: plain FP64 or FP32 sweeps only");
+  const unsigned R = (unsigned)s.range;
+  const unsigned es = (unsigned)elem_size(s), vec = 16u / es;
+  const unsigned C = (R % 2 == 0) ? 2u : 1u;
+  unsigned bx = (C == 2) ? 32u : 32u, by = (C == 2) ? 16u : 32u;
+  if (L && L->block[0]) {
+    bx = L->block[0];
+    by = L->block[1] ? L->block[1] : 1u;
+  }
+  const unsigned EX = bx * C, EY = by * C;
+  if (EX <= 2 * R || EY <= 2 * R) return fail(TCS_ERR_UNSUPPORTED, "tb3: tile too small for the range");
+  const unsigned OX = EX - 2 * R, OY = EY - 2 * R;
+  if (OX % vec != 0) return fail(TCS_ERR_UNSUPPORTED, "tb3: output tile width not a multiple of 16 bytes");
+  const unsigned lshift = (unsigned)((((int)h->left_off - (int)R) % (int)vec + (int)vec) % (int)vec);
+  const unsigned ch = (L && L->chunk) ? L->chunk : 2u;
+  const unsigned rows = EY + 2 * R;
+  const unsigned W = pipe_width(EX, R, lshift, vec, ch, rows, es);
+  if (W > 256 || rows > 256) return fail(TCS_ERR_UNSUPPORTED, "tb3: tile exceeds the 256-element TMA box limit");
+  const unsigned chunk_bytes = ch * rows * W * es;
+  const unsigned buf_bytes = 2u * (EX + 2 * R) * (EY + 2 * R) * es;
+  PipeKey key{bx, by, ch, lshift, 0u, 0u, C};
+  PipeMod* pm = nullptr;
+  int rc = pipe_module(h, key, &pm);
+  if (rc) return rc;
+  const int nthr = (int)(bx * by);
+  int maxthr = 0;
+  TCS_CU(g_drv.FuncGetAttribute(&maxthr, CU_FUNC_ATTRIBUTE_MAX_THREADS_PER_BLOCK, pm->f));
+  if (nthr > maxthr) return fail(TCS_ERR_UNSUPPORTED, "tb3: block exceeds the kernel's thread limit");
+  unsigned nslot = (L && L->depth) ? 1 + L->depth : 3u, smem = 0;
+  for (;; --nslot) {
+    smem = ((nslot * 8 + 127) / 128) * 128 + 128 + nslot * chunk_bytes + buf_bytes;
+    if (smem <= (unsigned)h->smem_optin || nslot == 2) break;
+  }
+  if (smem > (unsigned)h->smem_optin) return fail(TCS_ERR_UNSUPPORTED, "tb3: ring does not fit in shared memory");
+  {
+    std::lock_guard<std::mutex> lock(h->mu);
+    if ((int)smem > pm->smem_attr) {
+      TCS_CU(g_drv.FuncSetAttribute(pm->f, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, (int)smem));
+      pm->smem_attr = (int)smem;
+    }
+  }
+  int occ = 0;
+  TCS_CU(g_drv.OccMaxActive(&occ, pm->f, nthr, smem));
+  if (occ < 1) return fail(TCS_ERR_UNSUPPORTED, "tb3 kernel cannot be resident at this shape");
+  const unsigned long long ex = g.x_lim > g.x0 ? g.x_lim - g.x0 : 0;
+  const unsigned ntx = std::max(1u, cdiv(ex, OX)), nty = std::max(1u, cdiv(g.y_lim - R, OY));
+  const unsigned long long M = g.z_lim - R;
+  const unsigned long long total = (unsigned long long)ntx * nty * M;
+  unsigned long long nctas = (unsigned long long)h->num_sms * (unsigned)occ;
+  if (L && L->segments) nctas = L->segments;
+  const unsigned long long per = std::max<unsigned long long>(1, (total + nctas - 1) / nctas);
+  const unsigned long long grid = std::max<unsigned long long>(1, (total + per - 1) / per);
+  out = Resolved{};
+  out.variant = TCS_VARIANT_PIPE;
+  out.geo = g;
+  out.geo.width = W;
+  out.geo.nslot = nslot;
+  out.pipe = pm;
+  out.chunk = ch;
+  TcsPipeGeo& pg = out.pgeo;
+  pg = TcsPipeGeo{};
+  pg.xdim = g.xdim;
+  pg.ydim = g.ydim;
+  pg.zdim = g.zdim;
+  pg.total = total;
+  pg.per_cta = per;
+  pg.x0 = g.x0;
+  pg.x_lim = g.x_lim;
+  pg.y_lim = g.y_lim;
+  pg.z_lim = g.z_lim;
+  pg.ntx = ntx;
+  pg.m = (unsigned)M;
+  pg.nslot = nslot;
+  pg.loader = ((g.xdim * es) % 16 == 0) ? 0u : 1u;
+  out.geo.loader = pg.loader;
+  out.grid[0] = (unsigned)grid;
+  out.block[0] = bx;
+  out.block[1] = by;
+  out.block[2] = 1;
+  out.box[0] = W;
+  out.box[1] = rows;
+  out.box[2] = ch;
+  out.smem = smem;
+  out.depth = nslot - 1;
+  out.occ = occ;
+  return TCS_OK;
+}
+
+int fill_plan(const tcs_stencil* h, const Resolved& r, tcs_plan* out) {
+  if (out) {
+    tcs_plan p{};
+    p.variant = r.variant;
+    for (int i = 0; i < 3; ++i) {
+      p.grid_blocks[i] = r.grid[i];
+      p.block[i] = r.block[i];
+    }
+    p.dyn_smem = r.smem;
+    p.seg_len = r.geo.seg;
+    p.nslot = r.geo.nslot;
+    p.width = r.geo.width;
+    p.chunk = r.chunk;
+    p.depth = r.depth;
+    p.loader = r.geo.loader;
+    p.ctas_per_sm = r.occ;
+    p.num_sms = h->num_sms;
+    *out = p;
+  }
+  return TCS_OK;
+}
+
 int resolve(tcs_stencil* h, const unsigned grid[3], unsigned right_offset, const tcs_launch* L,
             Resolved& out) {
   if (!h || !L) return fail(TCS_ERR_INVALID_VALUE, "NULL handle or launch");
@@ -950,6 +1076,23 @@ int launch_fringe(tcs_stencil* h, const TcsGeo& g, const void* in, void* out, co
     TCS_CU(g_drv.LaunchKernel(h->f_fringe, cdiv(xb - xa, bx), cdiv(yb - ya, by), d3 ? cdiv(zb - za, bz) : 1, bx, by,
                               bz, 0, st, args, nullptr));
   }
+  return TCS_OK;
+}
+
+int launch_tb3(tcs_stencil* h, const Resolved& r, const void* in, void* out, CUstream st) {
+  TcsPipeGeo pg = r.pgeo;
+  if (reinterpret_cast<uintptr_t>(in) % 16 != 0) pg.loader = 1;  // TMA needs a 16-byte aligned base
+  alignas(64) CUtensorMap pmap;
+  std::memset(&pmap, 0, sizeof(pmap));
+  if (pg.loader == 0) {
+    CUtensorMap* map = nullptr;
+    int rc = tensor_map(h, in, r, &map);
+    if (rc) return rc;
+    pmap = *map;
+  }
+  CUdeviceptr pin = (CUdeviceptr)in, pout = (CUdeviceptr)out;
+  void* args[] = {&pmap, &pin, &pout, &pg};
+  TCS_CU(g_drv.LaunchKernel(r.pipe->f, r.grid[0], 1, 1, r.block[0], r.block[1], 1, r.smem, st, args, nullptr));
   return TCS_OK;
 }
 
@@ -1193,25 +1336,7 @@ int tcs_plan_launch(tcs_stencil* h, const unsigned grid[3], unsigned right_offse
   Resolved r;
   int rc = resolve(h, grid, right_offset, launch, r);
   if (rc) return rc;
-  if (out) {
-    tcs_plan p{};
-    p.variant = r.variant;
-    for (int i = 0; i < 3; ++i) {
-      p.grid_blocks[i] = r.grid[i];
-      p.block[i] = r.block[i];
-    }
-    p.dyn_smem = r.smem;
-    p.seg_len = r.geo.seg;
-    p.nslot = r.geo.nslot;
-    p.width = r.geo.width;
-    p.chunk = r.chunk;
-    p.depth = r.depth;
-    p.loader = r.geo.loader;
-    p.ctas_per_sm = r.occ;
-    p.num_sms = h->num_sms;
-    *out = p;
-  }
-  return TCS_OK;
+  return fill_plan(h, r, out);
 }
 
 int tcs_update_grid(tcs_stencil* h, const unsigned grid[3], unsigned right_offset,
@@ -2297,6 +2422,73 @@ int tcs_sweeps_tb2(tcs_stencil* h, const unsigned grid[3], unsigned right_offset
     std::swap(src, dst);
   }
   if (result_in_b) *result_in_b = (src == b) ? 1 : 0;
+  return TCS_OK;
+}
+
+int tcs_sweeps_tb3(tcs_stencil* h, const unsigned grid[3], unsigned right_offset, const tcs_launch* launch,
+                   void* a, void* b, unsigned n, void* stream, int* result_in_b) {
+  if (!h) return fail(TCS_ERR_INVALID_VALUE, "NULL handle");
+  if (!a || !b || a == b) return fail(TCS_ERR_INVALID_VALUE, "need two distinct buffers");
+  TcsGeo g;
+  int rc = make_geo(h, grid, right_offset, g);
+  if (rc) return rc;
+  if (has_fringe(h, g)) return fail(TCS_ERR_UNSUPPORTED, "tb3: grids of whole coarsening tiles only");
+  Resolved r;
+  if ((rc = resolve_tb3(h, g, launch, r))) return rc;
+  void* src = a;
+  void* dst = b;
+  for (unsigned i = 0; i + 1 < n; i += 2) {  // pairs of sweeps, one pass each
+    if ((rc = launch_tb3(h, r, src, dst, (CUstream)stream))) return rc;
+    std::swap(src, dst);
+  }
+  if (n % 2 == 1) {  // the last odd sweep: one ordinary sweep
+    tcs_launch L{};
+    L.block[0] = 32;
+    L.block[1] = 4;
+    L.block[2] = 1;
+    L.variant = TCS_VARIANT_AUTO;
+    Resolved r1;
+    if ((rc = resolve(h, grid, right_offset, &L, r1))) return rc;
+    if ((rc = launch_resolved(h, r1, src, dst, (CUstream)stream))) return rc;
+    std::swap(src, dst);
+  }
+  if (result_in_b) *result_in_b = (src == b) ? 1 : 0;
+  return TCS_OK;
+}
+
+int tcs_plan_tb3(tcs_stencil* h, const unsigned grid[3], unsigned right_offset, const tcs_launch* launch,
+                 tcs_plan* plan) {
+  if (!h || !plan) return fail(TCS_ERR_INVALID_VALUE, "NULL argument");
+  TcsGeo g;
+  int rc = make_geo(h, grid, right_offset, g);
+  if (rc) return rc;
+  Resolved r;
+  if ((rc = resolve_tb3(h, g, launch, r))) return rc;
+  return fill_plan(h, r, plan);
+}
+
+int tcs_precompile_tb3(const tcs_spec* spec, unsigned bx, unsigned by, unsigned chunk, char* cubin_path,
+                       unsigned path_cap) {
+  int rc = validate(spec);
+  if (rc) return rc;
+  if (spec->dimension != 3) return fail(TCS_ERR_UNSUPPORTED, "tb3: 3D stencils only");
+  const unsigned R = (unsigned)spec->range, vec = 16u / (unsigned)elem_size(*spec);
+  const unsigned C = (R % 2 == 0) ? 2u : 1u;
+  if (bx == 0) {
+    bx = 32;
+    by = (C == 2) ? 16u : 32u;
+  }
+  if (bx * C <= 2 * R || by * C <= 2 * R || (bx * C - 2 * R) % vec != 0)
+    return fail(TCS_ERR_UNSUPPORTED, "tb3: no output tile of 16-byte multiples for this range and block");
+  const unsigned lshift = (unsigned)((((int)left_offset_of(*spec) - (int)R) % (int)vec + (int)vec) % (int)vec);
+  PipeKey key{bx, by, chunk ? chunk : 2u, lshift, 0u, 0u, C};
+  std::vector<char> cubin;
+  std::string path;
+  if ((rc = instantiate(*spec, &key, cubin, &path))) return rc;
+  if (cubin_path && path_cap) {
+    std::strncpy(cubin_path, path.c_str(), path_cap - 1);
+    cubin_path[path_cap - 1] = '\0';
+  }
   return TCS_OK;
 }
 

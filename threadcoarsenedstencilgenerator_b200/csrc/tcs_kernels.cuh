@@ -873,7 +873,7 @@ __device__ __forceinline__ PipeState pipe_setup(tcs_u32 nslot, bool single_arriv
 
 }  // namespace tcs
 
-#ifndef TCS_BATCH
+#if !defined(TCS_BATCH) && !defined(TCS_TB3)
 extern "C" __global__ void __launch_bounds__(TCS_BX * ((TCS_DIM == 3) ? TCS_BY : 1))
     tcs_pipe(const __grid_constant__ TcsTmaMap tmap, const T* __restrict__ in,
              T* __restrict__ out, const T* __restrict__ src, const TcsPipeGeo g, void* aux,
@@ -940,7 +940,7 @@ extern "C" __global__ void __launch_bounds__(TCS_BX * ((TCS_DIM == 3) ? TCS_BY :
     }
   }
 }
-#endif  // !TCS_BATCH
+#endif  // !TCS_BATCH && !TCS_TB3
 
 #ifdef TCS_BATCH
 // ---- tcs_pipe_batch: one persistent launch over many grids of the same parameter set ---------
@@ -995,4 +995,220 @@ extern "C" __global__ void __launch_bounds__(TCS_BX * ((TCS_DIM == 3) ? TCS_BY :
   }
 }
 #endif  // TCS_BATCH
+
+#ifdef TCS_TB3
+// ---- tcs_tb3: two sweeps in one pass over HBM (temporal blocking, 3D) -------------------------
+// The pipelined sweep run twice in the same CTA, stage 2 on the output of stage 1.  A CTA owns an
+// extended tile of TB_EX x TB_EY columns (its threads' coverage, CX x CY per thread, with CX = CY
+// dividing R) and streams its input planes through the TMA ring as tcs_pipe does.  Stage 1 keeps
+// 2R+1 planes of S(in) over the extended tile in registers (pipeline 1); each completed plane of
+// S(in) goes to a shared-memory plane buffer (two, used in turn), where points outside the grid's
+// interior take the input's value (the fixed border of the ping-pong pair).  Stage 2 applies that
+// plane to its own register pipeline (pipeline 2) and stores the completed planes of S(S(in)) for
+// the inner (TB_EX - 2R) x (TB_EY - 2R) columns; the outer ring of threads only serves stage 1.
+// Both stages use the per-output term order of one sweep, so out = S(S(in)) bit for bit.
+namespace tcs {
+constexpr int TB_EX = TXP, TB_EY = TYP;                      // extended tile (stage 1)
+constexpr int TB_OX = TB_EX - 2 * R, TB_OY = TB_EY - 2 * R;  // output tile (stage 2)
+constexpr int TB_BW = TB_EX + 2 * R, TB_BH = TB_EY + 2 * R;  // plane buffer, range-wide margin
+static_assert(DIM == 3, "tcs_tb3 is the 3D two-sweep kernel");
+static_assert(TB_OX > 0 && TB_OY > 0 && TB_OX % VEC == 0, "output tile: positive, 16-byte multiple");
+static_assert(R % CX == 0 && R % CY == 0, "thread tiles must not straddle the output tile's edge");
+static_assert(!COMP && EPI == 0, "plain sweeps only");
+
+// Reader of a stage-1 plane in the plane buffer at a thread origin (row pitch TB_BW).  Pairs are
+// aligned where the buffer column R + gx is even (the buffer starts on 128 bytes, TB_BW is even).
+struct TbPlane {
+  const T* p;
+  __host__ __device__ static constexpr bool pair_aligned(int gx) {
+    return (CX % 2 == 0) && (TB_BW % 2 == 0) && (((R + gx) % 2 + 2) % 2 == 0);
+  }
+  template <int GX, int GY>
+  __device__ __forceinline__ T one() const {
+    return p[GY * TB_BW + GX];
+  }
+  template <int GX, int GY>
+  __device__ __forceinline__ void two(T& a, T& b) const {
+    const typename PairOf<T>::type v = *reinterpret_cast<const typename PairOf<T>::type*>(p + GY * TB_BW + GX);
+    a = v.x;
+    b = v.y;
+  }
+};
+
+// One piece: tile `tile`, output planes [R + zs, R + ze).  Returns false when a wait expired.
+__device__ __forceinline__ bool tb3_piece(const PipeGridView& G, tcs_u32 tile, tcs_u32 zs, tcs_u32 ze,
+                                          PipeState& st, PipeSlot (&acc1)[NP2], PipeSlot (&acc2)[NP2],
+                                          T* bbuf) {
+  constexpr tcs_u32 CHUNK_BYTES = CHUNK * (tcs_u32)sizeof(T);
+  const tcs_u32 nslot = st.nslot, tid = st.tid, bars = st.bars, gc = st.gc;
+  const bool use_tma = G.use_tma;
+  const int ms = R + (int)zs;                       // first output plane
+  const int nout = (int)(ze - zs);
+  const int np = nout + 4 * R;                      // input planes streamed
+  const tcs_u32 nch = (tcs_u32)((np + CHP - 1) / CHP);
+  const int m_first = ms - 2 * R;                   // input plane of pi = 0
+  const int X0 = (int)G.x0 - R + (int)(tile % G.ntx) * TB_OX;  // extended tile origin
+  const int Y0 = (int)(tile / G.ntx) * TB_OY;                  // = R + ty*TB_OY - R
+  const int xl = X0 - R - LSHIFT;                   // TMA x start: a multiple of VEC (may be < 0)
+  auto issue = [&](tcs_u32 j) {
+    const tcs_u32 slot = (gc + j) % nslot;
+    const tcs_u32 bar = bars + 8u * slot;
+    const int m0 = m_first + (int)(j * CHP);
+    if (use_tma) {
+      mbar_expect_tx(bar, CHUNK_BYTES);
+      tma_load_3d(st.ring_s + slot * CHUNK_BYTES, G.map, bar, xl, Y0 - R, m0);
+    } else {
+      // negative coordinates wrap to large unsigned values and read as zeros
+      pipe_copy_chunk<1>(G, st.ring_s + slot * CHUNK_BYTES, (tcs_u32)xl, (tcs_u32)(Y0 - R), (tcs_u32)m0, tid);
+      cp_async_arrive(bar);
+    }
+  };
+  {
+    const tcs_u32 pro = min(nslot - 1, nch);
+    if (use_tma) {
+      if (tid == 0)
+        for (tcs_u32 j = 0; j < pro; ++j) issue(j);
+    } else {
+      for (tcs_u32 j = 0; j < pro; ++j) issue(j);
+    }
+  }
+  const int ex0 = (int)threadIdx.x * CX, ey0 = (int)threadIdx.y * CY;  // thread tile in the extended tile
+  const tcs_u32 lane_off = (R + threadIdx.y * CY) * PW + LSHIFT + R + threadIdx.x * CX;
+  const bool inner = ex0 >= R && ex0 < TB_EX - R && ey0 >= R && ey0 < TB_EY - R;
+  const tcs_i64 xdim = (tcs_i64)G.xdim, plane_g = (tcs_i64)(G.xdim * G.ydim);
+  constexpr T c = T(1) / T(S);
+  tcs_u32 cur_slot = gc % nslot;
+  tcs_u32 cur_par = (gc / nslot) & 1u;
+  bool aborted = false;
+  for (tcs_u32 j = 0; j < nch; ++j) {
+    const bool expired = mbar_wait_bounded(bars + 8u * cur_slot, cur_par, TCS_WAIT_LIMIT);
+    if (__syncthreads_or(expired)) {
+      if (use_tma) {
+        if (tid == 0) {
+          atomicOr(&tcs_status, TCS_DEV_TIMEOUT);
+          const tcs_u32 hi = min(j + nslot - 2, nch - 1);
+          for (tcs_u32 jj = j; jj <= hi; ++jj)
+            (void)mbar_wait_bounded(bars + 8u * ((gc + jj) % nslot), ((gc + jj) / nslot) & 1u, TCS_WAIT_LIMIT);
+        }
+      } else {
+        if (tid == 0) atomicOr(&tcs_status, TCS_DEV_TIMEOUT);
+        cp_async_wait_all();
+      }
+      aborted = true;
+      break;
+    }
+    if (j + nslot - 1 < nch) {
+      if (!use_tma)
+        issue(j + nslot - 1);
+      else if (tid == 0)
+        issue(j + nslot - 1);
+    }
+    const T* pc = st.ring + cur_slot * CHUNK + lane_off;
+    static_for<0, CHP>([&](auto tt) {
+      constexpr int t = decltype(tt)::value;
+      const int pi = (int)(j * CHP) + t;
+      if (pi < np) {
+        // stage 1: input plane m_first + pi; completes plane q = m_first + pi - R of S(in)
+        const PipeRing lda{pc + t * PLANE};
+        auto slot1 = [&](auto kk) -> PipeSlot& {
+          constexpr int k = decltype(kk)::value;
+          return acc1[((t - k) % NP2 + NP2) % NP2];
+        };
+        pipe_plane(lda, slot1);
+        const int q = m_first + pi - R;
+        T* bq = bbuf + (pi & 1) * (TB_BW * TB_BH);
+        PipeSlot& d1 = acc1[((t - 2 * R) % NP2 + NP2) % NP2];
+        static_for<0, CY>([&](auto ey) {
+          static_for<0, CX>([&](auto ex) {
+            constexpr int e = decltype(ex)::value + decltype(ey)::value * CX;
+            const int gx = X0 + ex0 + decltype(ex)::value, gy = Y0 + ey0 + decltype(ey)::value;
+            const bool interior = gx >= (int)G.x0 && gx < (int)G.x_lim && gy >= R && gy < (int)G.y_lim &&
+                                  q >= R && q < (int)G.z_lim;
+            T v = (COEFF == 0) ? slot_value<e>(d1) * c : slot_value<e>(d1);
+            if (!interior) {
+              const bool in_grid = gx >= 0 && gx < (int)G.xdim && gy >= 0 && gy < (int)G.ydim && q >= 0 &&
+                                   q < (int)G.zdim;
+              v = in_grid ? G.in[gx + gy * xdim + q * plane_g] : T(0);
+            }
+            bq[(R + ey0 + decltype(ey)::value) * TB_BW + R + ex0 + decltype(ex)::value] = v;
+          });
+        });
+        __syncthreads();
+        // stage 2: plane q of S(in); completes plane p = q - R of S(S(in)), output pi - 4R
+        const TbPlane ldb{bq + (R + ey0) * TB_BW + R + ex0};
+        auto slot2 = [&](auto kk) -> PipeSlot& {
+          constexpr int k = decltype(kk)::value;
+          return acc2[((t - k) % NP2 + NP2) % NP2];
+        };
+        pipe_plane(ldb, slot2);
+        const int op = pi - 4 * R;
+        if (inner && op >= 0 && op < nout) {
+          PipeSlot& d2 = acc2[((t - 2 * R) % NP2 + NP2) % NP2];
+          const tcs_i64 pz = (tcs_i64)(ms + op) * plane_g;
+          static_for<0, CY>([&](auto ey) {
+            static_for<0, CX>([&](auto ex) {
+              constexpr int e = decltype(ex)::value + decltype(ey)::value * CX;
+              const int ox = X0 + ex0 + decltype(ex)::value, oy = Y0 + ey0 + decltype(ey)::value;
+              if (ox < (int)G.x_lim && oy < (int)G.y_lim)
+                G.out[ox + oy * xdim + pz] = (COEFF == 0) ? slot_value<e>(d2) * c : slot_value<e>(d2);
+            });
+          });
+        }
+      }
+    });
+    if constexpr (CHP % NP2 != 0) {
+      PipeSlot tmp[NP2];
+      static_for<0, NP2>([&](auto m) { tmp[decltype(m)::value] = acc1[decltype(m)::value]; });
+      static_for<0, NP2>([&](auto m) { acc1[decltype(m)::value] = tmp[(decltype(m)::value + CHP) % NP2]; });
+      static_for<0, NP2>([&](auto m) { tmp[decltype(m)::value] = acc2[decltype(m)::value]; });
+      static_for<0, NP2>([&](auto m) { acc2[decltype(m)::value] = tmp[(decltype(m)::value + CHP) % NP2]; });
+    }
+    if (++cur_slot == nslot) {
+      cur_slot = 0;
+      cur_par ^= 1u;
+    }
+  }
+  st.gc = gc + nch;
+  return !aborted;
+}
+}  // namespace tcs
+
+// Work list: (output tile, output plane) items over persistent CTAs, as in tcs_pipe; the plane
+// buffer follows the ring in dynamic shared memory.
+extern "C" __global__ void __launch_bounds__(TCS_BX * TCS_BY)
+    tcs_tb3(const __grid_constant__ TcsTmaMap tmap, const T* __restrict__ in, T* __restrict__ out,
+            const TcsPipeGeo g) {
+  using namespace tcs;
+  PipeGridView G;
+  G.map = &tmap;
+  G.in = in;
+  G.out = out;
+  G.src = nullptr;
+  G.xdim = g.xdim;
+  G.ydim = g.ydim;
+  G.zdim = g.zdim;
+  G.x0 = g.x0;
+  G.x_lim = g.x_lim;
+  G.y_lim = g.y_lim;
+  G.z_lim = g.z_lim;
+  G.ntx = g.ntx;
+  G.use_tma = (g.loader == 0);
+  G.cp_pair = false;
+  G.st_pair = false;
+  G.aux = nullptr;
+  if (G.use_tma && threadIdx.x == 0 && threadIdx.y == 0) tma_prefetch_map(&tmap);
+  PipeState st = pipe_setup(g.nslot, G.use_tma);
+  T* bbuf = st.ring + g.nslot * CHUNK;
+  PipeSlot acc1[NP2], acc2[NP2];
+  const tcs_u64 w_begin = (tcs_u64)blockIdx.x * g.per_cta;
+  const tcs_u64 w_end = min(w_begin + g.per_cta, g.total);
+  for (tcs_u64 w = w_begin; w < w_end;) {
+    const tcs_u32 tile = (tcs_u32)(w / g.m);
+    const tcs_u32 zs = (tcs_u32)(w % g.m);
+    const tcs_u32 ze = (tcs_u32)min((tcs_u64)g.m, (tcs_u64)zs + (w_end - w));
+    w += ze - zs;
+    if (!tb3_piece(G, tile, zs, ze, st, acc1, acc2, bbuf)) return;
+  }
+}
+#endif  // TCS_TB3
 #endif  // TCS_PIPE

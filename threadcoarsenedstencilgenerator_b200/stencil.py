@@ -212,6 +212,24 @@ class Stencil:
                                             int(n), _stream(stream), ctypes.byref(in_b)))
         return b if in_b.value else a
 
+    def sweeps_tb3(self, geom: Geometry, a, b, n: int, launch: Launch | None = None, stream=None):
+        """n ping-pong sweeps starting from a, two per pass over HBM (3D temporal blocking,
+        bit-identical to n ordinary sweeps); returns the buffer holding the result.  ``launch``
+        optionally sets the kernel's block, ring chunk and depth."""
+        in_b = ctypes.c_int()
+        _lib.check(self._lib.tcs_sweeps_tb3(self._h, _lib.U3(*geom.grid), geom.right_offset,
+                                            None if launch is None else ctypes.byref(launch.to_c()), _ptr(a),
+                                            _ptr(b), int(n), _stream(stream), ctypes.byref(in_b)))
+        return b if in_b.value else a
+
+    def plan_tb3(self, geom: Geometry, launch: Launch | None = None) -> Plan:
+        """The launch of the two-sweep kernel for this grid."""
+        p = _lib.CPlan()
+        _lib.check(self._lib.tcs_plan_tb3(self._h, _lib.U3(*geom.grid), geom.right_offset,
+                                          None if launch is None else ctypes.byref(launch.to_c()), ctypes.byref(p)))
+        return Plan("tb3", tuple(p.grid_blocks), tuple(p.block), p.dyn_smem, p.seg_len, p.nslot, p.width, p.chunk,
+                    p.depth, {0: "tma"}.get(p.loader, "cp.async"), p.ctas_per_sm, p.num_sms)
+
     def tc_update_grid(self, geom: Geometry, src, dst, source=None, stream=None) -> None:
         """One FP32 sweep dst = stencil(src) (+ source) on the tensor cores (2D Box only; BF16
         hi/lo split, FP32 accumulation: a precision option, not the reference's bits)."""
@@ -305,6 +323,14 @@ def precompile_pipe_epilogue(spec: StencilSpec, block, chunk: int, epi: int) -> 
     b = tuple(block) + (1,) * (3 - len(block))
     _lib.check(_lib.load().tcs_precompile_pipe_epilogue(ctypes.byref(spec.to_c()), b[0], b[1], int(chunk), int(epi),
                                                         buf, 1024))
+    return buf.value.decode()
+
+
+def precompile_tb3(spec: StencilSpec, block=(0, 0), chunk: int = 0) -> str:
+    """Instantiate the 3D two-sweep kernel of ``spec`` into the cubin cache."""
+    buf = ctypes.create_string_buffer(1024)
+    _lib.check(_lib.load().tcs_precompile_tb3(ctypes.byref(spec.to_c()), int(block[0]), int(block[1]), int(chunk),
+                                              buf, 1024))
     return buf.value.decode()
 
 
