@@ -56,6 +56,9 @@ __global__ void __launch_bounds__(kThreads)
     uint64_t y, z;
     row_of(g, row, y, z);
     const uint64_t base = y * g.xdim + z * g.xdim * g.ydim;
+    // unrolled: several loads of a thread in flight at once (two blocks per SM alone do not
+    // keep enough bytes in flight to stream at the HBM rate)
+#pragma unroll 4
     for (uint32_t xx = g.x0 + threadIdx.x; xx < g.x_lim; xx += kThreads) {
       const double d = sx[base + xx] - x[base + xx];
       r[base + xx] = (float)d;
@@ -79,6 +82,9 @@ __global__ void __launch_bounds__(kThreads)
     uint64_t y, z;
     row_of(g, row, y, z);
     const uint64_t base = y * g.xdim + z * g.xdim * g.ydim;
+    // unrolled: several loads of a thread in flight at once (two blocks per SM alone do not
+    // keep enough bytes in flight to stream at the HBM rate)
+#pragma unroll 4
     for (uint32_t xx = g.x0 + threadIdx.x; xx < g.x_lim; xx += kThreads) {
       const double bv = b[base + xx];
       const double av = a_f32 ? (double)af[base + xx] : ad[base + xx];
@@ -116,6 +122,9 @@ __global__ void __launch_bounds__(kThreads)
     uint64_t y, z;
     row_of(g, row, y, z);
     const uint64_t base = y * g.xdim + z * g.xdim * g.ydim;
+    // unrolled: several loads of a thread in flight at once (two blocks per SM alone do not
+    // keep enough bytes in flight to stream at the HBM rate)
+#pragma unroll 4
     for (uint32_t xx = g.x0 + threadIdx.x; xx < g.x_lim; xx += kThreads) x[base + xx] += (double)e[base + xx];
   }
 }
