@@ -189,8 +189,10 @@ def exhaustive(st: Stencil, geom: Geometry, x, y, blocks, sweeps: int = 2) -> li
 class CostModel:
     """3-layer perceptron on standardised features, predicting log GLup/s (tcs_mlp_* kernels)."""
 
-    def __init__(self, n_in: int = len(FEATURES), hidden: int = HIDDEN, max_batch: int = 4096,
-                 params: np.ndarray | None = None, seed: int = 0):
+    def __init__(self, n_in: int | None = None, hidden: int = HIDDEN, max_batch: int = 4096,
+                 params: np.ndarray | None = None, seed: int = 0, features: list | None = None):
+        self.features = list(features or FEATURES)
+        n_in = n_in or len(self.features)
         self._lib = _lib.load()
         self.n_in, self.hidden, self.max_batch = n_in, hidden, max_batch
         h = ctypes.c_void_p()
@@ -308,15 +310,16 @@ class CostModel:
         path.parent.mkdir(parents=True, exist_ok=True)
         np.savez_compressed(path, params=self.params(), x_mean=self.x_mean, x_std=self.x_std,
                             y_mean=self.y_mean, y_std=self.y_std, feature_lo=self.feature_lo,
-                            feature_hi=self.feature_hi, hidden=self.hidden, features=np.array(FEATURES),
+                            feature_hi=self.feature_hi, hidden=self.hidden, features=np.array(self.features),
                             meta=json.dumps(meta))
 
     @classmethod
-    def load(cls, path: Path = MODEL_PATH) -> "CostModel":
+    def load(cls, path: Path = MODEL_PATH, features: list | None = None) -> "CostModel":
         d = np.load(path, allow_pickle=False)
-        if list(d["features"]) != FEATURES:
+        names = list(features or FEATURES)
+        if list(d["features"]) != names:
             raise ValueError("cost model was trained on another feature set")
-        m = cls(n_in=len(FEATURES), hidden=int(d["hidden"]), params=d["params"])
+        m = cls(n_in=len(names), hidden=int(d["hidden"]), params=d["params"], features=names)
         m.x_mean, m.x_std = d["x_mean"], d["x_std"]
         m.y_mean, m.y_std = float(d["y_mean"]), float(d["y_std"])
         m.feature_lo, m.feature_hi = d["feature_lo"], d["feature_hi"]
