@@ -19,7 +19,7 @@
 extern "C" {
 #endif
 
-#define TCS_ABI_VERSION 1
+#define TCS_ABI_VERSION 2
 
 /* Status codes. */
 #define TCS_OK 0
@@ -89,7 +89,13 @@ typedef struct tcs_launch {
   unsigned segments;        /* march: CTAs along the march axis per tile column (0 = auto) */
   unsigned depth;           /* march/pipe: chunks in flight ahead of the current step (0 = auto) */
   unsigned chunk;           /* pipe: planes per ring chunk (0 = auto) */
+  unsigned flags;           /* TCS_LAUNCH_* options (0: the planner's choice) */
 } tcs_launch;
+
+/* tcs_launch.flags: the pipelined sweep's middle rows of a Star stencil (Row order, block x extent a
+ * multiple of 32) through warp shuffles, or through shared-memory loads only. */
+#define TCS_LAUNCH_SHUFFLE 1u
+#define TCS_LAUNCH_NO_SHUFFLE 2u
 
 /* Resolved launch of one sweep (what tcs_update_grid will run). */
 typedef struct tcs_plan {
@@ -231,6 +237,10 @@ int tcs_precompile(const tcs_spec* spec, char* cubin_path, unsigned path_cap);
  * 0 = the planner's default). */
 int tcs_precompile_pipe(const tcs_spec* spec, unsigned bx, unsigned by, unsigned chunk,
                         char* cubin_path, unsigned path_cap);
+
+/* Same with launch options (TCS_LAUNCH_* flags). */
+int tcs_precompile_pipe_flags(const tcs_spec* spec, unsigned bx, unsigned by, unsigned chunk, unsigned flags,
+                              char* cubin_path, unsigned path_cap);
 
 /* Same with an epilogue: 1 = the FP64 defect sweep, 2 = the FP32 accumulating sweep. */
 int tcs_precompile_pipe_epilogue(const tcs_spec* spec, unsigned bx, unsigned by, unsigned chunk, unsigned epi,

@@ -35,7 +35,7 @@ def test_library_exports_every_declared_symbol():
 
 
 def test_abi_version():
-    assert _lib.load().tcs_abi_version() == 1
+    assert _lib.load().tcs_abi_version() == 2
 
 
 @pytest.mark.parametrize("bad", [

@@ -24,6 +24,9 @@ VARIANT_DIRECT = 1
 VARIANT_MARCH = 2
 VARIANT_PIPE = 3
 
+LAUNCH_SHUFFLE = 1
+LAUNCH_NO_SHUFFLE = 2
+
 
 class TcsError(RuntimeError):
     """A libtcs call returned a non-zero status."""
@@ -76,6 +79,7 @@ class CLaunch(ctypes.Structure):
         ("segments", ctypes.c_uint),
         ("depth", ctypes.c_uint),
         ("chunk", ctypes.c_uint),
+        ("flags", ctypes.c_uint),
     ]
 
 
@@ -137,6 +141,7 @@ SIGNATURES = {
     "tcs_defect_sweep": [_vp, U3, _u, _P(CLaunch), _vp, _vp, _P(ctypes.c_double), _vp],
     "tcs_update_grid_accumulate": [_vp, U3, _u, _P(CLaunch), _vp, _vp, _vp, _vp],
     "tcs_precompile_pipe_epilogue": [_P(CSpec), _u, _u, _u, _u, ctypes.c_char_p, _u],
+    "tcs_precompile_pipe_flags": [_P(CSpec), _u, _u, _u, _u, ctypes.c_char_p, _u],
     "tcs_sweeps_tb3": [_vp, U3, _u, _P(CLaunch), _vp, _vp, _u, _vp, _P(ctypes.c_int)],
     "tcs_plan_tb3": [_vp, U3, _u, _P(CLaunch), _P(CPlan)],
     "tcs_precompile_tb3": [_P(CSpec), _u, _u, _u, ctypes.c_char_p, _u],

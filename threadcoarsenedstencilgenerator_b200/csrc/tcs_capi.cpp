@@ -218,9 +218,10 @@ struct PipeKey {
   unsigned batch = 0;
   unsigned epi = 0;  // epilogue mode (tcs_kernels.cuh, TCS_EPI): 0 plain, 1 FP64 defect, 2 FP32 accumulate
   unsigned tb3 = 0;  // tcs_tb3 (two sweeps per pass, 3D) with thread tiles tb3 x tb3; 0: tcs_pipe
+  unsigned shfl = 0;  // Star middle rows through warp shuffles (TCS_SHFL)
   bool operator==(const PipeKey& o) const {
     return bx == o.bx && by == o.by && ch == o.ch && lshift == o.lshift && batch == o.batch && epi == o.epi &&
-           tb3 == o.tb3;
+           tb3 == o.tb3 && shfl == o.shfl;
   }
 };
 
@@ -232,6 +233,7 @@ std::string instance_macros(const tcs_spec& s, const PipeKey* pk) {
   if (pk && pk->batch) m << "#define TCS_BATCH 1\n";
   if (pk && pk->epi) m << "#define TCS_EPI " << pk->epi << "\n";
   if (pk && pk->tb3) m << "#define TCS_TB3 1\n";
+  if (pk && pk->shfl) m << "#define TCS_SHFL 1\n";
   // the two-sweep kernel has thread tiles of its own (tb3 x tb3 x 1); the term order of every
   // output does not depend on them
   const int cx = (pk && pk->tb3) ? (int)pk->tb3 : s.cx, cy = (pk && pk->tb3) ? (int)pk->tb3 : s.cy;
@@ -716,7 +718,14 @@ int resolve_pipe(tcs_stencil* h, const TcsGeo& g, const tcs_launch* L, Resolved&
     return fail(TCS_ERR_UNSUPPORTED, "pipe: tile exceeds the 256-element TMA box limit");
   const bool no_tma = W > 256;
   const unsigned chunk_bytes = ch * rows * W * es;
-  PipeKey key{L->block[0], s.dimension == 3 ? L->block[1] : 1u, ch, lshift, batch ? 1u : 0u, epi};
+  // Star middle rows through warp shuffles: on request (TCS_LAUNCH_SHUFFLE), where the block's rows
+  // are whole warps
+  const bool shfl_ok = s.neighbourhood == TCS_STAR && (s.dimension == 2 || s.orientation == TCS_ROW) &&
+                       L->block[0] % 32 == 0;
+  if ((L->flags & TCS_LAUNCH_SHUFFLE) && !shfl_ok)
+    return fail(TCS_ERR_UNSUPPORTED, "pipe: shuffled rows need a Star stencil in Row order and bx % 32 == 0");
+  const unsigned shfl = ((L->flags & TCS_LAUNCH_SHUFFLE) && shfl_ok) ? 1u : 0u;
+  PipeKey key{L->block[0], s.dimension == 3 ? L->block[1] : 1u, ch, lshift, batch ? 1u : 0u, epi, 0u, shfl};
   PipeMod* pm = nullptr;
   int rc = pipe_module(h, key, &pm);
   if (rc) return rc;
@@ -1625,7 +1634,7 @@ int tcs_precompile(const tcs_spec* spec, char* cubin_path, unsigned path_cap) {
 namespace {
 
 int precompile_pipe(const tcs_spec* spec, unsigned bx, unsigned by, unsigned chunk, bool batch,
-                    char* cubin_path, unsigned path_cap, unsigned epi = 0) {
+                    char* cubin_path, unsigned path_cap, unsigned epi = 0, unsigned shfl = 0) {
   int rc = validate(spec);
   if (rc) return rc;
   tcs_spec s = *spec;
@@ -1640,7 +1649,9 @@ int precompile_pipe(const tcs_spec* spec, unsigned bx, unsigned by, unsigned chu
   if (chunk == 0) chunk = pipe_auto_chunk(s, bx, by);
   if (epi > 2 || (epi == 1 && s.precision != TCS_F64) || (epi == 2 && s.precision != TCS_F32) || (epi && batch))
     return fail(TCS_ERR_UNSUPPORTED, "pipe: epilogue not available for this precision");
-  PipeKey key{bx, s.dimension == 3 ? by : 1u, chunk, left_offset_of(s) % vec, batch ? 1u : 0u, epi};
+  if (shfl && !(s.neighbourhood == TCS_STAR && (s.dimension == 2 || s.orientation == TCS_ROW) && bx % 32 == 0))
+    return fail(TCS_ERR_UNSUPPORTED, "pipe: shuffled rows need a Star stencil in Row order and bx % 32 == 0");
+  PipeKey key{bx, s.dimension == 3 ? by : 1u, chunk, left_offset_of(s) % vec, batch ? 1u : 0u, epi, 0u, shfl ? 1u : 0u};
   std::vector<char> cubin;
   std::string path;
   rc = instantiate(s, &key, cubin, &path);
@@ -1706,6 +1717,11 @@ int tcs_precompile_pipe(const tcs_spec* spec, unsigned bx, unsigned by, unsigned
 int tcs_precompile_pipe_epilogue(const tcs_spec* spec, unsigned bx, unsigned by, unsigned chunk, unsigned epi,
                                  char* cubin_path, unsigned path_cap) {
   return precompile_pipe(spec, bx, by, chunk, false, cubin_path, path_cap, epi);
+}
+
+int tcs_precompile_pipe_flags(const tcs_spec* spec, unsigned bx, unsigned by, unsigned chunk, unsigned flags,
+                              char* cubin_path, unsigned path_cap) {
+  return precompile_pipe(spec, bx, by, chunk, false, cubin_path, path_cap, 0, (flags & TCS_LAUNCH_SHUFFLE) ? 1u : 0u);
 }
 
 int tcs_precompile_batch(const tcs_spec* spec, unsigned bx, unsigned by, unsigned chunk,

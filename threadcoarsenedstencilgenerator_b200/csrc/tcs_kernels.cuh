@@ -524,6 +524,8 @@ constexpr int CHUNK = CHP * PLANE;   // elements per ring slot
 constexpr int NP2 = 2 * R + 1;       // pipeline depth (output planes in flight)
 static_assert(!(DIM == 2 && ORIENT == 1), "2D Column orientation is not pipelined");
 static_assert(!COMP || PAIRS, "compensated pipelined sweeps take the packed Box path only");
+static_assert(!TCS_SHFL || (BX % 32 == 0 && SHAPE == 1 && (DIM == 2 || ORIENT == 0)),
+              "shuffled rows: Star stencils in Row order, block x extent a multiple of the warp");
 static_assert(CHP >= 1, "planes per chunk");
 static_assert(TXP % VEC == 0, "tile width must be a multiple of the 16-byte granule");
 // Columns whose element index is even for every thread: the thread origin sits at ring column

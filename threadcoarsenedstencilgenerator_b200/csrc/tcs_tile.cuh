@@ -474,6 +474,48 @@ __device__ __forceinline__ void load_row(const LD& ld, T (&v)[N]) {
   });
 }
 
+// Middle rows of a Star stencil by warp shuffles (pipelined sweep instances built with TCS_SHFL,
+// blocks whose x extent is a multiple of 32, so a warp is 32 consecutive thread tiles of one row):
+// every lane loads only its own CX values from shared memory; the R-wide halos on either side are
+// the own values of the neighbouring lanes, passed with __shfl_up/down_sync, and only the lanes at
+// the warp's edges, whose neighbours are outside the warp, read them from shared memory.  Same
+// values as load_row<GY, -R, 2R + CX>, less shared-memory traffic.
+#ifndef TCS_SHFL
+#define TCS_SHFL 0
+#endif
+template <int GY, class LD>
+__device__ __forceinline__ void load_row_shfl(const LD& ld, T (&v)[2 * R + CX]) {
+#if TCS_SHFL
+  T own[CX];
+  load_row<GY, 0, CX>(ld, own);
+  static_for<0, CX>([&](auto ex) { v[R + decltype(ex)::value] = own[decltype(ex)::value]; });
+  const int lane = (int)(threadIdx.x & 31u);
+  constexpr int J = (R + CX - 1) / CX;  // neighbour lanes per side that hold halo values
+  static_for<1, J + 1>([&](auto jj) {
+    constexpr int j = decltype(jj)::value;
+    T l[CX], r[CX];
+    static_for<0, CX>([&](auto ex) {
+      l[decltype(ex)::value] = __shfl_up_sync(0xffffffffu, own[decltype(ex)::value], j);
+      r[decltype(ex)::value] = __shfl_down_sync(0xffffffffu, own[decltype(ex)::value], j);
+    });
+    static_for<0, CX>([&](auto ex) {
+      constexpr int gl = -j * CX + decltype(ex)::value;  // column of l[ex] relative to the thread
+      constexpr int gr = j * CX + decltype(ex)::value;   // column of r[ex]
+      if constexpr (gl >= -R) {
+        if (lane < j) l[decltype(ex)::value] = ld.template one<gl, GY>();
+        v[gl + R] = l[decltype(ex)::value];
+      }
+      if constexpr (gr < CX + R) {
+        if (lane >= 32 - j) r[decltype(ex)::value] = ld.template one<gr, GY>();
+        v[gr + R] = r[decltype(ex)::value];
+      }
+    });
+  });
+#else
+  load_row<GY, -R, 2 * R + CX>(ld, v);
+#endif
+}
+
 // Apply input plane (offset DZ relative to pending outputs) held in shared memory to the 2R+1
 // pipeline slots.  `ld` reads the plane at in-plane offsets from the thread origin (see load_row);
 // `slot(ic<k>)` returns the accumulators of the output at march-axis offset k - R.
@@ -581,7 +623,7 @@ __device__ __forceinline__ void pipe_plane(const LD& ld, SLOTS&& slot) {
       static_for<0, NY>([&](auto gyc) {  // middle rows: gx in [-R, R + CX)
         constexpr int gy = decltype(gyc)::value;
         T row[2 * R + CX];
-        load_row<gy, -R, 2 * R + CX>(ld, row);
+        load_row_shfl<gy>(ld, row);
         static_for<0, CX>([&](auto ex) { cv[decltype(ex)::value + gy * CX] = row[R + decltype(ex)::value]; });
         static_for<0, 2 * R + CX>([&](auto ix) {
           apply_slot<decltype(ix)::value - R, gy, 0>(s0, row[decltype(ix)::value]);

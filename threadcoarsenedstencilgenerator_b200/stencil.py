@@ -42,6 +42,7 @@ class Launch:
     segments: int = 0               # march: CTAs along the march axis per tile column (0 = auto)
     depth: int = 0                  # march/pipe: chunks in flight (0 = auto)
     chunk: int = 0                  # pipe: planes per ring chunk (0 = auto)
+    shuffle: bool | None = None     # pipe, Star: middle rows through warp shuffles (None: planner's choice)
 
     _VARIANTS = {"auto": _lib.VARIANT_AUTO, "direct": _lib.VARIANT_DIRECT, "march": _lib.VARIANT_MARCH,
                  "pipe": _lib.VARIANT_PIPE}
@@ -49,8 +50,9 @@ class Launch:
     def to_c(self) -> _lib.CLaunch:
         b = tuple(self.block) + (1,) * (3 - len(self.block))
         g = tuple(self.grid_blocks) + (0,) * (3 - len(self.grid_blocks))
+        flags = 0 if self.shuffle is None else (_lib.LAUNCH_SHUFFLE if self.shuffle else _lib.LAUNCH_NO_SHUFFLE)
         return _lib.CLaunch(_lib.U3(*b), _lib.U3(*g), self._VARIANTS[self.variant], int(self.segments),
-                            int(self.depth), int(self.chunk))
+                            int(self.depth), int(self.chunk), flags)
 
 
 @dataclass
@@ -309,11 +311,15 @@ def precompile(spec: StencilSpec) -> str:
     return buf.value.decode()
 
 
-def precompile_pipe(spec: StencilSpec, block, chunk: int) -> str:
+def precompile_pipe(spec: StencilSpec, block, chunk: int, shuffle: bool = False) -> str:
     """Instantiate the pipelined sweep of ``spec`` for one launch shape into the cubin cache."""
     buf = ctypes.create_string_buffer(1024)
     b = tuple(block) + (1,) * (3 - len(block))
-    _lib.check(_lib.load().tcs_precompile_pipe(ctypes.byref(spec.to_c()), b[0], b[1], int(chunk), buf, 1024))
+    if shuffle:
+        _lib.check(_lib.load().tcs_precompile_pipe_flags(ctypes.byref(spec.to_c()), b[0], b[1], int(chunk),
+                                                         _lib.LAUNCH_SHUFFLE, buf, 1024))
+    else:
+        _lib.check(_lib.load().tcs_precompile_pipe(ctypes.byref(spec.to_c()), b[0], b[1], int(chunk), buf, 1024))
     return buf.value.decode()
 
 
