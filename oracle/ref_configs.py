@@ -57,6 +57,7 @@ BENCH = [
     (3, "Star", "Row", "Variable", 4, 2, 2, 2, "Read", 16),
     (3, "Star", "Row", "Variable", 4, 4, 2, 1, "Read", 16),
     (3, "Star", "Row", "Variable", 4, 1, 4, 2, "Read", 16),
+    (3, "Star", "Row", "Variable", 4, 3, 4, 3, "Read", 16),  # best of the launch-shape sweep (ref_sweep.py)
     (2, "Box", "Row", "Variable", 6, 1, 1, 1, "None", 0),
     (2, "Box", "Row", "Variable", 6, 2, 2, 1, "None", 0),
     (2, "Box", "Row", "Variable", 6, 4, 4, 1, "None", 0),

@@ -27,7 +27,8 @@ SINGLE = {
         "stencil": (3, "Star", "Row", "Variable", 4, 1, 2, 2, "Read", 16),
         "grid": (512, 512, 512), "sweeps": 50, "value_range": (0.0, 1.0), "mask_kind": "normal_sum1", "seed": 2024,
         "launch": {"block": (32, 8, 1), "variant": "march"},
-        "reference": ((1, 4, 2), (128, 2, 1)),
+        # the reference kernel's best shape over 64 coarsening triples x 46 blocks (oracle/ref_sweep.py)
+        "reference": ((3, 4, 3), (32, 2, 2)),
     },
     # 2D Box Variable r6 (169-point), FP64, 16384x8192, mask N(0,1)/169, values U[-1,1], 200 sweeps
     "2d_box_var_r6_16384x8192": {
