@@ -601,6 +601,7 @@ struct PipeGridView {
   bool cp_pair;  // cp.async loader moves two elements per copy (FP32, even pitch, 8-byte base)
   bool st_pair;  // output pairs stored with one access (even pitch, pair-aligned base)
   void* aux;     // epilogues 1 and 2: the float defect array / the double state (same layout)
+  bool src_pair;  // source pairs read with one access (the store's rule for the source's base)
 };
 
 // cp.async fill of one ring chunk: CHP planes of ROWS rows (3D) or CHP rows (2D), PW elements
@@ -812,8 +813,14 @@ __device__ __forceinline__ bool pipe_piece(const PipeGridView& G, tcs_u32 tile, 
                 T v0 = (COEFF == 0) ? slot_value<e>(done) * c : slot_value<e>(done);
                 T v1 = (COEFF == 0) ? slot_value<e + 1>(done) * c : slot_value<e + 1>(done);
                 if (so) {
-                  v0 = v0 + so[0];
-                  v1 = v1 + so[1];
+                  if (G.src_pair) {  // the source pair in one access, like the store
+                    const typename PairOf<T>::type s2 = *reinterpret_cast<const typename PairOf<T>::type*>(so);
+                    v0 = v0 + s2.x;
+                    v1 = v1 + s2.y;
+                  } else {
+                    v0 = v0 + so[0];
+                    v1 = v1 + so[1];
+                  }
                 }
                 if (G.st_pair) {
                   typename PairOf<T>::type v2;
@@ -900,6 +907,7 @@ extern "C" __global__ void __launch_bounds__(TCS_BX * ((TCS_DIM == 3) ? TCS_BY :
   // Output pairs are stored with one access only when every row keeps the parity of the first:
   // an even row pitch and a pair-aligned base address.
   G.st_pair = (g.xdim % 2 == 0) && (reinterpret_cast<tcs_u64>(out) % (2 * sizeof(T)) == 0);
+  G.src_pair = G.st_pair && (reinterpret_cast<tcs_u64>(src) % (2 * sizeof(T)) == 0);
   if (G.use_tma && threadIdx.x == 0 && threadIdx.y == 0) tma_prefetch_map(&tmap);
   PipeState st = pipe_setup(g.nslot, G.use_tma);
   PipeSlot acc[NP2];
@@ -987,6 +995,7 @@ extern "C" __global__ void __launch_bounds__(TCS_BX * ((TCS_DIM == 3) ? TCS_BY :
     G.use_tma = (B.loader == 0);
     G.cp_pair = (B.loader == 2);
     G.st_pair = (B.xdim % 2 == 0) && (reinterpret_cast<tcs_u64>(B.out) % (2 * sizeof(T)) == 0);
+    G.src_pair = G.st_pair && (reinterpret_cast<tcs_u64>(B.src) % (2 * sizeof(T)) == 0);
     G.aux = nullptr;
     const tcs_u64 local = w - B.first;
     const tcs_u32 tile = (tcs_u32)(local / B.m);
@@ -1197,6 +1206,7 @@ extern "C" __global__ void __launch_bounds__(TCS_BX * TCS_BY)
   G.use_tma = (g.loader == 0);
   G.cp_pair = false;
   G.st_pair = false;
+  G.src_pair = false;
   G.aux = nullptr;
   if (G.use_tma && threadIdx.x == 0 && threadIdx.y == 0) tma_prefetch_map(&tmap);
   PipeState st = pipe_setup(g.nslot, G.use_tma);
