@@ -43,9 +43,13 @@ extern "C" {
 #define TCS_ALIGN_WRITE 2
 #define TCS_F64 0 /* the reference's arithmetic (double) */
 #define TCS_F32 1 /* single-precision grids */
-#define TCS_F32C 2 /* single-precision grids, compensated accumulation: every output also sums the
-                      rounding errors of its additions (two-sum) and products (fma(v,m,-v*m)) in the
-                      reference's term order and adds them at the end (direct and march kernels) */
+#define TCS_F32C 2 /* single-precision grids, compensated accumulation in the reference's term order.
+                      Direct and march kernels: every output also sums the rounding errors of its
+                      additions (two-sum) and products (fma(v,m,-v*m)) and adds them at the end;
+                      |error| <= 3u|exact| + 4Su^2 sum|m||x| (u = 2^-24).  Pipelined kernel (Box,
+                      Row order, even x coarsening): each footprint row's 2R+1 terms are summed with
+                      plain FMAs and the row partials combined with two-sum;
+                      |error| <= 3u|exact| + (2R+2)u sum|m||x|. */
 
 /* Kernel variants. */
 #define TCS_VARIANT_AUTO 0   /* pipe, else march, else direct: the first that supports the shape */
