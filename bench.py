@@ -987,6 +987,8 @@ def run_case(args) -> dict:
     w = WORKLOADS[args.workload]
     spec = w.tuned_spec(args.case_precision).replace(precision=args.case_precision)
     launch = w.tuned_launch(args.case_precision)
+    if args.case_launch:
+        spec, launch = case_launch(spec, args.case_launch)
     grid = tuple(args.grid) + (1,) * (3 - len(args.grid))
     geom = spec.geometry(*grid)
     st = tcs.Stencil(spec)
@@ -1010,7 +1012,21 @@ def run_case(args) -> dict:
         raise RuntimeError("device status word set")
     plan = st.plan(geom, launch)
     return {"case": args.workload, "grid": list(grid), "points": geom.interior_points, "sweeps": args.steps,
-            "kernel": args.case, "variant": plan.variant, "block": list(plan.block), "chunk": plan.chunk}
+            "kernel": args.case, "variant": plan.variant, "block": list(plan.block), "chunk": plan.chunk,
+            "coarsening": [spec.cx, spec.cy, spec.cz], "shuffle": bool(launch.shuffle)}
+
+
+def case_launch(spec, text: str):
+    """(spec, Launch) of a pipelined launch written cx,cy,bx,by,chunk[,shuffle]: the profiling case
+    of one point of the launch space instead of the tuned launch."""
+    from threadcoarsenedstencilgenerator_b200.stencil import Launch
+
+    v = [int(t) for t in text.split(",")]
+    if len(v) not in (5, 6):
+        raise SystemExit("--case-launch wants cx,cy,bx,by,chunk[,shuffle]")
+    cx, cy, bx, by, ch = v[:5]
+    spec = spec.replace(cx=cx, cy=cy, cz=1) if spec.dimension == 3 else spec.replace(cx=cx, cy=1)
+    return spec, Launch(block=(bx, by, 1), variant="pipe", chunk=ch, shuffle=bool(v[5]) if len(v) == 6 else False)
 
 
 def check_world(gpus: int, world: int) -> str | None:
@@ -1046,6 +1062,8 @@ def main(argv=None) -> int:
     ap.add_argument("--case", default="sweep", choices=["sweep", "tensor-cores", "temporal"],
                     help="profiling case: which kernel")
     ap.add_argument("--case-precision", default="f64", choices=["f64", "f32"], help="profiling case: precision")
+    ap.add_argument("--case-launch", default="", help="profiling case: pipelined launch cx,cy,bx,by,chunk[,shuffle] "
+                    "instead of the tuned one")
     args = ap.parse_args(argv)
     args.warmup = max(3, args.warmup)
     err = check_world(args.gpus, _dist()[0])

@@ -82,3 +82,28 @@ def test_tuner_times_top_k_or_falls_back(monkeypatch, scenario):
     else:
         assert r.fell_back and len(timed) == 5 * (scenario == "disagrees") + len(cands)
         assert r.candidate == max(timings, key=timings.get)
+
+
+def test_write_tuned_records_a_launch_the_workload_reads(tmp_path, monkeypatch):
+    """The tuner's record is the tuned-launch format: the workload turns it back into the same
+    coarsening, block and chunk; other entries of the file survive."""
+    from threadcoarsenedstencilgenerator_b200 import workloads as W
+
+    path = tmp_path / "tuned.json"
+    path.write_text('{"other": {"block": [8, 8, 1]}}\n')
+    r = P.PipeTuneResult((2, 2, 64, 8, 3), 270.0, 140, 148, True, 1.0, "no model",
+                         {(2, 2, 64, 8, 3): 270.0, (2, 4, 64, 4, 3): 269.6})
+    e = P.write_tuned(path, "3d_star_var_r4_512", "f64", r)
+    assert "269.6" in e["source"] and "exhaustive" in e["source"]
+    P.write_tuned(path, "3d_star_var_r4_512", "f32",
+                  P.PipeTuneResult((1, 4, 128, 4, 2), 400.0, 5, 148, False, 0.1, "model top-5", {}))
+    monkeypatch.setattr(W, "TUNED_PATH", path)
+    w = W.WORKLOADS["3d_star_var_r4_512"]
+    L, s = w.tuned_launch(), w.tuned_spec()
+    assert (L.variant, tuple(L.block), L.chunk) == ("pipe", (64, 8, 1), 3)
+    assert (s.cx, s.cy, s.cz) == (2, 2, 1)
+    L32, s32 = w.tuned_launch("f32"), w.tuned_spec("f32")
+    assert (tuple(L32.block), L32.chunk, s32.cx, s32.cy) == ((128, 4, 1), 2, 1, 4)
+    import json
+
+    assert json.loads(path.read_text())["other"] == {"block": [8, 8, 1]}

@@ -15,6 +15,9 @@ to the exhaustive search when the model is missing, the problem lies outside the
 ranges, or the timed candidates disagree with the predicted ordering by more than a tolerance.
 
     python -m threadcoarsenedstencilgenerator_b200.pipetune precompile|corpus|train|evaluate|tune
+
+``tune --workload NAME [--precision f32] --exhaustive --write`` records the chosen launch in the
+package's tuned.json, the file the benchmark workloads read their launches from.
 """
 
 from __future__ import annotations
@@ -37,6 +40,7 @@ from .stencil import Launch, Stencil
 DATA = Path(__file__).resolve().parent / "data"
 PIPE_CORPUS_PATH = DATA / "pipe_corpus.npz"
 PIPE_MODEL_PATH = DATA / "pipe_costmodel.npz"
+TUNED_PATH = Path(__file__).resolve().parent / "tuned.json"
 GRID_BYTES = 256 << 20  # one buffer of a corpus grid (two buffers: ~0.5 GB)
 
 PIPE_FEATURES = [
@@ -332,6 +336,28 @@ def workload_base(w, precision: str = "f64") -> StencilSpec:
     return w.spec.replace(precision=precision, cx=1, cy=1, cz=1)
 
 
+def tuned_entry(r: PipeTuneResult) -> dict:
+    """A tuned-launch record (the format workloads.py reads) of a tuning result."""
+    cx, cy, bx, by, ch = r.candidate
+    runner_up = sorted(((v, k) for k, v in r.measured.items() if k != r.candidate), reverse=True)[:1]
+    how = "exhaustive" if r.fell_back else "learned (%s)" % r.reason
+    src = "pipetune %s over %d of %d pipelined launches: %.1f GLup/s" % (how, r.timed, r.candidates, r.glups)
+    if runner_up:
+        src += "; next %s: %.1f" % ("x".join(map(str, runner_up[0][1])), runner_up[0][0])
+    return {"coarsening": [cx, cy, 1], "block": [bx, by, 1], "variant": "pipe", "chunk": ch, "source": src}
+
+
+def write_tuned(path: Path, name: str, precision: str, r: PipeTuneResult) -> dict:
+    """Record a workload's tuned pipelined launch under ``name`` (FP64) or ``name_precision``,
+    keeping the file's other entries."""
+    d = json.loads(path.read_text()) if path.exists() else {}
+    k = name if precision == "f64" else name + "_" + precision
+    d[k] = tuned_entry(r)
+    path.parent.mkdir(parents=True, exist_ok=True)
+    path.write_text(json.dumps(d, indent=1) + "\n")
+    return d[k]
+
+
 def _name(s: StencilSpec) -> str:
     return "%dD %s %s r%d %s" % (s.dimension, s.neighbourhood, s.coefficients, s.range, s.precision)
 
@@ -346,6 +372,17 @@ def holdout_ids(n_problems: int, n_holdout: int = 8, seed: int = 3) -> list:
     """Seeded held-out problem ids (never trained on)."""
     rng = np.random.default_rng(seed)
     return sorted(rng.choice(n_problems, size=min(n_holdout, n_problems // 4), replace=False).tolist())
+
+
+def live_check_problem(n_problems: int = 40) -> int:
+    """The held-out problem a quick live check tunes: the first 3D FP64 Jacobi one (its 148
+    instantiations compile fastest of the 3D spaces)."""
+    problems = sample_problems(n_problems)
+    for pid in holdout_ids(n_problems):
+        b = problems[pid]
+        if b.dimension == 3 and b.precision == "f64" and b.coefficients == "Jacobi":
+            return pid
+    return holdout_ids(n_problems)[0]
 
 
 def split(pids: np.ndarray, n_problems: int):
@@ -417,6 +454,8 @@ def main(argv=None) -> int:
     t.add_argument("--workload", required=True)
     t.add_argument("--precision", default="f64")
     t.add_argument("--exhaustive", action="store_true")
+    t.add_argument("--write", type=Path, nargs="?", const=TUNED_PATH, default=None,
+                   help="record the chosen launch in a tuned-launch file (default: the package's tuned.json)")
     a = ap.parse_args(argv)
     if a.cmd == "precompile":
         import multiprocessing as mp
@@ -452,6 +491,8 @@ def main(argv=None) -> int:
                           "candidates": r.candidates, "fell_back": r.fell_back, "seconds": r.seconds,
                           "reason": r.reason, "top": sorted(([list(k), v] for k, v in r.measured.items()),
                                                             key=lambda q: -q[1])[:10]}))
+        if a.write is not None:
+            write_tuned(a.write, w.name, a.precision, r)
         return 0
     pids, X, y = load_corpus()
     hold, train_mask = split(pids, int(np.load(PIPE_CORPUS_PATH)["n_problems"]))
