@@ -234,6 +234,12 @@ std::string instance_macros(const tcs_spec& s, const PipeKey* pk) {
   if (pk && pk->epi) m << "#define TCS_EPI " << pk->epi << "\n";
   if (pk && pk->tb3) m << "#define TCS_TB3 1\n";
   if (pk && pk->shfl) m << "#define TCS_SHFL 1\n";
+  // TCS_PIPE_CYCLE=0 in the environment builds the pipelined kernels with a one-chunk loop body
+  // (register slots rotated at the back-edge) instead of one whole slot cycle per iteration
+  if (pk) {
+    const char* cyc = std::getenv("TCS_PIPE_CYCLE");
+    if (cyc && std::string(cyc) == "0") m << "#define TCS_CYCLE 0\n";
+  }
   // the two-sweep kernel has thread tiles of its own (tb3 x tb3 x 1); the term order of every
   // output does not depend on them
   const int cx = (pk && pk->tb3) ? (int)pk->tb3 : s.cx, cy = (pk && pk->tb3) ? (int)pk->tb3 : s.cy;

@@ -528,6 +528,9 @@ extern "C" __global__ void tcs_init(T* __restrict__ a, const tcs_u64 xdim, const
 // still accumulates in exactly the reference order) and completes output p-R.  Each input element
 // is read from HBM once and from shared memory once per thread that needs it; with the plane loop
 // unrolled by 2R+1 every register slot and every shared-memory offset is a compile-time constant.
+#ifndef TCS_CYCLE
+#define TCS_CYCLE 1
+#endif
 #ifndef TCS_EPI
 #define TCS_EPI 0
 #endif
@@ -751,144 +754,158 @@ __device__ __forceinline__ bool pipe_piece(const PipeGridView& G, tcs_u32 tile, 
   const tcs_i64 plane_g = (tcs_i64)G.xdim;
   T* obase = G.out + (tcs_u64)x;
 #endif
-  // One loop iteration consumes one ring chunk: wait for it (bounded), release the slot of the
+  // One chunk step consumes one ring chunk: wait for it (bounded), release the slot of the
   // previous chunk to the next copy, then run its CHP planes as straight-line code.  The slot
   // cursor advances by additions only.  Output pi - 2R is complete after input plane pi.
+  // Register slot of output plane p: (p - first) mod 2R+1.  When CHP divides 2R+1 the loop runs
+  // U = (2R+1)/CHP chunk steps per iteration, a whole cycle of slots, so every slot index stays a
+  // compile-time constant without moving registers at the back-edge; otherwise one step per
+  // iteration and the slots rotate by CHP at the back-edge.  The cycle is unrolled only while its
+  // straight-line code stays near the size of a one-step body (about 2400 terms).
+  constexpr int U = (NP2 % CHP == 0 && TCS_CYCLE != 0 && NP2 * S * NEP <= 2400) ? NP2 / CHP : 1;
   tcs_u32 cur_slot = gc % nslot;
   tcs_u32 cur_par = (gc / nslot) & 1u;
   T* optr = obase + ((tcs_i64)ms - 2 * R) * plane_g;
   // A return from inside this loop costs registers across the whole body: leave it by break.
   bool aborted = false;
-  for (tcs_u32 j = 0; j < nch; ++j) {
-    const bool expired = mbar_wait_bounded(bars + 8u * cur_slot, cur_par, TCS_WAIT_LIMIT);
-    if (__syncthreads_or(expired)) {
-      if (use_tma) {
-        if (tid == 0) {
-          atomicOr(&tcs_status, TCS_DEV_TIMEOUT);
-          const tcs_u32 hi = min(j + nslot - 2, nch - 1);
-          for (tcs_u32 jj = j; jj <= hi; ++jj)
-            (void)mbar_wait_bounded(bars + 8u * ((gc + jj) % nslot), ((gc + jj) / nslot) & 1u,
-                                    TCS_WAIT_LIMIT);
+  for (tcs_u32 j0 = 0; j0 < nch; j0 += U) {
+    static_for<0, U>([&](auto uu) {
+      constexpr int u = decltype(uu)::value;
+      const tcs_u32 j = j0 + u;
+      if (aborted || j >= nch) return;
+      const bool expired = mbar_wait_bounded(bars + 8u * cur_slot, cur_par, TCS_WAIT_LIMIT);
+      if (__syncthreads_or(expired)) {
+        if (use_tma) {
+          if (tid == 0) {
+            atomicOr(&tcs_status, TCS_DEV_TIMEOUT);
+            const tcs_u32 hi = min(j + nslot - 2, nch - 1);
+            for (tcs_u32 jj = j; jj <= hi; ++jj)
+              (void)mbar_wait_bounded(bars + 8u * ((gc + jj) % nslot), ((gc + jj) / nslot) & 1u,
+                                      TCS_WAIT_LIMIT);
+          }
+        } else {
+          if (tid == 0) atomicOr(&tcs_status, TCS_DEV_TIMEOUT);
+          cp_async_wait_all();
         }
-      } else {
-        if (tid == 0) atomicOr(&tcs_status, TCS_DEV_TIMEOUT);
-        cp_async_wait_all();
+        aborted = true;
+        return;
       }
-      aborted = true;
-      break;
-    }
-    if (j + nslot - 1 < nch) {
-      if (!use_tma || MIXED)
-        issue(j + nslot - 1);
-      else if (tid == 0)
-        issue(j + nslot - 1);
-    }
-    const T* pc = st.ring + cur_slot * CHUNK + lane_off;
-    const tcs_u32 pbase = j * CHP;  // input plane index (within the piece) of the chunk's first
-    static_for<0, CHP>([&](auto tt) {
-      constexpr int t = decltype(tt)::value;
-      const tcs_u32 pi = pbase + t;
-      if (pi < np) {
-        // A source term is read from global memory when its output row is stored: fetch the rows
-        // of the output completed PF planes later into L1 now, so that the store does not wait
-        // for the latency of DRAM or L2.
-        constexpr int PF = 2;
-        if (G.src && lane_ok) {
-          const int opf = (int)pi - 2 * R + PF;
-          if (opf >= 0 && opf < (int)nout) {
-            const T* sp = G.src + ((optr - G.out) + (tcs_i64)(t + PF) * plane_g);
+      if (j + nslot - 1 < nch) {
+        if (!use_tma || MIXED)
+          issue(j + nslot - 1);
+        else if (tid == 0)
+          issue(j + nslot - 1);
+      }
+      const T* pc = st.ring + cur_slot * CHUNK + lane_off;
+      const tcs_u32 pbase = j * CHP;  // input plane index (within the piece) of the chunk's first
+      static_for<0, CHP>([&](auto tt) {
+        constexpr int t = decltype(tt)::value;
+        constexpr int tc = u * CHP + t;  // position of the plane in the slot cycle
+        const tcs_u32 pi = pbase + t;
+        if (pi < np) {
+          // A source term is read from global memory when its output row is stored: fetch the rows
+          // of the output completed PF planes later into L1 now, so that the store does not wait
+          // for the latency of DRAM or L2.
+          constexpr int PF = 2;
+          if (G.src && lane_ok) {
+            const int opf = (int)pi - 2 * R + PF;
+            if (opf >= 0 && opf < (int)nout) {
+              const T* sp = G.src + ((optr - G.out) + (tcs_i64)(t + PF) * plane_g);
+              static_for<0, (DIM == 3) ? CY : 1>([&](auto ey) {
+                const T* q = sp + decltype(ey)::value * (tcs_i64)G.xdim;
+                asm volatile("prefetch.global.L1 [%0];" ::"l"(q));
+                if constexpr (CX * sizeof(T) > 16) asm volatile("prefetch.global.L1 [%0];" ::"l"(q + CX - 1));
+              });
+            }
+          }
+          const PipeRing ld{pc + t * PLANE};
+          auto slot = [&](auto kk) -> PipeSlot& {
+            constexpr int k = decltype(kk)::value;
+            return acc[((tc - k) % NP2 + NP2) % NP2];
+          };
+          pipe_plane(ld, slot);
+          const int op = (int)pi - 2 * R;
+          if (EPI != 0 && lane_ok && op >= 0 && op < (int)nout) {
+            constexpr T c = T(1) / T(S);
+            PipeSlot& done = acc[((tc - 2 * R) % NP2 + NP2) % NP2];
+            const tcs_i64 rowoff = (optr - G.out) + (tcs_i64)t * plane_g;
             static_for<0, (DIM == 3) ? CY : 1>([&](auto ey) {
-              const T* q = sp + decltype(ey)::value * (tcs_i64)G.xdim;
-              asm volatile("prefetch.global.L1 [%0];" ::"l"(q));
-              if constexpr (CX * sizeof(T) > 16) asm volatile("prefetch.global.L1 [%0];" ::"l"(q + CX - 1));
+              static_for<0, CX>([&](auto ex) {
+                constexpr int e = decltype(ex)::value + decltype(ey)::value * CX;
+                const tcs_i64 off = rowoff + decltype(ex)::value + decltype(ey)::value * (tcs_i64)G.xdim;
+                T v = (COEFF == 0) ? slot_value<e>(done) * c : slot_value<e>(done);
+                if constexpr (EPI == 1) {
+                  const double d = (double)v - (double)G.src[off];
+                  static_cast<float*>(G.aux)[off] = (float)d;
+                  st.nmax = fmax(st.nmax, fabs(d));
+                  st.nsum = fma(d, d, st.nsum);
+                } else {
+                  if (G.src) v = v + G.src[off];
+                  double* xg = static_cast<double*>(G.aux);
+                  xg[off] = xg[off] + (double)v;
+                }
+              });
+            });
+          }
+          if (EPI == 0 && lane_ok && op >= 0 && op < (int)nout) {
+            constexpr T c = T(1) / T(S);
+            PipeSlot& done = acc[((tc - 2 * R) % NP2 + NP2) % NP2];
+            T* orow = optr + (tcs_i64)t * plane_g;
+            // Output x is R + leftOff + an even offset when CX is even: pairs are aligned when
+            // R + LSHIFT is even (the shared-memory pair rule at gx = 0).
+            static_for<0, (DIM == 3) ? CY : 1>([&](auto ey) {
+              static_for<0, CX>([&](auto ex) {
+                constexpr int e = decltype(ex)::value + decltype(ey)::value * CX;
+                constexpr bool pair = pipe_pair_aligned(0) && (decltype(ex)::value % 2 == 0);
+                constexpr bool tail = pipe_pair_aligned(0) && (decltype(ex)::value % 2 == 1);
+                T* o = orow + decltype(ex)::value + decltype(ey)::value * (tcs_i64)G.xdim;
+                const T* so = G.src ? G.src + (o - G.out) : nullptr;
+                if constexpr (pair) {
+                  T v0 = (COEFF == 0) ? slot_value<e>(done) * c : slot_value<e>(done);
+                  T v1 = (COEFF == 0) ? slot_value<e + 1>(done) * c : slot_value<e + 1>(done);
+                  if (so) {
+                    if (G.src_pair) {  // the source pair in one access, like the store
+                      const typename PairOf<T>::type s2 = *reinterpret_cast<const typename PairOf<T>::type*>(so);
+                      v0 = v0 + s2.x;
+                      v1 = v1 + s2.y;
+                    } else {
+                      v0 = v0 + so[0];
+                      v1 = v1 + so[1];
+                    }
+                  }
+                  if (G.st_pair) {
+                    typename PairOf<T>::type v2;
+                    v2.x = v0;
+                    v2.y = v1;
+                    *reinterpret_cast<typename PairOf<T>::type*>(o) = v2;
+                  } else {
+                    o[0] = v0;
+                    o[1] = v1;
+                  }
+                } else if constexpr (!tail) {
+                  T v = (COEFF == 0) ? slot_value<e>(done) * c : slot_value<e>(done);
+                  if (so) v = v + so[0];
+                  *o = v;
+                }
+              });
             });
           }
         }
-        const PipeRing ld{pc + t * PLANE};
-        auto slot = [&](auto kk) -> PipeSlot& {
-          constexpr int k = decltype(kk)::value;
-          return acc[((t - k) % NP2 + NP2) % NP2];
-        };
-        pipe_plane(ld, slot);
-        const int op = (int)pi - 2 * R;
-        if (EPI != 0 && lane_ok && op >= 0 && op < (int)nout) {
-          constexpr T c = T(1) / T(S);
-          PipeSlot& done = acc[((t - 2 * R) % NP2 + NP2) % NP2];
-          const tcs_i64 rowoff = (optr - G.out) + (tcs_i64)t * plane_g;
-          static_for<0, (DIM == 3) ? CY : 1>([&](auto ey) {
-            static_for<0, CX>([&](auto ex) {
-              constexpr int e = decltype(ex)::value + decltype(ey)::value * CX;
-              const tcs_i64 off = rowoff + decltype(ex)::value + decltype(ey)::value * (tcs_i64)G.xdim;
-              T v = (COEFF == 0) ? slot_value<e>(done) * c : slot_value<e>(done);
-              if constexpr (EPI == 1) {
-                const double d = (double)v - (double)G.src[off];
-                static_cast<float*>(G.aux)[off] = (float)d;
-                st.nmax = fmax(st.nmax, fabs(d));
-                st.nsum = fma(d, d, st.nsum);
-              } else {
-                if (G.src) v = v + G.src[off];
-                double* xg = static_cast<double*>(G.aux);
-                xg[off] = xg[off] + (double)v;
-              }
-            });
-          });
-        }
-        if (EPI == 0 && lane_ok && op >= 0 && op < (int)nout) {
-          constexpr T c = T(1) / T(S);
-          PipeSlot& done = acc[((t - 2 * R) % NP2 + NP2) % NP2];
-          T* orow = optr + (tcs_i64)t * plane_g;
-          // Output x is R + leftOff + an even offset when CX is even: pairs are aligned when
-          // R + LSHIFT is even (the shared-memory pair rule at gx = 0).
-          static_for<0, (DIM == 3) ? CY : 1>([&](auto ey) {
-            static_for<0, CX>([&](auto ex) {
-              constexpr int e = decltype(ex)::value + decltype(ey)::value * CX;
-              constexpr bool pair = pipe_pair_aligned(0) && (decltype(ex)::value % 2 == 0);
-              constexpr bool tail = pipe_pair_aligned(0) && (decltype(ex)::value % 2 == 1);
-              T* o = orow + decltype(ex)::value + decltype(ey)::value * (tcs_i64)G.xdim;
-              const T* so = G.src ? G.src + (o - G.out) : nullptr;
-              if constexpr (pair) {
-                T v0 = (COEFF == 0) ? slot_value<e>(done) * c : slot_value<e>(done);
-                T v1 = (COEFF == 0) ? slot_value<e + 1>(done) * c : slot_value<e + 1>(done);
-                if (so) {
-                  if (G.src_pair) {  // the source pair in one access, like the store
-                    const typename PairOf<T>::type s2 = *reinterpret_cast<const typename PairOf<T>::type*>(so);
-                    v0 = v0 + s2.x;
-                    v1 = v1 + s2.y;
-                  } else {
-                    v0 = v0 + so[0];
-                    v1 = v1 + so[1];
-                  }
-                }
-                if (G.st_pair) {
-                  typename PairOf<T>::type v2;
-                  v2.x = v0;
-                  v2.y = v1;
-                  *reinterpret_cast<typename PairOf<T>::type*>(o) = v2;
-                } else {
-                  o[0] = v0;
-                  o[1] = v1;
-                }
-              } else if constexpr (!tail) {
-                T v = (COEFF == 0) ? slot_value<e>(done) * c : slot_value<e>(done);
-                if (so) v = v + so[0];
-                *o = v;
-              }
-            });
-          });
-        }
+      });
+      // One step per iteration: re-align the register slots with the next chunk (slot m takes
+      // what slot (m + CHP) held).
+      if constexpr (U == 1 && CHP % NP2 != 0) {
+        PipeSlot tmp[NP2];
+        static_for<0, NP2>([&](auto m) { tmp[decltype(m)::value] = acc[decltype(m)::value]; });
+        static_for<0, NP2>([&](auto m) { acc[decltype(m)::value] = tmp[(decltype(m)::value + CHP) % NP2]; });
+      }
+      optr += (tcs_i64)CHP * plane_g;
+      if (++cur_slot == nslot) {
+        cur_slot = 0;
+        cur_par ^= 1u;
       }
     });
-    // Re-align the register slots with the next chunk: slot m takes what slot (m + CHP) held.
-    if constexpr (CHP % NP2 != 0) {
-      PipeSlot tmp[NP2];
-      static_for<0, NP2>([&](auto m) { tmp[decltype(m)::value] = acc[decltype(m)::value]; });
-      static_for<0, NP2>([&](auto m) { acc[decltype(m)::value] = tmp[(decltype(m)::value + CHP) % NP2]; });
-    }
-    optr += (tcs_i64)CHP * plane_g;
-    if (++cur_slot == nslot) {
-      cur_slot = 0;
-      cur_par ^= 1u;
-    }
+    if (aborted) break;
   }
   st.gc = gc + nch;
   return !aborted;
