@@ -2,10 +2,9 @@
 tests/test_kernel_host.py.
 
 Transcribes the launch of ``launch_tb2`` (tcs_capi.cpp: output tile 128 x 256/es, thread tile
-1 x 8, persistent CTAs that walk the output tiles x fastest with a stride of the grid size, two
-input tiles and a first-sweep tile of dynamic shared memory) and the indexing of ``tcs_tb2``
-(tcs_kernels.cuh): the input tile's copies (zero outside the grid), the first-sweep tile written
-from thread tiles with its interior select, and the second sweep into the output.
+1 x 8, one CTA per output tile over the interior, the dynamic shared-memory size) and the indexing
+of ``tcs_tb2`` (tcs_kernels.cuh): the input tile's copies (zero outside the grid), the first-sweep
+tile written from thread tiles with its interior select, and the second sweep into the output.
 Every shared-memory index the thread tiles read or write is checked against the tile it addresses,
 and every stage-2 read must hit a value stage 1 wrote.  The tiles carry values, so the model also
 checks the result: on integer data with integer weights (exact sums in any order) one pass equals
@@ -18,7 +17,7 @@ import numpy as np
 
 from march_model import cdiv
 
-TB_TX, TB_CX, TB_CY, TB_THREADS = 128, 1, 8, 512
+TB_TX, TB_CX, TB_CY, TB_THREADS = 128, 1, 8, 256
 SMEM_OPTIN = 232448  # bytes of dynamic shared memory a B200 CTA may opt in to
 
 
@@ -34,11 +33,10 @@ def tiles(R: int, es: int):
 
 
 def smem_bytes(R: int, es: int) -> int:
-    """launch_tb2's dynamic shared memory: (2 (bw + 2R)(bh + 2R) + bw bh) elements (two input tiles
-    and the first-sweep tile)."""
+    """launch_tb2's dynamic shared memory: ((bw + 2R)(bh + 2R) + bw bh) elements."""
     bw = cdiv(TB_TX + 2 * R, TB_CX) * TB_CX
     bh = cdiv(tb_ty(es) + 2 * R, TB_CY) * TB_CY
-    return (2 * (bw + 2 * R) * (bh + 2 * R) + bw * bh) * es
+    return ((bw + 2 * R) * (bh + 2 * R) + bw * bh) * es
 
 
 def footprint(shape: str, R: int):
@@ -79,14 +77,13 @@ def _stage(src, sw, tiles_w, tiles_h, off, fp, w, size_src):
     return r0, c0, base, vals
 
 
-def sweep_tb2(a: np.ndarray, shape: str, R: int, w: dict, es: int, x0: int, x_lim: int, y_lim: int,
-              grid: int = 148):
+def sweep_tb2(a: np.ndarray, shape: str, R: int, w: dict, es: int, x0: int, x_lim: int, y_lim: int):
     """One tcs_tb2 launch over grid `a` (int64, rows y, columns x): returns (out, writes).  `out`
     starts as a copy of `a`, as the second ping-pong buffer carries the same border."""
     ydim, xdim = a.shape
     ty = tb_ty(es)
     BW, BH, AW, AH = tiles(R, es)
-    assert smem_bytes(R, es) == (2 * AW * AH + BW * BH) * es <= SMEM_OPTIN
+    assert smem_bytes(R, es) == (AW * AH + BW * BH) * es <= SMEM_OPTIN
     assert TB_TX % TB_CX == 0 and ty % TB_CY == 0
     fp = footprint(shape, R)
     hole = np.iinfo(np.int64).min
@@ -94,12 +91,8 @@ def sweep_tb2(a: np.ndarray, shape: str, R: int, w: dict, es: int, x0: int, x_li
     writes = np.zeros(a.shape, dtype=np.int64)
     ex, ey = max(0, x_lim - x0), y_lim - R
     gx_n, gy_n = max(1, cdiv(ex, TB_TX)), max(1, cdiv(ey, ty))
-    ntiles = gx_n * gy_n
-    order = [t for cta in range(min(grid, ntiles)) for t in range(cta, ntiles, min(grid, ntiles))]
-    assert sorted(order) == list(range(ntiles)), "every tile exactly once"
-    for t in order:
-        if True:
-            bx, by = t % gx_n, t // gx_n
+    for by in range(gy_n):
+        for bx in range(gx_n):
             xs, ys = x0 + bx * TB_TX, R + by * ty
             # input tile: q -> (r, cc), zero outside the grid
             q = np.arange(AW * AH)

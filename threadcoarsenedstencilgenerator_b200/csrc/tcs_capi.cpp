@@ -2357,7 +2357,7 @@ namespace {
 
 // The tile sizes match tcs_tb2's constants.  Thread tile 1 x 8: a warp reads 32 consecutive points
 // of a row (no bank conflicts) and each value loaded serves up to 8 outputs of a column.
-constexpr unsigned TB_TX = 128, TB_CX = 1, TB_CY = 8, TB_THREADS = 512;
+constexpr unsigned TB_TX = 128, TB_CX = 1, TB_CY = 8, TB_THREADS = 256;
 unsigned tb_ty(unsigned es) { return 256 / es; }  // tile rows: 32 FP64, 64 FP32
 
 // A parameter set's 2D spec with the TB thread tile; every other parameter as given.
@@ -2391,12 +2391,11 @@ int tb_module(tcs_stencil* h) {
 int launch_tb2(tcs_stencil* h, const TcsGeo& g, const void* in, void* out, CUstream st) {
   const unsigned R = (unsigned)h->spec.range;
   const unsigned es = (unsigned)elem_size(h->spec);
-  // first-sweep tile rounded up to whole thread tiles, input tile R wider on each side; two input
-  // tiles (the next tile's copies fill one while the CTA sweeps the other) and the first-sweep tile
+  // first-sweep tile rounded up to whole thread tiles, input tile R wider on each side
   const unsigned TB_TY = tb_ty(es);
   const unsigned bw = cdiv(TB_TX + 2 * R, TB_CX) * TB_CX, bh = cdiv(TB_TY + 2 * R, TB_CY) * TB_CY;
-  const unsigned smem = (2 * (bw + 2 * R) * (bh + 2 * R) + bw * bh) * es;
-  if (smem > (unsigned)h->smem_optin) return fail(TCS_ERR_UNSUPPORTED, "tb2: tiles do not fit in shared memory");
+  const unsigned smem = ((bw + 2 * R) * (bh + 2 * R) + bw * bh) * es;
+  if (smem > (unsigned)h->smem_optin) return fail(TCS_ERR_UNSUPPORTED, "tb2: tile does not fit in shared memory");
   {
     std::lock_guard<std::mutex> lock(h->mu);
     if ((int)smem > h->tb2_smem_attr) {
@@ -2404,19 +2403,13 @@ int launch_tb2(tcs_stencil* h, const TcsGeo& g, const void* in, void* out, CUstr
       h->tb2_smem_attr = (int)smem;
     }
   }
-  int occ = 0;
-  TCS_CU(g_drv.OccMaxActive(&occ, h->f_tb2, (int)TB_THREADS, smem));
-  if (occ < 1) return fail(TCS_ERR_UNSUPPORTED, "tb2 kernel cannot be resident");
   const unsigned long long ex = g.x_lim > g.x0 ? g.x_lim - g.x0 : 0, ey = g.y_lim - R;
-  const unsigned ntx = std::max(1u, cdiv(ex, TB_TX)), nty = std::max(1u, cdiv(ey, TB_TY));
-  const unsigned long long ntiles = (unsigned long long)ntx * nty;
-  if (ntiles > 0xffffffffull) return fail(TCS_ERR_UNSUPPORTED, "tb2: too many tiles");
-  const unsigned grid = (unsigned)std::min<unsigned long long>(ntiles, (unsigned long long)h->num_sms * occ);
+  const unsigned gx = std::max(1u, cdiv(ex, TB_TX)), gy = std::max(1u, cdiv(ey, TB_TY));
+  if (gy > 65535) return fail(TCS_ERR_UNSUPPORTED, "tb2: too many tile rows");
   CUdeviceptr pin = (CUdeviceptr)in, pout = (CUdeviceptr)out;
   TcsGeo geo = g;
-  unsigned nt = (unsigned)ntiles;
-  void* args[] = {&pin, &pout, &geo, (void*)&ntx, &nt};
-  TCS_CU(g_drv.LaunchKernel(h->f_tb2, grid, 1, 1, TB_THREADS, 1, 1, smem, st, args, nullptr));
+  void* args[] = {&pin, &pout, &geo};
+  TCS_CU(g_drv.LaunchKernel(h->f_tb2, gx, gy, 1, TB_THREADS, 1, 1, smem, st, args, nullptr));
   return TCS_OK;
 }
 

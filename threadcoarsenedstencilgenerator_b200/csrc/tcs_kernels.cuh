@@ -382,113 +382,76 @@ extern "C" __global__ void tcs_march(const __grid_constant__ TcsTmaMap tmap,
 #if defined(TCS_TB) && TCS_DIM == 2
 // ---- tcs_tb2: two sweeps in one pass over HBM (temporal blocking, 2D) -------------------------
 // Runs on an instance with coarsening CX x CY = 1 x 8 (the thread tile; independent of the
-// caller's coarsening).  Persistent CTAs walk the output tiles (TB_TY x TB_TX, x fastest) with a
-// stride of the grid size.  For each tile the CTA computes the first sweep on the tile plus a
-// range-wide halo into a shared tile -- interior points with the stencil, every other point keeps
-// its input value (the fixed border, as in the second buffer of a ping-pong pair) -- and then the
-// second sweep of its outputs from that.  Two input tiles alternate: while the CTA sweeps one, the
-// async copy unit fills the other with the CTA's next tile (cp.async, zero outside the grid;
-// commit groups, so only the current tile's copies are waited for).  Both stages run the tile
-// arithmetic on CX x CY thread tiles, so every footprint value read from shared memory serves all
-// the outputs it touches.  The per-point term order does not depend on the tile, so
-// out = S(S(in)) bit for bit; `out` needs in's border (the ping-pong invariant).
-constexpr int TB_TX = 128, TB_TY = 256 / (int)sizeof(T), TB_THREADS = 512;  // TB_TY: 32 FP64, 64 FP32
+// caller's coarsening).  A CTA loads an input tile into shared memory, computes the first sweep on
+// the region of TB_TY x TB_TX outputs plus a range-wide halo into a second tile -- interior points
+// with the stencil, every other point keeps its input value (the fixed border, as in the second
+// buffer of a ping-pong pair) -- and then the second sweep of its outputs from that.  Both stages
+// run the tile arithmetic on CX x CY thread tiles, so every footprint value read from shared
+// memory serves all the outputs it touches.  The per-point term order does not depend on the
+// tile, so out = S(S(in)) bit for bit; `out` needs in's border (the ping-pong invariant).
+constexpr int TB_TX = 128, TB_TY = 256 / (int)sizeof(T), TB_THREADS = 256;  // TB_TY: 32 FP64, 64 FP32
 
-namespace tcs {
-constexpr int TB_BW = (TB_TX + 2 * R + CX - 1) / CX * CX;  // first-sweep tile (rounded to thread tiles)
-constexpr int TB_BH = (TB_TY + 2 * R + CY - 1) / CY * CY;
-constexpr int TB_AW = TB_BW + 2 * R, TB_AH = TB_BH + 2 * R;  // input tile
-
-// Copies of the input tile whose first output is (xs, ys) into A (points outside the grid: zero).
-__device__ __forceinline__ void tb2_load(const T* __restrict__ in, const TcsGeo& g, tcs_i64 xs, tcs_i64 ys,
-                                         T* A) {
+extern "C" __global__ void __launch_bounds__(TB_THREADS)
+    tcs_tb2(const T* __restrict__ in, T* __restrict__ out, const TcsGeo g) {
+  using namespace tcs;
+  static_assert(TB_TX % CX == 0 && TB_TY % CY == 0, "output tile is a multiple of the thread tile");
+  extern __shared__ __align__(16) unsigned char tb_smem[];
+  constexpr int BW = (TB_TX + 2 * R + CX - 1) / CX * CX;  // first-sweep tile (rounded to thread tiles)
+  constexpr int BH = (TB_TY + 2 * R + CY - 1) / CY * CY;
+  constexpr int AW = BW + 2 * R, AH = BH + 2 * R;         // input tile
+  T* A = reinterpret_cast<T*>(tb_smem);
+  T* Bt = A + AW * AH;
+  constexpr T c = T(1) / T(S);
   const tcs_i64 xdim = (tcs_i64)g.xdim, ydim = (tcs_i64)g.ydim;
+  const tcs_i64 xs = (tcs_i64)g.x0 + (tcs_i64)blockIdx.x * TB_TX;  // first output column
+  const tcs_i64 ys = (tcs_i64)R + (tcs_i64)blockIdx.y * TB_TY;     // first output row
+  // Input tile through the async copy unit: every thread issues all its copies before waiting, so
+  // the whole tile is in flight at once; points outside the grid read as zero.
   const tcs_u32 a_s = (tcs_u32)__cvta_generic_to_shared(A);
-  for (int q = threadIdx.x; q < TB_AW * TB_AH; q += TB_THREADS) {
-    const int r = q / TB_AW, cc = q - r * TB_AW;
+  for (int q = threadIdx.x; q < AW * AH; q += TB_THREADS) {
+    const int r = q / AW, cc = q - r * AW;
     const tcs_i64 gy = ys - 2 * R + r, gx = xs - 2 * R + cc;
     const bool inside = gy >= 0 && gy < ydim && gx >= 0 && gx < xdim;
     cp_async_elem(a_s + (tcs_u32)q * (tcs_u32)sizeof(T), in + (inside ? gy * xdim + gx : 0),
                   inside ? (tcs_u32)sizeof(T) : 0u);
   }
-}
-}  // namespace tcs
-
-extern "C" __global__ void __launch_bounds__(TB_THREADS)
-    tcs_tb2(const T* __restrict__ in, T* __restrict__ out, const TcsGeo g, const tcs_u32 ntx,
-            const tcs_u32 ntiles) {
-  using namespace tcs;
-  static_assert(TB_TX % CX == 0 && TB_TY % CY == 0, "output tile is a multiple of the thread tile");
-  extern __shared__ __align__(16) unsigned char tb_smem[];
-  T* const A0 = reinterpret_cast<T*>(tb_smem);
-  T* const A1 = A0 + TB_AW * TB_AH;
-  T* const Bt = A1 + TB_AW * TB_AH;
-  constexpr T c = T(1) / T(S);
-  const tcs_i64 xdim = (tcs_i64)g.xdim;
-  tcs_u32 tile = blockIdx.x;
-  if (tile >= ntiles) return;
-  auto origin = [&](tcs_u32 t, tcs_i64& xs, tcs_i64& ys) {
-    xs = (tcs_i64)g.x0 + (tcs_i64)(t % ntx) * TB_TX;  // first output column
-    ys = (tcs_i64)R + (tcs_i64)(t / ntx) * TB_TY;     // first output row
-  };
-  {
-    tcs_i64 xs, ys;
-    origin(tile, xs, ys);
-    tb2_load(in, g, xs, ys, A0);
-    asm volatile("cp.async.commit_group;" ::: "memory");
-  }
-  for (tcs_u32 i = 0; tile < ntiles; ++i) {
-    const tcs_u32 next = tile + gridDim.x;
-    T* const A = (i & 1u) ? A1 : A0;
-    if (next < ntiles) {  // the next tile's copies run during this tile's two stages
-      tcs_i64 xn, yn;
-      origin(next, xn, yn);
-      tb2_load(in, g, xn, yn, (i & 1u) ? A0 : A1);
-    }
-    asm volatile("cp.async.commit_group;" ::: "memory");
-    asm volatile("cp.async.wait_group 1;" ::: "memory");  // this tile's copies (all but the newest group)
-    __syncthreads();
-    tcs_i64 xs, ys;
-    origin(tile, xs, ys);
-    constexpr int NT1 = (TB_BW / CX) * (TB_BH / CY);
-    for (int t = threadIdx.x; t < NT1; t += TB_THREADS) {
-      const int r0 = (t / (TB_BW / CX)) * CY, c0 = (t % (TB_BW / CX)) * CX;  // first-sweep tile coordinates
-      const T* p = A + (r0 + R) * TB_AW + (c0 + R);
-      auto ld = [&](int dx, int dy, int) { return p[dx + dy * TB_AW]; };
-      Acc acc[NE];
-      traverse(ld, acc);
-      static_for<0, CY>([&](auto ey) {
-        static_for<0, CX>([&](auto ex) {
-          constexpr int e = decltype(ex)::value + decltype(ey)::value * CX;
-          const tcs_i64 gy = ys - R + r0 + decltype(ey)::value, gx = xs - R + c0 + decltype(ex)::value;
-          const bool interior = gx >= (tcs_i64)g.x0 && gx < (tcs_i64)g.x_lim && gy >= R && gy < (tcs_i64)g.y_lim;
-          const T v = (COEFF == 0) ? acc_value(acc[e]) * c : acc_value(acc[e]);
-          Bt[(r0 + decltype(ey)::value) * TB_BW + c0 + decltype(ex)::value] =
-              interior ? v : p[decltype(ex)::value + decltype(ey)::value * TB_AW];  // not swept: keeps its value
-        });
-      });
-    }
-    __syncthreads();
-    constexpr int NT2 = (TB_TX / CX) * (TB_TY / CY);
-    for (int t = threadIdx.x; t < NT2; t += TB_THREADS) {
-      const int r0 = (t / (TB_TX / CX)) * CY, c0 = (t % (TB_TX / CX)) * CX;  // output tile coordinates
-      const T* p = Bt + (r0 + R) * TB_BW + (c0 + R);
-      auto ld = [&](int dx, int dy, int) { return p[dx + dy * TB_BW]; };
-      Acc acc[NE];
-      traverse(ld, acc);
-      static_for<0, CY>([&](auto ey) {
-        static_for<0, CX>([&](auto ex) {
-          constexpr int e = decltype(ex)::value + decltype(ey)::value * CX;
-          const tcs_i64 gy = ys + r0 + decltype(ey)::value, gx = xs + c0 + decltype(ex)::value;
-          if (gx < (tcs_i64)g.x_lim && gy < (tcs_i64)g.y_lim)
-            out[gy * xdim + gx] = (COEFF == 0) ? acc_value(acc[e]) * c : acc_value(acc[e]);
-        });
-      });
-    }
-    __syncthreads();  // Bt and this tile's input buffer are reused two tiles on
-    tile = next;
-  }
   cp_async_wait_all();
+  __syncthreads();
+  constexpr int NT1 = (BW / CX) * (BH / CY);
+  for (int t = threadIdx.x; t < NT1; t += TB_THREADS) {
+    const int r0 = (t / (BW / CX)) * CY, c0 = (t % (BW / CX)) * CX;  // first-sweep tile coordinates
+    const T* p = A + (r0 + R) * AW + (c0 + R);
+    auto ld = [&](int dx, int dy, int) { return p[dx + dy * AW]; };
+    Acc acc[NE];
+    traverse(ld, acc);
+    static_for<0, CY>([&](auto ey) {
+      static_for<0, CX>([&](auto ex) {
+        constexpr int e = decltype(ex)::value + decltype(ey)::value * CX;
+        const tcs_i64 gy = ys - R + r0 + decltype(ey)::value, gx = xs - R + c0 + decltype(ex)::value;
+        const bool interior = gx >= (tcs_i64)g.x0 && gx < (tcs_i64)g.x_lim && gy >= R && gy < (tcs_i64)g.y_lim;
+        const T v = (COEFF == 0) ? acc_value(acc[e]) * c : acc_value(acc[e]);
+        Bt[(r0 + decltype(ey)::value) * BW + c0 + decltype(ex)::value] =
+            interior ? v : p[decltype(ex)::value + decltype(ey)::value * AW];  // not swept: keeps its value
+      });
+    });
+  }
+  __syncthreads();
+  constexpr int NT2 = (TB_TX / CX) * (TB_TY / CY);
+  for (int t = threadIdx.x; t < NT2; t += TB_THREADS) {
+    const int r0 = (t / (TB_TX / CX)) * CY, c0 = (t % (TB_TX / CX)) * CX;  // output tile coordinates
+    const T* p = Bt + (r0 + R) * BW + (c0 + R);
+    auto ld = [&](int dx, int dy, int) { return p[dx + dy * BW]; };
+    Acc acc[NE];
+    traverse(ld, acc);
+    static_for<0, CY>([&](auto ey) {
+      static_for<0, CX>([&](auto ex) {
+        constexpr int e = decltype(ex)::value + decltype(ey)::value * CX;
+        const tcs_i64 gy = ys + r0 + decltype(ey)::value, gx = xs + c0 + decltype(ex)::value;
+        if (gx < (tcs_i64)g.x_lim && gy < (tcs_i64)g.y_lim)
+          out[gy * xdim + gx] = (COEFF == 0) ? acc_value(acc[e]) * c : acc_value(acc[e]);
+      });
+    });
+  }
 }
 #endif
 
