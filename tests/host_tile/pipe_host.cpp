@@ -43,6 +43,8 @@ extern "C" int pipe_sweep(const unsigned grid[3], unsigned left_offset, unsigned
   constexpr int NP2 = 2 * R + 1;
   if (COEFF == 1)
     for (int k = 0; k < S; ++k) tcs_mask[k] = (T)mask[k];
+  if (COEFF == 1 && tcs::PAIRS)
+    for (int k = 0; k < S; ++k) tcs_mask_pairs[k] = make_float2((float)mask[k], (float)mask[k]);
   const long long xdim = grid[0], ydim = grid[1], zdim = DIM == 3 ? grid[2] : 1;
   const long long plane = DIM == 3 ? xdim * ydim : xdim;  // stride of the march axis
   const long long x_lim = xdim - R - (aligned ? right_offset : 0);

@@ -57,6 +57,8 @@ extern "C" int tb3_pass(const unsigned grid[3], unsigned left_offset, unsigned r
   constexpr int NP2 = 2 * R + 1;
   if (COEFF == 1)
     for (int k = 0; k < S; ++k) tcs_mask[k] = (T)mask[k];
+  if (COEFF == 1 && tcs::PAIRS)
+    for (int k = 0; k < S; ++k) tcs_mask_pairs[k] = make_float2((float)mask[k], (float)mask[k]);
   const long long xdim = grid[0], ydim = grid[1], zdim = grid[2];
   const long long plane = xdim * ydim;
   const long long x0 = R + left_offset;

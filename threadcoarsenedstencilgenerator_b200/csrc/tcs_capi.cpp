@@ -344,6 +344,8 @@ struct PipeMod {
   CUfunction f = nullptr;
   CUdeviceptr mask_ptr = 0;
   size_t mask_bytes = 0;
+  CUdeviceptr pairs_ptr = 0;  // tcs_mask_pairs (packed FP32 instances), 0 when absent
+  size_t pairs_bytes = 0;
   CUdeviceptr status_ptr = 0;
   int smem_attr = 0;
 };
@@ -595,6 +597,20 @@ int upload_mask(tcs_stencil* h, CUdeviceptr dst) {
   return TCS_OK;
 }
 
+// The mask of a pipelined module: tcs_mask, and the (m_k, m_k) pairs of packed FP32 instances.
+int upload_pipe_mask(tcs_stencil* h, const PipeMod* pm) {
+  int rc = upload_mask(h, pm->mask_ptr);
+  if (rc) return rc;
+  const unsigned n = (unsigned)h->mask_host.size();
+  if (!pm->pairs_ptr || n == 0 || h->spec.coefficients == TCS_JACOBI || h->spec.precision == TCS_F64 ||
+      pm->pairs_bytes != 2 * sizeof(float) * n)
+    return TCS_OK;
+  std::vector<float> f(2 * n);
+  for (unsigned k = 0; k < n; ++k) f[2 * k] = f[2 * k + 1] = (float)h->mask_host[k];
+  TCS_RT(cudaMemcpy((void*)pm->pairs_ptr, f.data(), sizeof(float) * 2 * n, cudaMemcpyHostToDevice));
+  return TCS_OK;
+}
+
 // Pipelined-sweep module for a launch shape: instantiate (NVRTC, cached) and load on first use.
 int pipe_module(tcs_stencil* h, const PipeKey& key, PipeMod** out) {
   std::lock_guard<std::mutex> lock(h->mu);
@@ -623,8 +639,12 @@ int pipe_module(tcs_stencil* h, const PipeKey& key, PipeMod** out) {
     delete pm;
     return fail(TCS_ERR_CUDA, "pipe module symbols: " + cu_msg(cr));
   }
+  if (g_drv.ModuleGetGlobal(&pm->pairs_ptr, &pm->pairs_bytes, pm->mod, "tcs_mask_pairs") != CUDA_SUCCESS) {
+    pm->pairs_ptr = 0;
+    pm->pairs_bytes = 0;
+  }
   cudaMemset((void*)pm->status_ptr, 0, sizeof(unsigned));
-  rc = upload_mask(h, pm->mask_ptr);
+  rc = upload_pipe_mask(h, pm);
   if (rc) {
     g_drv.ModuleUnload(pm->mod);
     delete pm;
@@ -1329,7 +1349,7 @@ int tcs_copy_mask(tcs_stencil* h, const double* mask, unsigned n) {
   int rc = upload_mask(h, h->mask_ptr);
   if (rc) return rc;
   for (PipeMod* p : h->pipes) {
-    rc = upload_mask(h, p->mask_ptr);
+    rc = upload_pipe_mask(h, p);
     if (rc) return rc;
   }
   if (h->fringe_mod && (rc = upload_mask(h, h->fringe_mask))) return rc;

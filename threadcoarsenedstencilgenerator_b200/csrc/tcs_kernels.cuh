@@ -605,6 +605,7 @@ struct PipeGridView {
   bool st_pair;  // output pairs stored with one access (even pitch, pair-aligned base)
   void* aux;     // epilogues 1 and 2: the float defect array / the double state (same layout)
   bool src_pair;  // source pairs read with one access (the store's rule for the source's base)
+  bool aux_pair;  // epilogue 2: FP64 state pairs with one access (even pitch, 16-byte base)
 };
 
 // cp.async fill of one ring chunk: CHP planes of ROWS rows (3D) or CHP rows (2D), PW elements
@@ -769,15 +770,23 @@ __device__ __forceinline__ bool pipe_piece(const PipeGridView& G, tcs_u32 tile, 
           // A source term is read from global memory when its output row is stored: fetch the rows
           // of the output completed PF planes later into L1 now, so that the store does not wait
           // for the latency of DRAM or L2.
+          // (Epilogue 2 reads and writes the FP64 state the same way: its rows too.)
           constexpr int PF = 2;
-          if (G.src && lane_ok) {
+          if ((G.src || EPI == 2) && lane_ok) {
             const int opf = (int)pi - 2 * R + PF;
             if (opf >= 0 && opf < (int)nout) {
-              const T* sp = G.src + ((optr - G.out) + (tcs_i64)(t + PF) * plane_g);
+              const tcs_i64 off0 = (optr - G.out) + (tcs_i64)(t + PF) * plane_g;
               static_for<0, (DIM == 3) ? CY : 1>([&](auto ey) {
-                const T* q = sp + decltype(ey)::value * (tcs_i64)G.xdim;
-                asm volatile("prefetch.global.L1 [%0];" ::"l"(q));
-                if constexpr (CX * sizeof(T) > 16) asm volatile("prefetch.global.L1 [%0];" ::"l"(q + CX - 1));
+                const tcs_i64 off = off0 + decltype(ey)::value * (tcs_i64)G.xdim;
+                if (G.src) {
+                  asm volatile("prefetch.global.L1 [%0];" ::"l"(G.src + off));
+                  if constexpr (CX * sizeof(T) > 16) asm volatile("prefetch.global.L1 [%0];" ::"l"(G.src + off + CX - 1));
+                }
+                if constexpr (EPI == 2) {
+                  const double* xq = static_cast<const double*>(G.aux) + off;
+                  asm volatile("prefetch.global.L1 [%0];" ::"l"(xq));
+                  if constexpr (CX * sizeof(double) > 16) asm volatile("prefetch.global.L1 [%0];" ::"l"(xq + CX - 1));
+                }
               });
             }
           }
@@ -803,9 +812,29 @@ __device__ __forceinline__ bool pipe_piece(const PipeGridView& G, tcs_u32 tile, 
                   st.nmax = fmax(st.nmax, fabs(d));
                   st.nsum = fma(d, d, st.nsum);
                 } else {
-                  if (G.src) v = v + G.src[off];
+                  // the state's pairs with one access each way where the output pair rule holds
+                  constexpr bool pair = pipe_pair_aligned(0) && (decltype(ex)::value % 2 == 0);
+                  constexpr bool tail = pipe_pair_aligned(0) && (decltype(ex)::value % 2 == 1);
                   double* xg = static_cast<double*>(G.aux);
-                  xg[off] = xg[off] + (double)v;
+                  if constexpr (pair) {
+                    T v1 = (COEFF == 0) ? slot_value<e + 1>(done) * c : slot_value<e + 1>(done);
+                    if (G.src) {
+                      v = v + G.src[off];
+                      v1 = v1 + G.src[off + 1];
+                    }
+                    if (G.aux_pair) {
+                      double2 x2 = *reinterpret_cast<const double2*>(xg + off);
+                      x2.x = x2.x + (double)v;
+                      x2.y = x2.y + (double)v1;
+                      *reinterpret_cast<double2*>(xg + off) = x2;
+                    } else {
+                      xg[off] = xg[off] + (double)v;
+                      xg[off + 1] = xg[off + 1] + (double)v1;
+                    }
+                  } else if constexpr (!tail) {
+                    if (G.src) v = v + G.src[off];
+                    xg[off] = xg[off] + (double)v;
+                  }
                 }
               });
             });
@@ -925,6 +954,7 @@ extern "C" __global__ void __launch_bounds__(TCS_BX * ((TCS_DIM == 3) ? TCS_BY :
   // an even row pitch and a pair-aligned base address.
   G.st_pair = (g.xdim % 2 == 0) && (reinterpret_cast<tcs_u64>(out) % (2 * sizeof(T)) == 0);
   G.src_pair = G.st_pair && (reinterpret_cast<tcs_u64>(src) % (2 * sizeof(T)) == 0);
+  G.aux_pair = (g.xdim % 2 == 0) && (reinterpret_cast<tcs_u64>(aux) % 16 == 0);
   if (G.use_tma && threadIdx.x == 0 && threadIdx.y == 0) tma_prefetch_map(&tmap);
   PipeState st = pipe_setup(g.nslot, G.use_tma);
   PipeSlot acc[NP2];
@@ -1014,6 +1044,7 @@ extern "C" __global__ void __launch_bounds__(TCS_BX * ((TCS_DIM == 3) ? TCS_BY :
     G.st_pair = (B.xdim % 2 == 0) && (reinterpret_cast<tcs_u64>(B.out) % (2 * sizeof(T)) == 0);
     G.src_pair = G.st_pair && (reinterpret_cast<tcs_u64>(B.src) % (2 * sizeof(T)) == 0);
     G.aux = nullptr;
+    G.aux_pair = false;
     const tcs_u64 local = w - B.first;
     const tcs_u32 tile = (tcs_u32)(local / B.m);
     const tcs_u32 zs = (tcs_u32)(local % B.m);

@@ -327,6 +327,15 @@ constexpr int NEP = (DIM == 3) ? CX * CY : CX;  // outputs per thread and plane
 constexpr bool PAIRS = (TCS_PAIRS != 0) && sizeof(T) == 4 && SHAPE == 0 && CX % 2 == 0 &&
                        (DIM == 2 || ORIENT == 0);
 constexpr int NPAIR = (NEP / 2 > 0) ? NEP / 2 : 1;
+}  // namespace tcs
+
+// The packed path's coefficients as pairs (m_k, m_k): a term's broadcast operand of the packed
+// fma is one 64-bit constant read instead of a pair assembled in registers.  The host fills it
+// from the same mask as tcs_mask (pipelined modules that declare it with S entries).
+__constant__ float2 tcs_mask_pairs[tcs::PAIRS ? tcs::S : 1];
+
+namespace tcs {
+__device__ __forceinline__ float2 mask_pair(int k) { return tcs_mask_pairs[k]; }
 
 // The accumulators of one output plane of a thread: NEP scalars, or NEP/2 packed pairs (output
 // e = ex + ey*CX is lane e%2 of pair e/2).  The compensated form (FP32 grids, TCS_COMP) keeps, per
@@ -404,12 +413,11 @@ __device__ __forceinline__ void apply_pair(float2& a, const float2 v) {
   } else if constexpr (COEFF == 0) {
     a = __fadd2_rn(a, v);
   } else {
-    const float m = tcs_mask[mask_index(RX, RY, RZ)];
+    const float2 mm = mask_pair(mask_index(RX, RY, RZ));
     if constexpr (is_second(RX, RY, RZ)) {
-      const float m0 = tcs_mask[first_mask_index()];
-      a = __ffma2_rn(a, make_float2(m0, m0), __fmul2_rn(v, make_float2(m, m)));
+      a = __ffma2_rn(a, mask_pair(first_mask_index()), __fmul2_rn(v, mm));
     } else {
-      a = __ffma2_rn(v, make_float2(m, m), a);
+      a = __ffma2_rn(v, mm, a);
     }
   }
 }
@@ -425,14 +433,12 @@ __device__ __forceinline__ void row_term_pair(float2& q, const float2 v) {
     if constexpr (COEFF == 0) {
       q = v;
     } else {
-      const float m = tcs_mask[mask_index(RX, RY, RZ)];
-      q = __fmul2_rn(v, make_float2(m, m));
+      q = __fmul2_rn(v, mask_pair(mask_index(RX, RY, RZ)));
     }
   } else if constexpr (COEFF == 0) {
     q = __fadd2_rn(q, v);
   } else {
-    const float m = tcs_mask[mask_index(RX, RY, RZ)];
-    q = __ffma2_rn(v, make_float2(m, m), q);
+    q = __ffma2_rn(v, mask_pair(mask_index(RX, RY, RZ)), q);
   }
 }
 
