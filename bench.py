@@ -952,7 +952,9 @@ def run_case(args) -> dict:
     of a batch (--grids), for profilers: a small case of the same kernel that an ncu capture
     finishes in a minute.  Keep each buffer above the L2 size (126 MB) so that DRAM counters
     stay meaningful.  --case tensor-cores / temporal select the tcgen05 FP32 sweep / the
-    two-sweeps-per-pass kernel (2D)."""
+    two-sweeps-per-pass kernel (2D); --case-launch one pipelined launch instead of the tuned one.
+    One warm-up sweep (two for temporal) precedes the --steps sweeps, whose rate is reported from
+    CUDA events ("glups"; 1-GPU case timing, not the bench line)."""
     import numpy as np
     import torch
 
@@ -998,22 +1000,35 @@ def run_case(args) -> dict:
     dt = torch.float64 if args.case_precision == "f64" else torch.float32
     x = torch.from_numpy(w.make_input(geom)).to("cuda", dtype=dt)
     y = x.clone()
-    if args.case == "temporal":
-        st.sweeps_tb2(geom, x, y, args.steps)
-    else:
-        for _ in range(args.steps):
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def run(n):
+        nonlocal x, y
+        if args.case == "temporal":
+            st.sweeps_tb2(geom, x, y, n)
+            return
+        for _ in range(n):
             if args.case == "tensor-cores":
                 st.tc_update_grid(geom, x, y)
             else:
                 st.update_grid(geom, x, y, launch)
             x, y = y, x
+
+    run(2 if args.case == "temporal" else 1)  # warm-up (module load, first touch)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    run(args.steps)
+    e1.record(stream)
     torch.cuda.synchronize()
     if st.device_status() != 0:
         raise RuntimeError("device status word set")
     plan = st.plan(geom, launch)
+    ms = e0.elapsed_time(e1)  # CUDA events around the --steps sweeps after the warm-up
     return {"case": args.workload, "grid": list(grid), "points": geom.interior_points, "sweeps": args.steps,
             "kernel": args.case, "variant": plan.variant, "block": list(plan.block), "chunk": plan.chunk,
-            "coarsening": [spec.cx, spec.cy, spec.cz], "shuffle": bool(launch.shuffle)}
+            "coarsening": [spec.cx, spec.cy, spec.cz], "shuffle": bool(launch.shuffle),
+            "glups": geom.interior_points * args.steps / (ms / 1e3) / 1e9 if ms > 0 else None}
 
 
 def case_launch(spec, text: str):

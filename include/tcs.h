@@ -100,6 +100,10 @@ typedef struct tcs_launch {
  * multiple of 32) through warp shuffles, or through shared-memory loads only. */
 #define TCS_LAUNCH_SHUFFLE 1u
 #define TCS_LAUNCH_NO_SHUFFLE 2u
+/* tcs_launch.flags: the pipelined sweep of a 3D Star stencil in Row order in its ring form: own
+ * centre values and finished crosses in two R-entry rings in tensor memory, two output planes in
+ * registers (plain single-grid sweeps; cx*cy*sizeof(element)/4 of 4, 8 or 16). */
+#define TCS_LAUNCH_TMEM 4u
 
 /* Resolved launch of one sweep (what tcs_update_grid will run). */
 typedef struct tcs_plan {

@@ -77,6 +77,25 @@ def pipe_sweeps(cfg, a: np.ndarray, grid, left_offset, right_offset, n: int, mas
     return x
 
 
+def pipe_ring_sweeps(cfg, a: np.ndarray, grid, left_offset, right_offset, n: int, mask=None, precision="f64",
+                     piece: int = 1 << 30):
+    """n sweeps through the host build of the ring form of the pipelined sweep (3D Star, Row)."""
+    lib = build(cfg, precision, "pipe_host.cpp")
+    d, sh, o, c, r, cx, cy, cz, al, cl = cfg
+    x = np.ascontiguousarray(a).copy()
+    y = x.copy()
+    m = np.ascontiguousarray(np.zeros(1) if mask is None else np.asarray(mask, dtype=np.float64))
+    u3 = ctypes.c_uint * 3
+    for _ in range(n):
+        rc = lib.pipe_sweep_ring(u3(*grid), ctypes.c_uint(left_offset), ctypes.c_uint(right_offset),
+                                 ctypes.c_int(0 if al == "None" else 1), x.ctypes.data_as(ctypes.c_void_p),
+                                 y.ctypes.data_as(ctypes.c_void_p), m.ctypes.data_as(ctypes.c_void_p),
+                                 ctypes.c_uint(piece))
+        assert rc == 0
+        x, y = y, x
+    return x
+
+
 def tb3_passes(cfg, a: np.ndarray, grid, left_offset, right_offset, n: int, mask=None, precision="f64",
                block=(8, 8), piece: int = 1 << 30, unroll: int = 2):
     """n passes (2n sweeps) through the host build of the 3D two-sweep kernel's control flow,

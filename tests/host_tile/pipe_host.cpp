@@ -90,3 +90,69 @@ extern "C" int pipe_sweep(const unsigned grid[3], unsigned left_offset, unsigned
       }
   return 0;
 }
+
+// The ring form (tcs::ring_step, the kernel's TCS_TMEM variant) of 3D Star stencils in Row
+// order: per input plane c of a piece, the output centred on c - R is completed from the rings and
+// stored; the rings are plain arrays here (tensor memory in the kernel), entry (plane mod R).
+#if TCS_DIM == 3 && TCS_SHAPE == 1 && TCS_ORIENT == 0
+struct HostRing {
+  T (*raw)[tcs::NEP];
+  tcs::PipeSlot* acc;
+  long long c;  // current input plane (piece-relative)
+  int entry(long long p) const { return (int)(((p % tcs::R) + tcs::R) % tcs::R); }
+  void load_acc(tcs::PipeSlot& s) const { s = acc[entry(c - tcs::R)]; }
+  template <int I>
+  void load_raw(T (&v)[tcs::NEP]) const {
+    std::memcpy(v, raw[entry(c - tcs::R + I)], sizeof(v));
+  }
+  void store(const tcs::PipeSlot& s, const T (&v)[tcs::NEP]) {
+    acc[entry(c)] = s;
+    std::memcpy(raw[entry(c)], v, sizeof(v));
+  }
+};
+
+extern "C" int pipe_sweep_ring(const unsigned grid[3], unsigned left_offset, unsigned right_offset,
+                               int aligned, const T* in, T* out, const double* mask, unsigned piece) {
+  using namespace tcs;
+  if (COEFF == 1)
+    for (int k = 0; k < S; ++k) tcs_mask[k] = (T)mask[k];
+  const long long xdim = grid[0], ydim = grid[1], zdim = grid[2];
+  const long long plane = xdim * ydim;
+  const long long x_lim = xdim - R - (aligned ? right_offset : 0);
+  const long long y_lim = ydim - R, z_lim = zdim - R;
+  // stale ring contents from the previous piece (or column) must not matter: start from garbage
+  T raw[R][NEP];
+  PipeSlot acc[R];
+  for (int i = 0; i < R; ++i)
+    for (int e = 0; e < NEP; ++e) raw[i][e] = (T)NAN;
+  std::memset(static_cast<void*>(acc), 0xff, sizeof(acc));
+  for (long long y = R; y + CY - 1 < y_lim; y += CY)
+    for (long long x = R + left_offset; x + CX - 1 < x_lim; x += CX)
+      for (long long ms = R; ms < z_lim; ms += piece) {
+        const long long me = (ms + piece < z_lim) ? ms + piece : z_lim;
+        const long long np = me - ms + 2 * R;
+        for (long long pi = 0; pi < np; ++pi) {
+          const long long p = ms - R + pi;
+          const HostPlane ld{in + x + y * xdim + p * plane, xdim};
+          HostRing ring{raw, acc, pi};
+          PipeSlot done;
+          ring_step(ld, ring, done);
+          const long long op = pi - 2 * R;
+          if (op >= 0 && op < me - ms) {
+            constexpr T c = T(1) / T(S);
+            T* o = out + x + y * xdim + (ms + op) * plane;
+            for (int ey = 0; ey < CY; ++ey)
+              for (int ex = 0; ex < CX; ++ex) {
+                const T v = slot_value_rt(done, ex + ey * CX);
+                o[ex + ey * xdim] = (COEFF == 0) ? v * c : v;
+              }
+          }
+        }
+      }
+  return 0;
+}
+#else
+extern "C" int pipe_sweep_ring(const unsigned*, unsigned, unsigned, int, const T*, T*, const double*, unsigned) {
+  return -1;
+}
+#endif

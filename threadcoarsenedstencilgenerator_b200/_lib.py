@@ -26,6 +26,7 @@ VARIANT_PIPE = 3
 
 LAUNCH_SHUFFLE = 1
 LAUNCH_NO_SHUFFLE = 2
+LAUNCH_TMEM = 4
 
 
 class TcsError(RuntimeError):

@@ -219,11 +219,28 @@ struct PipeKey {
   unsigned epi = 0;  // epilogue mode (tcs_kernels.cuh, TCS_EPI): 0 plain, 1 FP64 defect, 2 FP32 accumulate
   unsigned tb3 = 0;  // tcs_tb3 (two sweeps per pass, 3D) with thread tiles tb3 x tb3; 0: tcs_pipe
   unsigned shfl = 0;  // Star middle rows through warp shuffles (TCS_SHFL)
+  unsigned tmem = 0;  // ring form in tensor memory (TCS_TMEM)
   bool operator==(const PipeKey& o) const {
     return bx == o.bx && by == o.by && ch == o.ch && lshift == o.lshift && batch == o.batch && epi == o.epi &&
-           tb3 == o.tb3 && shfl == o.shfl;
+           tb3 == o.tb3 && shfl == o.shfl && tmem == o.tmem;
   }
 };
+
+// The ring form (TCS_TMEM, tcs_kernels.cuh): 3D Star stencils in Row order, FP64 or FP32, plain
+// epilogue, ring entries of 4, 8 or 16 columns, blocks of whole warps.  Its tensor-memory columns per CTA (the
+// allocation, a power of two) or 0 when the form does not apply.
+unsigned tmem_cols(const tcs_spec& s, unsigned bx, unsigned by) {
+  if (s.dimension != 3 || s.neighbourhood != TCS_STAR || s.orientation != TCS_ROW || s.precision == TCS_F32C)
+    return 0;
+  if ((bx * by) % 32u != 0) return 0;  // tensor-memory loads and stores are whole-warp instructions
+  const unsigned w = (unsigned)(s.cx * s.cy) * (s.precision == TCS_F64 ? 2u : 1u);
+  if (w != 4 && w != 8 && w != 16) return 0;
+  const unsigned groups = (bx * by + 127u) / 128u;
+  const unsigned need = groups * 2u * (unsigned)s.range * w;
+  unsigned n = 32;
+  while (n < need) n *= 2;
+  return n <= 512 ? n : 0;
+}
 
 std::string instance_macros(const tcs_spec& s, const PipeKey* pk) {
   std::ostringstream m;
@@ -234,6 +251,7 @@ std::string instance_macros(const tcs_spec& s, const PipeKey* pk) {
   if (pk && pk->epi) m << "#define TCS_EPI " << pk->epi << "\n";
   if (pk && pk->tb3) m << "#define TCS_TB3 1\n";
   if (pk && pk->shfl) m << "#define TCS_SHFL 1\n";
+  if (pk && pk->tmem) m << "#define TCS_TMEM 1\n";
   // TCS_PIPE_CYCLE=0 in the environment builds the pipelined kernels with a one-chunk loop body
   // (register slots rotated at the back-edge) instead of one whole slot cycle per iteration
   if (pk) {
@@ -751,7 +769,14 @@ int resolve_pipe(tcs_stencil* h, const TcsGeo& g, const tcs_launch* L, Resolved&
   if ((L->flags & TCS_LAUNCH_SHUFFLE) && !shfl_ok)
     return fail(TCS_ERR_UNSUPPORTED, "pipe: shuffled rows need a Star stencil in Row order and bx % 32 == 0");
   const unsigned shfl = ((L->flags & TCS_LAUNCH_SHUFFLE) && shfl_ok) ? 1u : 0u;
-  PipeKey key{L->block[0], s.dimension == 3 ? L->block[1] : 1u, ch, lshift, batch ? 1u : 0u, epi, 0u, shfl};
+  // the ring form in tensor memory: on request (TCS_LAUNCH_TMEM), plain single-grid sweeps
+  const unsigned tm_cols = tmem_cols(s, L->block[0], s.dimension == 3 ? L->block[1] : 1u);
+  if ((L->flags & TCS_LAUNCH_TMEM) && (tm_cols == 0 || batch || epi || shfl))
+    return fail(TCS_ERR_UNSUPPORTED,
+                "pipe: the tensor-memory ring form needs a 3D Star stencil in Row order (FP64 or FP32), "
+                "cx*cy*sizeof/4 of 4, 8 or 16, a plain single-grid sweep");
+  const unsigned tmem = (L->flags & TCS_LAUNCH_TMEM) ? 1u : 0u;
+  PipeKey key{L->block[0], s.dimension == 3 ? L->block[1] : 1u, ch, lshift, batch ? 1u : 0u, epi, 0u, shfl, tmem};
   PipeMod* pm = nullptr;
   int rc = pipe_module(h, key, &pm);
   if (rc) return rc;
@@ -798,6 +823,26 @@ int resolve_pipe(tcs_stencil* h, const TcsGeo& g, const tcs_launch* L, Resolved&
   int occ = 0;
   TCS_CU(g_drv.OccMaxActive(&occ, pm->f, nthr, smem));
   if (occ < 1) return fail(TCS_ERR_UNSUPPORTED, "pipe kernel cannot be resident at this shape");
+  if (tmem) {
+    // Every resident CTA holds tm_cols tensor-memory columns: no more CTAs on an SM than its 512
+    // columns serve (an allocation beyond them would wait for another CTA to finish).  Where the
+    // registers and the ring would admit more, the dynamic shared memory grows until they do not.
+    const int cap = (int)(512u / tm_cols);
+    while (occ > cap) {
+      smem = std::min<unsigned>((unsigned)h->smem_optin, smem + 4096u);
+      {
+        std::lock_guard<std::mutex> lock(h->mu);
+        if ((int)smem > pm->smem_attr) {
+          TCS_CU(g_drv.FuncSetAttribute(pm->f, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, (int)smem));
+          pm->smem_attr = (int)smem;
+        }
+      }
+      TCS_CU(g_drv.OccMaxActive(&occ, pm->f, nthr, smem));
+      if (smem >= (unsigned)h->smem_optin && occ > cap)
+        return fail(TCS_ERR_UNSUPPORTED, "pipe: cannot limit the CTAs per SM to the tensor-memory columns");
+    }
+    if (occ < 1) return fail(TCS_ERR_UNSUPPORTED, "pipe kernel cannot be resident at this shape");
+  }
   const unsigned long long ex = g.x_lim > g.x0 ? g.x_lim - g.x0 : 0;
   const unsigned long long ey = g.y_lim - R;
   const unsigned ntx = std::max(1u, cdiv(ex, TX));
@@ -1660,7 +1705,7 @@ int tcs_precompile(const tcs_spec* spec, char* cubin_path, unsigned path_cap) {
 namespace {
 
 int precompile_pipe(const tcs_spec* spec, unsigned bx, unsigned by, unsigned chunk, bool batch,
-                    char* cubin_path, unsigned path_cap, unsigned epi = 0, unsigned shfl = 0) {
+                    char* cubin_path, unsigned path_cap, unsigned epi = 0, unsigned shfl = 0, unsigned tmem = 0) {
   int rc = validate(spec);
   if (rc) return rc;
   tcs_spec s = *spec;
@@ -1677,7 +1722,10 @@ int precompile_pipe(const tcs_spec* spec, unsigned bx, unsigned by, unsigned chu
     return fail(TCS_ERR_UNSUPPORTED, "pipe: epilogue not available for this precision");
   if (shfl && !(s.neighbourhood == TCS_STAR && (s.dimension == 2 || s.orientation == TCS_ROW) && bx % 32 == 0))
     return fail(TCS_ERR_UNSUPPORTED, "pipe: shuffled rows need a Star stencil in Row order and bx % 32 == 0");
-  PipeKey key{bx, s.dimension == 3 ? by : 1u, chunk, left_offset_of(s) % vec, batch ? 1u : 0u, epi, 0u, shfl ? 1u : 0u};
+  if (tmem && (tmem_cols(s, bx, s.dimension == 3 ? by : 1u) == 0 || batch || epi || shfl))
+    return fail(TCS_ERR_UNSUPPORTED, "pipe: the tensor-memory ring form does not apply to this instance");
+  PipeKey key{bx, s.dimension == 3 ? by : 1u, chunk, left_offset_of(s) % vec, batch ? 1u : 0u, epi, 0u, shfl ? 1u : 0u,
+              tmem ? 1u : 0u};
   std::vector<char> cubin;
   std::string path;
   rc = instantiate(s, &key, cubin, &path);
@@ -1747,7 +1795,8 @@ int tcs_precompile_pipe_epilogue(const tcs_spec* spec, unsigned bx, unsigned by,
 
 int tcs_precompile_pipe_flags(const tcs_spec* spec, unsigned bx, unsigned by, unsigned chunk, unsigned flags,
                               char* cubin_path, unsigned path_cap) {
-  return precompile_pipe(spec, bx, by, chunk, false, cubin_path, path_cap, 0, (flags & TCS_LAUNCH_SHUFFLE) ? 1u : 0u);
+  return precompile_pipe(spec, bx, by, chunk, false, cubin_path, path_cap, 0, (flags & TCS_LAUNCH_SHUFFLE) ? 1u : 0u,
+                         (flags & TCS_LAUNCH_TMEM) ? 1u : 0u);
 }
 
 int tcs_precompile_batch(const tcs_spec* spec, unsigned bx, unsigned by, unsigned chunk,

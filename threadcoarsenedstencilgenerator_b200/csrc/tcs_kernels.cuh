@@ -531,6 +531,29 @@ static_assert(!TCS_SHFL || (BX % 32 == 0 && SHAPE == 1 && (DIM == 2 || ORIENT ==
               "shuffled rows: Star stencils in Row order, block x extent a multiple of the warp");
 static_assert(CHP >= 1, "planes per chunk");
 static_assert(TXP % VEC == 0, "tile width must be a multiple of the 16-byte granule");
+
+// TCS_TMEM: the ring form of the Star pipeline (tcs::ring_step).  Each thread keeps, in tensor
+// memory, R entries of its own centre values (one input plane each) and R entries of output
+// accumulators whose in-plane cross is done, instead of 2R+1 output planes in registers: the
+// registers hold two output planes, so twice the warps fit on an SM.  A warp reaches the 32 TMEM
+// lanes of its quarter (warp % 4); warps w and w + 4k share the lanes and use column groups k.
+#ifndef TCS_TMEM
+#define TCS_TMEM 0
+#endif
+constexpr bool TMEM = TCS_TMEM != 0;
+constexpr int TM_W = NEP * (int)sizeof(T) / 4;         // 32-bit columns per ring entry
+constexpr int TM_THREAD_COLS = 2 * R * TM_W;           // R raw entries + R accumulator entries
+constexpr int TM_GROUPS = (BX * BY + 127) / 128;       // column groups (warps per lane quarter)
+constexpr int tm_cols() {
+  int n = 32;
+  while (n < TM_GROUPS * TM_THREAD_COLS) n *= 2;
+  return n;
+}
+constexpr int TM_COLS = tm_cols();                     // allocation: a power of two >= 32
+static_assert(!TMEM || (DIM == 3 && SHAPE == 1 && ORIENT == 0 && EPI == 0 && !COMP && !TCS_SHFL),
+              "the ring form is built for 3D Star stencils in Row order, plain epilogue");
+static_assert(!TMEM || TM_W == 4 || TM_W == 8 || TM_W == 16, "ring entries of 4, 8 or 16 columns");
+static_assert(!TMEM || TM_COLS <= 512, "ring exceeds the 512 tensor-memory columns of an SM");
 // Columns whose element index is even for every thread: the thread origin sits at ring column
 // LSHIFT + R + tx*CX and every row, plane and chunk starts on a 16-byte boundary, so with CX even
 // the pair (gx, gx+1) is 16-byte (8-byte for float) aligned exactly when LSHIFT + R + gx is even.
@@ -562,6 +585,111 @@ struct PipeRing {
     b = v.y;
   }
 };
+
+#if TCS_TMEM
+// tcgen05.ld / st of N consecutive 32-bit columns of this thread's TMEM lane (shape 32x32b).  The
+// wait takes the loaded registers as read-write operands, so no use of them moves above it.
+#define TCS_R4(a, o) "=r"(a[o + 0]), "=r"(a[o + 1]), "=r"(a[o + 2]), "=r"(a[o + 3])
+#define TCS_W4(a, o) "+r"(a[o + 0]), "+r"(a[o + 1]), "+r"(a[o + 2]), "+r"(a[o + 3])
+#define TCS_S4(a, o) "r"(a[o + 0]), "r"(a[o + 1]), "r"(a[o + 2]), "r"(a[o + 3])
+template <int N>
+__device__ __forceinline__ void tm_ld(tcs_u32 taddr, tcs_u32 (&r)[N]) {
+  if constexpr (N == 4) {
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0, %1, %2, %3}, [%4];" : TCS_R4(r, 0) : "r"(taddr) : "memory");
+  } else if constexpr (N == 8) {
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                 : TCS_R4(r, 0), TCS_R4(r, 4) : "r"(taddr) : "memory");
+  } else {
+    static_assert(N == 16, "4, 8 or 16 columns");
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15}, [%16];"
+        : TCS_R4(r, 0), TCS_R4(r, 4), TCS_R4(r, 8), TCS_R4(r, 12) : "r"(taddr) : "memory");
+  }
+}
+template <int N>
+__device__ __forceinline__ void tm_wait_ld(tcs_u32 (&r)[N]) {
+  if constexpr (N == 4) {
+    asm volatile("tcgen05.wait::ld.sync.aligned;" : TCS_W4(r, 0) :: "memory");
+  } else if constexpr (N == 8) {
+    asm volatile("tcgen05.wait::ld.sync.aligned;" : TCS_W4(r, 0), TCS_W4(r, 4) :: "memory");
+  } else {
+    asm volatile("tcgen05.wait::ld.sync.aligned;" : TCS_W4(r, 0), TCS_W4(r, 4), TCS_W4(r, 8), TCS_W4(r, 12) :: "memory");
+  }
+}
+template <int N>
+__device__ __forceinline__ void tm_st(tcs_u32 taddr, const tcs_u32 (&r)[N]) {
+  if constexpr (N == 4) {
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x4.b32 [%0], {%1, %2, %3, %4};" ::"r"(taddr), TCS_S4(r, 0) : "memory");
+  } else if constexpr (N == 8) {
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"r"(taddr),
+                 TCS_S4(r, 0), TCS_S4(r, 4) : "memory");
+  } else {
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15, %16};" ::"r"(taddr),
+        TCS_S4(r, 0), TCS_S4(r, 4), TCS_S4(r, 8), TCS_S4(r, 12) : "memory");
+  }
+}
+#undef TCS_R4
+#undef TCS_W4
+#undef TCS_S4
+__device__ __forceinline__ void tm_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
+
+// T values <-> 32-bit TMEM columns (a double is two columns: low word, high word).
+__device__ __forceinline__ void tm_pack(const T (&v)[NEP], tcs_u32 (&w)[TM_W]) {
+#pragma unroll
+  for (int e = 0; e < NEP; ++e) {
+    if constexpr (sizeof(T) == 8) {
+      w[2 * e] = (tcs_u32)__double2loint((double)v[e]);
+      w[2 * e + 1] = (tcs_u32)__double2hiint((double)v[e]);
+    } else {
+      w[e] = __float_as_uint((float)v[e]);
+    }
+  }
+}
+__device__ __forceinline__ void tm_unpack(const tcs_u32 (&w)[TM_W], T (&v)[NEP]) {
+#pragma unroll
+  for (int e = 0; e < NEP; ++e) {
+    if constexpr (sizeof(T) == 8)
+      v[e] = (T)__hiloint2double((int)w[2 * e + 1], (int)w[2 * e]);
+    else
+      v[e] = (T)__uint_as_float(w[e]);
+  }
+}
+
+// The two rings of one thread in tensor memory, addressed relative to input plane c (entry
+// e0 = c mod R): raw entries at columns [0, R*TM_W), accumulator entries at [R*TM_W, 2R*TM_W).
+struct TmemRing {
+  tcs_u32 base;  // this thread's lane quarter and column group
+  tcs_u32 e0;
+  __device__ __forceinline__ tcs_u32 raw_col(tcs_u32 i) const {
+    const tcs_u32 e = e0 + i;
+    return base + (e >= (tcs_u32)R ? e - R : e) * TM_W;
+  }
+  __device__ __forceinline__ void load_acc(PipeSlot& s) const {
+    tm_wait_st();  // the previous plane's stores are in tensor memory
+    tcs_u32 w[TM_W];
+    tm_ld<TM_W>(base + (R + e0) * TM_W, w);
+    tm_wait_ld<TM_W>(w);
+    tm_unpack(w, s.v);
+  }
+  template <int I>
+  __device__ __forceinline__ void load_raw(T (&v)[NEP]) const {
+    tcs_u32 w[TM_W];
+    tm_ld<TM_W>(raw_col(I), w);
+    tm_wait_ld<TM_W>(w);
+    tm_unpack(w, v);
+  }
+  __device__ __forceinline__ void store(const PipeSlot& s, const T (&v)[NEP]) const {
+    tcs_u32 a[TM_W], r[TM_W];
+    tm_pack(s.v, a);
+    tm_pack(v, r);
+    tm_st<TM_W>(base + (R + e0) * TM_W, a);
+    tm_st<TM_W>(base + e0 * TM_W, r);
+  }
+};
+#endif
 }  // namespace tcs
 
 struct TcsPipeGeo {
@@ -641,6 +769,7 @@ __device__ __forceinline__ void pipe_copy_chunk(const PipeGridView& G, tcs_u32 d
 // Per-CTA streaming state that survives from piece to piece.
 struct PipeState {
   tcs_u32 bars, ring_s, nslot, tid, gc;
+  tcs_u32 tm;  // TCS_TMEM: this thread's tensor-memory ring base
   T* ring;
   double nmax, nsum;  // epilogue 1: this thread's running defect norms
 };
@@ -726,7 +855,8 @@ __device__ __forceinline__ bool pipe_piece(const PipeGridView& G, tcs_u32 tile, 
   // compile-time constant without moving registers at the back-edge; otherwise one step per
   // iteration and the slots rotate by CHP at the back-edge.  The cycle is unrolled only while its
   // straight-line code stays near the size of a one-step body (about 2400 terms).
-  constexpr int U = (NP2 % CHP == 0 && TCS_CYCLE != 0 && NP2 * S * NEP <= 2400) ? NP2 / CHP : 1;
+  constexpr int U = (!TMEM && NP2 % CHP == 0 && TCS_CYCLE != 0 && NP2 * S * NEP <= 2400) ? NP2 / CHP : 1;
+  tcs_u32 tslot = 0;  // TCS_TMEM: ring entry of the current input plane (plane mod R)
   tcs_u32 cur_slot = gc % nslot;
   tcs_u32 cur_par = (gc / nslot) & 1u;
   T* optr = obase + ((tcs_i64)ms - 2 * R) * plane_g;
@@ -791,11 +921,20 @@ __device__ __forceinline__ bool pipe_piece(const PipeGridView& G, tcs_u32 tile, 
             }
           }
           const PipeRing ld{pc + t * PLANE};
+#if TCS_TMEM
+          PipeSlot ring_done;  // the output centred R planes back, complete after this plane
+          {
+            const TmemRing ring{st.tm, tslot};
+            ring_step(ld, ring, ring_done);
+            tslot = (tslot + 1u == (tcs_u32)R) ? 0u : tslot + 1u;
+          }
+#else
           auto slot = [&](auto kk) -> PipeSlot& {
             constexpr int k = decltype(kk)::value;
             return acc[((tc - k) % NP2 + NP2) % NP2];
           };
           pipe_plane(ld, slot);
+#endif
           const int op = (int)pi - 2 * R;
           if (EPI != 0 && lane_ok && op >= 0 && op < (int)nout) {
             constexpr T c = T(1) / T(S);
@@ -841,7 +980,11 @@ __device__ __forceinline__ bool pipe_piece(const PipeGridView& G, tcs_u32 tile, 
           }
           if (EPI == 0 && lane_ok && op >= 0 && op < (int)nout) {
             constexpr T c = T(1) / T(S);
+#if TCS_TMEM
+            PipeSlot& done = ring_done;
+#else
             PipeSlot& done = acc[((tc - 2 * R) % NP2 + NP2) % NP2];
+#endif
             T* orow = optr + (tcs_i64)t * plane_g;
             // Output x is R + leftOff + an even offset when CX is even: pairs are aligned when
             // R + LSHIFT is even (the shared-memory pair rule at gx = 0).
@@ -886,7 +1029,7 @@ __device__ __forceinline__ bool pipe_piece(const PipeGridView& G, tcs_u32 tile, 
       });
       // One step per iteration: re-align the register slots with the next chunk (slot m takes
       // what slot (m + CHP) held).
-      if constexpr (U == 1 && CHP % NP2 != 0) {
+      if constexpr (!TMEM && U == 1 && CHP % NP2 != 0) {
         PipeSlot tmp[NP2];
         static_for<0, NP2>([&](auto m) { tmp[decltype(m)::value] = acc[decltype(m)::value]; });
         static_for<0, NP2>([&](auto m) { acc[decltype(m)::value] = tmp[(decltype(m)::value + CHP) % NP2]; });
@@ -957,16 +1100,50 @@ extern "C" __global__ void __launch_bounds__(TCS_BX * ((TCS_DIM == 3) ? TCS_BY :
   G.aux_pair = (g.xdim % 2 == 0) && (reinterpret_cast<tcs_u64>(aux) % 16 == 0);
   if (G.use_tma && threadIdx.x == 0 && threadIdx.y == 0) tma_prefetch_map(&tmap);
   PipeState st = pipe_setup(g.nslot, G.use_tma);
+#if TCS_TMEM
+  // Warp 0 allocates the CTA's tensor-memory columns (the host limits the CTAs per SM so that
+  // their allocations fit the SM's 512 columns) and frees them when the CTA is done, on the
+  // error path too.
+  __shared__ tcs_u32 tm_base;
+  const tcs_u32 warp_id = st.tid >> 5;
+  if (warp_id == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(&tm_base)),
+                 "r"((tcs_u32)TM_COLS)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  st.tm = tm_base + ((32u * (warp_id & 3u)) << 16) + (warp_id >> 2) * (tcs_u32)TM_THREAD_COLS;
+#else
+  st.tm = 0;
+#endif
   PipeSlot acc[NP2];
   const tcs_u64 w_begin = (tcs_u64)blockIdx.x * g.per_cta;
   const tcs_u64 w_end = min(w_begin + g.per_cta, g.total);
+  bool ok = true;
   for (tcs_u64 w = w_begin; w < w_end;) {
     const tcs_u32 tile = (tcs_u32)(w / g.m);
     const tcs_u32 zs = (tcs_u32)(w % g.m);
     const tcs_u32 ze = (tcs_u32)min((tcs_u64)g.m, (tcs_u64)zs + (w_end - w));
     w += ze - zs;
-    if (!pipe_piece<false>(G, tile, zs, ze, st, acc)) return;
+    if (!pipe_piece<false>(G, tile, zs, ze, st, acc)) {
+      ok = false;
+      break;
+    }
   }
+#if TCS_TMEM
+  asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp_id == 0) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tm_base), "r"((tcs_u32)TM_COLS)
+                 : "memory");
+  }
+#endif
+  if (!ok) return;
   if constexpr (EPI == 1) {
     // this CTA's defect norms: shuffles within each warp, then one value per warp in shared memory
     __shared__ double red[2][32];

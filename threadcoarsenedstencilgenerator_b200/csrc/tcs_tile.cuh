@@ -522,6 +522,80 @@ __device__ __forceinline__ void load_row_shfl(const LD& ld, T (&v)[2 * R + CX]) 
 #endif
 }
 
+// In-plane cross of a Star stencil in Row order into the slot of the outputs centred on this
+// plane (DZ = 0): the column segments above (3D), the middle rows -- contiguous segments that
+// also hold the thread's own centre points, returned in cv -- and the column segments below.
+template <class LD, class SL>
+__device__ __forceinline__ void pipe_cross(const LD& ld, SL& s0, T (&cv)[NEP]) {
+  constexpr int NY = (DIM == 3) ? CY : 1;
+  if constexpr (DIM == 3) {
+    static_for<0, R>([&](auto i) {  // gy in [-R, 0): the thread's columns
+      constexpr int gy = decltype(i)::value - R;
+      T seg[CX];
+      load_row<gy, 0, CX>(ld, seg);
+      static_for<0, CX>([&](auto gx) { apply_slot<decltype(gx)::value, gy, 0>(s0, seg[decltype(gx)::value]); });
+    });
+  }
+  static_for<0, NY>([&](auto gyc) {  // middle rows: gx in [-R, R + CX)
+    constexpr int gy = decltype(gyc)::value;
+    T row[2 * R + CX];
+    load_row_shfl<gy>(ld, row);
+    static_for<0, CX>([&](auto ex) { cv[decltype(ex)::value + gy * CX] = row[R + decltype(ex)::value]; });
+    static_for<0, 2 * R + CX>([&](auto ix) {
+      apply_slot<decltype(ix)::value - R, gy, 0>(s0, row[decltype(ix)::value]);
+    });
+  });
+  if constexpr (DIM == 3) {
+    static_for<0, R>([&](auto i) {  // gy in [CY, CY + R)
+      constexpr int gy = CY + decltype(i)::value;
+      T seg[CX];
+      load_row<gy, 0, CX>(ld, seg);
+      static_for<0, CX>([&](auto gx) { apply_slot<decltype(gx)::value, gy, 0>(s0, seg[decltype(gx)::value]); });
+    });
+  }
+}
+
+// The march-axis arm term of each of the thread's outputs: own value v[e] of the plane at offset
+// DZ (!= 0) from the output's centre plane.
+template <int DZ, class SL>
+__device__ __forceinline__ void apply_own(SL& s, const T (&v)[NEP]) {
+  static_for<0, (DIM == 3) ? CY : 1>([&](auto ey) {
+    static_for<0, CX>([&](auto ex) {
+      apply_slot<decltype(ex)::value, decltype(ey)::value, DZ>(s, v[decltype(ex)::value + decltype(ey)::value * CX]);
+    });
+  });
+}
+
+// Ring form of the Star pipeline (3D, Row order; the kernel's TCS_TMEM variant).  Instead of
+// 2R+1 output planes in registers, a thread keeps two rings of R entries elsewhere (tensor memory
+// in the kernel): the own centre values of the last R input planes, and the accumulators of the
+// last R outputs whose in-plane cross is done.  For input plane c, `ring_step`
+//   * starts the output centred on c: its R lower arm terms from the own values of planes
+//     c-R .. c-1 (ring), then the cross of plane c -- the reference's per-output order;
+//   * finishes the output centred on c-R (accumulators from the ring): its R upper arm terms
+//     from planes c-R+1 .. c-1 (ring) and c (the centre values just read);
+//   * stores the new accumulators and plane c's own values into the ring entries just read.
+// RING provides load_acc(slot&), load_raw<i>(v) (own values of plane c-R+i) and
+// store(slot, v); its entries are addressed relative to plane c.
+template <class LD, class RING>
+__device__ __forceinline__ void ring_step(const LD& ld, RING& ring, PipeSlot& done) {
+  PipeSlot cur;
+  T v[NEP];
+  ring.load_acc(done);
+  ring.template load_raw<0>(v);
+  apply_own<-R>(cur, v);
+  static_for<1, R>([&](auto ii) {
+    constexpr int i = decltype(ii)::value;
+    ring.template load_raw<i>(v);
+    apply_own<i - R>(cur, v);
+    apply_own<i>(done, v);
+  });
+  T cv[NEP];
+  pipe_cross(ld, cur, cv);
+  apply_own<R>(done, cv);
+  ring.store(cur, cv);
+}
+
 // Apply input plane (offset DZ relative to pending outputs) held in shared memory to the 2R+1
 // pipeline slots.  `ld` reads the plane at in-plane offsets from the thread origin (see load_row);
 // `slot(ic<k>)` returns the accumulators of the output at march-axis offset k - R.
@@ -617,32 +691,7 @@ __device__ __forceinline__ void pipe_plane(const LD& ld, SLOTS&& slot) {
     auto& s0 = slot(ic<R>{});
     T cv[NEP];
     if constexpr (ORIENT == 0 || DIM == 2) {
-      // Row order: the middle rows are contiguous segments that also hold the centre points.
-      if constexpr (DIM == 3) {
-        static_for<0, R>([&](auto i) {  // gy in [-R, 0): the thread's columns
-          constexpr int gy = decltype(i)::value - R;
-          T seg[CX];
-          load_row<gy, 0, CX>(ld, seg);
-          static_for<0, CX>([&](auto gx) { apply_slot<decltype(gx)::value, gy, 0>(s0, seg[decltype(gx)::value]); });
-        });
-      }
-      static_for<0, NY>([&](auto gyc) {  // middle rows: gx in [-R, R + CX)
-        constexpr int gy = decltype(gyc)::value;
-        T row[2 * R + CX];
-        load_row_shfl<gy>(ld, row);
-        static_for<0, CX>([&](auto ex) { cv[decltype(ex)::value + gy * CX] = row[R + decltype(ex)::value]; });
-        static_for<0, 2 * R + CX>([&](auto ix) {
-          apply_slot<decltype(ix)::value - R, gy, 0>(s0, row[decltype(ix)::value]);
-        });
-      });
-      if constexpr (DIM == 3) {
-        static_for<0, R>([&](auto i) {  // gy in [CY, CY + R)
-          constexpr int gy = CY + decltype(i)::value;
-          T seg[CX];
-          load_row<gy, 0, CX>(ld, seg);
-          static_for<0, CX>([&](auto gx) { apply_slot<decltype(gx)::value, gy, 0>(s0, seg[decltype(gx)::value]); });
-        });
-      }
+      pipe_cross(ld, s0, cv);
     } else {
       // 3D Column order: columns of the cross, point by point.
       static_for<0, NY>([&](auto ey) {

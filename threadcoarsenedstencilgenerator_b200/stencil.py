@@ -43,6 +43,7 @@ class Launch:
     depth: int = 0                  # march/pipe: chunks in flight (0 = auto)
     chunk: int = 0                  # pipe: planes per ring chunk (0 = auto)
     shuffle: bool | None = None     # pipe, Star: middle rows through warp shuffles (None: planner's choice)
+    tmem: bool = False              # pipe, 3D Star Row: the ring form in tensor memory
 
     _VARIANTS = {"auto": _lib.VARIANT_AUTO, "direct": _lib.VARIANT_DIRECT, "march": _lib.VARIANT_MARCH,
                  "pipe": _lib.VARIANT_PIPE}
@@ -51,6 +52,8 @@ class Launch:
         b = tuple(self.block) + (1,) * (3 - len(self.block))
         g = tuple(self.grid_blocks) + (0,) * (3 - len(self.grid_blocks))
         flags = 0 if self.shuffle is None else (_lib.LAUNCH_SHUFFLE if self.shuffle else _lib.LAUNCH_NO_SHUFFLE)
+        if self.tmem:
+            flags |= _lib.LAUNCH_TMEM
         return _lib.CLaunch(_lib.U3(*b), _lib.U3(*g), self._VARIANTS[self.variant], int(self.segments),
                             int(self.depth), int(self.chunk), flags)
 
@@ -311,13 +314,14 @@ def precompile(spec: StencilSpec) -> str:
     return buf.value.decode()
 
 
-def precompile_pipe(spec: StencilSpec, block, chunk: int, shuffle: bool = False) -> str:
+def precompile_pipe(spec: StencilSpec, block, chunk: int, shuffle: bool = False, tmem: bool = False) -> str:
     """Instantiate the pipelined sweep of ``spec`` for one launch shape into the cubin cache."""
     buf = ctypes.create_string_buffer(1024)
     b = tuple(block) + (1,) * (3 - len(block))
-    if shuffle:
+    if shuffle or tmem:
+        flags = (_lib.LAUNCH_SHUFFLE if shuffle else 0) | (_lib.LAUNCH_TMEM if tmem else 0)
         _lib.check(_lib.load().tcs_precompile_pipe_flags(ctypes.byref(spec.to_c()), b[0], b[1], int(chunk),
-                                                         _lib.LAUNCH_SHUFFLE, buf, 1024))
+                                                         flags, buf, 1024))
     else:
         _lib.check(_lib.load().tcs_precompile_pipe(ctypes.byref(spec.to_c()), b[0], b[1], int(chunk), buf, 1024))
     return buf.value.decode()
