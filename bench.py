@@ -1027,21 +1027,22 @@ def run_case(args) -> dict:
     ms = e0.elapsed_time(e1)  # CUDA events around the --steps sweeps after the warm-up
     return {"case": args.workload, "grid": list(grid), "points": geom.interior_points, "sweeps": args.steps,
             "kernel": args.case, "variant": plan.variant, "block": list(plan.block), "chunk": plan.chunk,
-            "coarsening": [spec.cx, spec.cy, spec.cz], "shuffle": bool(launch.shuffle),
+            "coarsening": [spec.cx, spec.cy, spec.cz], "shuffle": bool(launch.shuffle), "tmem": bool(launch.tmem),
             "glups": geom.interior_points * args.steps / (ms / 1e3) / 1e9 if ms > 0 else None}
 
 
 def case_launch(spec, text: str):
-    """(spec, Launch) of a pipelined launch written cx,cy,bx,by,chunk[,shuffle]: the profiling case
-    of one point of the launch space instead of the tuned launch."""
+    """(spec, Launch) of a pipelined launch written cx,cy,bx,by,chunk[,shuffle[,tmem]]: the profiling
+    case of one point of the launch space instead of the tuned launch."""
     from threadcoarsenedstencilgenerator_b200.stencil import Launch
 
     v = [int(t) for t in text.split(",")]
-    if len(v) not in (5, 6):
-        raise SystemExit("--case-launch wants cx,cy,bx,by,chunk[,shuffle]")
+    if len(v) not in (5, 6, 7):
+        raise SystemExit("--case-launch wants cx,cy,bx,by,chunk[,shuffle[,tmem]]")
     cx, cy, bx, by, ch = v[:5]
     spec = spec.replace(cx=cx, cy=cy, cz=1) if spec.dimension == 3 else spec.replace(cx=cx, cy=1)
-    return spec, Launch(block=(bx, by, 1), variant="pipe", chunk=ch, shuffle=bool(v[5]) if len(v) == 6 else False)
+    return spec, Launch(block=(bx, by, 1), variant="pipe", chunk=ch, shuffle=bool(v[5]) if len(v) > 5 else False,
+                        tmem=bool(v[6]) if len(v) > 6 else False)
 
 
 def check_world(gpus: int, world: int) -> str | None:
@@ -1077,8 +1078,8 @@ def main(argv=None) -> int:
     ap.add_argument("--case", default="sweep", choices=["sweep", "tensor-cores", "temporal"],
                     help="profiling case: which kernel")
     ap.add_argument("--case-precision", default="f64", choices=["f64", "f32"], help="profiling case: precision")
-    ap.add_argument("--case-launch", default="", help="profiling case: pipelined launch cx,cy,bx,by,chunk[,shuffle] "
-                    "instead of the tuned one")
+    ap.add_argument("--case-launch", default="", help="profiling case: pipelined launch "
+                    "cx,cy,bx,by,chunk[,shuffle[,tmem]] instead of the tuned one")
     args = ap.parse_args(argv)
     args.warmup = max(3, args.warmup)
     err = check_world(args.gpus, _dist()[0])

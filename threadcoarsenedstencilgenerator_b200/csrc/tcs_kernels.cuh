@@ -854,8 +854,10 @@ __device__ __forceinline__ bool pipe_piece(const PipeGridView& G, tcs_u32 tile, 
   // U = (2R+1)/CHP chunk steps per iteration, a whole cycle of slots, so every slot index stays a
   // compile-time constant without moving registers at the back-edge; otherwise one step per
   // iteration and the slots rotate by CHP at the back-edge.  The cycle is unrolled only while its
-  // straight-line code stays near the size of a one-step body (about 2400 terms).
-  constexpr int U = (!TMEM && NP2 % CHP == 0 && TCS_CYCLE != 0 && NP2 * S * NEP <= 2400) ? NP2 / CHP : 1;
+  // straight-line code stays near the size of a one-step body (about 2400 terms) and spans at most
+  // three chunk steps (more ring waits in one body measured slower than the rotation).
+  constexpr int U = (!TMEM && NP2 % CHP == 0 && TCS_CYCLE != 0 && NP2 * S * NEP <= 2400 && NP2 / CHP <= 3)
+                        ? NP2 / CHP : 1;
   tcs_u32 tslot = 0;  // TCS_TMEM: ring entry of the current input plane (plane mod R)
   tcs_u32 cur_slot = gc % nslot;
   tcs_u32 cur_par = (gc / nslot) & 1u;
