@@ -102,7 +102,7 @@ typedef struct tcs_launch {
 #define TCS_LAUNCH_NO_SHUFFLE 2u
 /* tcs_launch.flags: the pipelined sweep of a 3D Star stencil in Row order in its ring form: own
  * centre values and finished crosses in two R-entry rings in tensor memory, two output planes in
- * registers (plain single-grid sweeps; cx*cy*sizeof(element)/4 of 4, 8 or 16). */
+ * registers (plain single-grid sweeps; cx*cy*sizeof(element)/4 of 4, 8, 16 or 32). */
 #define TCS_LAUNCH_TMEM 4u
 
 /* Resolved launch of one sweep (what tcs_update_grid will run). */

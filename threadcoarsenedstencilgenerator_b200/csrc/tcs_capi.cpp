@@ -227,14 +227,14 @@ struct PipeKey {
 };
 
 // The ring form (TCS_TMEM, tcs_kernels.cuh): 3D Star stencils in Row order, FP64 or FP32, plain
-// epilogue, ring entries of 4, 8 or 16 columns, blocks of whole warps.  Its tensor-memory columns per CTA (the
+// epilogue, ring entries of 4, 8, 16 or 32 columns, blocks of whole warps.  Its tensor-memory columns per CTA (the
 // allocation, a power of two) or 0 when the form does not apply.
 unsigned tmem_cols(const tcs_spec& s, unsigned bx, unsigned by) {
   if (s.dimension != 3 || s.neighbourhood != TCS_STAR || s.orientation != TCS_ROW || s.precision == TCS_F32C)
     return 0;
   if ((bx * by) % 32u != 0) return 0;  // tensor-memory loads and stores are whole-warp instructions
   const unsigned w = (unsigned)(s.cx * s.cy) * (s.precision == TCS_F64 ? 2u : 1u);
-  if (w != 4 && w != 8 && w != 16) return 0;
+  if (w != 4 && w != 8 && w != 16 && w != 32) return 0;
   const unsigned groups = (bx * by + 127u) / 128u;
   const unsigned need = groups * 2u * (unsigned)s.range * w;
   unsigned n = 32;
@@ -774,7 +774,7 @@ int resolve_pipe(tcs_stencil* h, const TcsGeo& g, const tcs_launch* L, Resolved&
   if ((L->flags & TCS_LAUNCH_TMEM) && (tm_cols == 0 || batch || epi || shfl))
     return fail(TCS_ERR_UNSUPPORTED,
                 "pipe: the tensor-memory ring form needs a 3D Star stencil in Row order (FP64 or FP32), "
-                "cx*cy*sizeof/4 of 4, 8 or 16, a plain single-grid sweep");
+                "cx*cy*sizeof/4 of 4, 8, 16 or 32, a plain single-grid sweep");
   const unsigned tmem = (L->flags & TCS_LAUNCH_TMEM) ? 1u : 0u;
   PipeKey key{L->block[0], s.dimension == 3 ? L->block[1] : 1u, ch, lshift, batch ? 1u : 0u, epi, 0u, shfl, tmem};
   PipeMod* pm = nullptr;

@@ -552,7 +552,7 @@ constexpr int tm_cols() {
 constexpr int TM_COLS = tm_cols();                     // allocation: a power of two >= 32
 static_assert(!TMEM || (DIM == 3 && SHAPE == 1 && ORIENT == 0 && EPI == 0 && !COMP && !TCS_SHFL),
               "the ring form is built for 3D Star stencils in Row order, plain epilogue");
-static_assert(!TMEM || TM_W == 4 || TM_W == 8 || TM_W == 16, "ring entries of 4, 8 or 16 columns");
+static_assert(!TMEM || TM_W == 4 || TM_W == 8 || TM_W == 16 || TM_W == 32, "ring entries of 4 to 32 columns");
 static_assert(!TMEM || TM_COLS <= 512, "ring exceeds the 512 tensor-memory columns of an SM");
 // Columns whose element index is even for every thread: the thread origin sits at ring column
 // LSHIFT + R + tx*CX and every row, plane and chunk starts on a 16-byte boundary, so with CX even
@@ -599,12 +599,20 @@ __device__ __forceinline__ void tm_ld(tcs_u32 taddr, tcs_u32 (&r)[N]) {
   } else if constexpr (N == 8) {
     asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
                  : TCS_R4(r, 0), TCS_R4(r, 4) : "r"(taddr) : "memory");
-  } else {
-    static_assert(N == 16, "4, 8 or 16 columns");
+  } else if constexpr (N == 16) {
     asm volatile(
         "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
         "%15}, [%16];"
         : TCS_R4(r, 0), TCS_R4(r, 4), TCS_R4(r, 8), TCS_R4(r, 12) : "r"(taddr) : "memory");
+  } else {
+    static_assert(N == 32, "4, 8, 16 or 32 columns");
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+        : TCS_R4(r, 0), TCS_R4(r, 4), TCS_R4(r, 8), TCS_R4(r, 12), TCS_R4(r, 16), TCS_R4(r, 20), TCS_R4(r, 24),
+          TCS_R4(r, 28)
+        : "r"(taddr)
+        : "memory");
   }
 }
 template <int N>
@@ -613,8 +621,12 @@ __device__ __forceinline__ void tm_wait_ld(tcs_u32 (&r)[N]) {
     asm volatile("tcgen05.wait::ld.sync.aligned;" : TCS_W4(r, 0) :: "memory");
   } else if constexpr (N == 8) {
     asm volatile("tcgen05.wait::ld.sync.aligned;" : TCS_W4(r, 0), TCS_W4(r, 4) :: "memory");
-  } else {
+  } else if constexpr (N == 16) {
     asm volatile("tcgen05.wait::ld.sync.aligned;" : TCS_W4(r, 0), TCS_W4(r, 4), TCS_W4(r, 8), TCS_W4(r, 12) :: "memory");
+  } else {
+    asm volatile("tcgen05.wait::ld.sync.aligned;"
+                 : TCS_W4(r, 0), TCS_W4(r, 4), TCS_W4(r, 8), TCS_W4(r, 12), TCS_W4(r, 16), TCS_W4(r, 20),
+                   TCS_W4(r, 24), TCS_W4(r, 28)::"memory");
   }
 }
 template <int N>
@@ -624,11 +636,18 @@ __device__ __forceinline__ void tm_st(tcs_u32 taddr, const tcs_u32 (&r)[N]) {
   } else if constexpr (N == 8) {
     asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"r"(taddr),
                  TCS_S4(r, 0), TCS_S4(r, 4) : "memory");
-  } else {
+  } else if constexpr (N == 16) {
     asm volatile(
         "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
         "%15, %16};" ::"r"(taddr),
         TCS_S4(r, 0), TCS_S4(r, 4), TCS_S4(r, 8), TCS_S4(r, 12) : "memory");
+  } else {
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31, %32};" ::"r"(taddr),
+        TCS_S4(r, 0), TCS_S4(r, 4), TCS_S4(r, 8), TCS_S4(r, 12), TCS_S4(r, 16), TCS_S4(r, 20), TCS_S4(r, 24),
+        TCS_S4(r, 28)
+        : "memory");
   }
 }
 #undef TCS_R4
