@@ -100,10 +100,14 @@ struct HostRing {
   tcs::PipeSlot* acc;
   long long c;  // current input plane (piece-relative)
   int entry(long long p) const { return (int)(((p % tcs::R) + tcs::R) % tcs::R); }
-  void load_acc(tcs::PipeSlot& s) const { s = acc[entry(c - tcs::R)]; }
+  void load_first(tcs::PipeSlot& s, T (&v)[tcs::NEP]) const {
+    s = acc[entry(c - tcs::R)];
+    std::memcpy(v, raw[entry(c - tcs::R)], sizeof(v));
+  }
   template <int I>
-  void load_raw(T (&v)[tcs::NEP]) const {
-    std::memcpy(v, raw[entry(c - tcs::R + I)], sizeof(v));
+  void load_two(T (&a)[tcs::NEP], T (&b)[tcs::NEP]) const {
+    std::memcpy(a, raw[entry(c - tcs::R + I)], sizeof(a));
+    if (I + 1 < tcs::R) std::memcpy(b, raw[entry(c - tcs::R + I + 1)], sizeof(b));
   }
   void store(const tcs::PipeSlot& s, const T (&v)[tcs::NEP]) {
     acc[entry(c)] = s;

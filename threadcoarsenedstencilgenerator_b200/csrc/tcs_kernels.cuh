@@ -588,22 +588,24 @@ struct PipeRing {
 
 #if TCS_TMEM
 // tcgen05.ld / st of N consecutive 32-bit columns of this thread's TMEM lane (shape 32x32b).  The
-// wait takes the loaded registers as read-write operands, so no use of them moves above it.
+// wait takes the loaded registers as read-write operands, so no use of them moves above it.  The
+// statements are volatile (kept in program order among themselves) without a memory clobber:
+// they touch no generic memory, and shared-memory loads of the plane may be scheduled across them.
 #define TCS_R4(a, o) "=r"(a[o + 0]), "=r"(a[o + 1]), "=r"(a[o + 2]), "=r"(a[o + 3])
 #define TCS_W4(a, o) "+r"(a[o + 0]), "+r"(a[o + 1]), "+r"(a[o + 2]), "+r"(a[o + 3])
 #define TCS_S4(a, o) "r"(a[o + 0]), "r"(a[o + 1]), "r"(a[o + 2]), "r"(a[o + 3])
 template <int N>
 __device__ __forceinline__ void tm_ld(tcs_u32 taddr, tcs_u32 (&r)[N]) {
   if constexpr (N == 4) {
-    asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0, %1, %2, %3}, [%4];" : TCS_R4(r, 0) : "r"(taddr) : "memory");
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0, %1, %2, %3}, [%4];" : TCS_R4(r, 0) : "r"(taddr));
   } else if constexpr (N == 8) {
     asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
-                 : TCS_R4(r, 0), TCS_R4(r, 4) : "r"(taddr) : "memory");
+                 : TCS_R4(r, 0), TCS_R4(r, 4) : "r"(taddr));
   } else if constexpr (N == 16) {
     asm volatile(
         "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
         "%15}, [%16];"
-        : TCS_R4(r, 0), TCS_R4(r, 4), TCS_R4(r, 8), TCS_R4(r, 12) : "r"(taddr) : "memory");
+        : TCS_R4(r, 0), TCS_R4(r, 4), TCS_R4(r, 8), TCS_R4(r, 12) : "r"(taddr));
   } else {
     static_assert(N == 32, "4, 8, 16 or 32 columns");
     asm volatile(
@@ -611,49 +613,52 @@ __device__ __forceinline__ void tm_ld(tcs_u32 taddr, tcs_u32 (&r)[N]) {
         "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
         : TCS_R4(r, 0), TCS_R4(r, 4), TCS_R4(r, 8), TCS_R4(r, 12), TCS_R4(r, 16), TCS_R4(r, 20), TCS_R4(r, 24),
           TCS_R4(r, 28)
-        : "r"(taddr)
-        : "memory");
+        : "r"(taddr));
   }
 }
 template <int N>
 __device__ __forceinline__ void tm_wait_ld(tcs_u32 (&r)[N]) {
   if constexpr (N == 4) {
-    asm volatile("tcgen05.wait::ld.sync.aligned;" : TCS_W4(r, 0) :: "memory");
+    asm volatile("tcgen05.wait::ld.sync.aligned;" : TCS_W4(r, 0));
   } else if constexpr (N == 8) {
-    asm volatile("tcgen05.wait::ld.sync.aligned;" : TCS_W4(r, 0), TCS_W4(r, 4) :: "memory");
+    asm volatile("tcgen05.wait::ld.sync.aligned;" : TCS_W4(r, 0), TCS_W4(r, 4));
   } else if constexpr (N == 16) {
-    asm volatile("tcgen05.wait::ld.sync.aligned;" : TCS_W4(r, 0), TCS_W4(r, 4), TCS_W4(r, 8), TCS_W4(r, 12) :: "memory");
+    asm volatile("tcgen05.wait::ld.sync.aligned;" : TCS_W4(r, 0), TCS_W4(r, 4), TCS_W4(r, 8), TCS_W4(r, 12));
   } else {
     asm volatile("tcgen05.wait::ld.sync.aligned;"
                  : TCS_W4(r, 0), TCS_W4(r, 4), TCS_W4(r, 8), TCS_W4(r, 12), TCS_W4(r, 16), TCS_W4(r, 20),
-                   TCS_W4(r, 24), TCS_W4(r, 28)::"memory");
+                   TCS_W4(r, 24), TCS_W4(r, 28));
   }
+}
+template <int N>
+__device__ __forceinline__ void tm_wait_ld2(tcs_u32 (&a)[N], tcs_u32 (&b)[N]) {
+  tm_wait_ld<N>(a);
+  tm_wait_ld<N>(b);  // nothing left in flight: returns at once, orders b's uses after the wait
 }
 template <int N>
 __device__ __forceinline__ void tm_st(tcs_u32 taddr, const tcs_u32 (&r)[N]) {
   if constexpr (N == 4) {
-    asm volatile("tcgen05.st.sync.aligned.32x32b.x4.b32 [%0], {%1, %2, %3, %4};" ::"r"(taddr), TCS_S4(r, 0) : "memory");
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x4.b32 [%0], {%1, %2, %3, %4};" ::"r"(taddr), TCS_S4(r, 0));
   } else if constexpr (N == 8) {
     asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"r"(taddr),
-                 TCS_S4(r, 0), TCS_S4(r, 4) : "memory");
+                 TCS_S4(r, 0), TCS_S4(r, 4));
   } else if constexpr (N == 16) {
     asm volatile(
         "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
         "%15, %16};" ::"r"(taddr),
-        TCS_S4(r, 0), TCS_S4(r, 4), TCS_S4(r, 8), TCS_S4(r, 12) : "memory");
+        TCS_S4(r, 0), TCS_S4(r, 4), TCS_S4(r, 8), TCS_S4(r, 12));
   } else {
     asm volatile(
         "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
         "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31, %32};" ::"r"(taddr),
         TCS_S4(r, 0), TCS_S4(r, 4), TCS_S4(r, 8), TCS_S4(r, 12), TCS_S4(r, 16), TCS_S4(r, 20), TCS_S4(r, 24),
-        TCS_S4(r, 28)
-        : "memory");
+        TCS_S4(r, 28));
   }
 }
 #undef TCS_R4
 #undef TCS_W4
 #undef TCS_S4
-__device__ __forceinline__ void tm_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
+__device__ __forceinline__ void tm_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;"); }
 
 // T values <-> 32-bit TMEM columns (a double is two columns: low word, high word).
 __device__ __forceinline__ void tm_pack(const T (&v)[NEP], tcs_u32 (&w)[TM_W]) {
@@ -686,19 +691,27 @@ struct TmemRing {
     const tcs_u32 e = e0 + i;
     return base + (e >= (tcs_u32)R ? e - R : e) * TM_W;
   }
-  __device__ __forceinline__ void load_acc(PipeSlot& s) const {
+  __device__ __forceinline__ void load_first(PipeSlot& s, T (&v)[NEP]) const {
     tm_wait_st();  // the previous plane's stores are in tensor memory
-    tcs_u32 w[TM_W];
+    tcs_u32 w[TM_W], x[TM_W];
     tm_ld<TM_W>(base + (R + e0) * TM_W, w);
-    tm_wait_ld<TM_W>(w);
+    tm_ld<TM_W>(raw_col(0), x);
+    tm_wait_ld2<TM_W>(w, x);
     tm_unpack(w, s.v);
+    tm_unpack(x, v);
   }
   template <int I>
-  __device__ __forceinline__ void load_raw(T (&v)[NEP]) const {
-    tcs_u32 w[TM_W];
+  __device__ __forceinline__ void load_two(T (&a)[NEP], T (&b)[NEP]) const {
+    tcs_u32 w[TM_W], x[TM_W];
     tm_ld<TM_W>(raw_col(I), w);
-    tm_wait_ld<TM_W>(w);
-    tm_unpack(w, v);
+    if constexpr (I + 1 < R) {
+      tm_ld<TM_W>(raw_col(I + 1), x);
+      tm_wait_ld2<TM_W>(w, x);
+      tm_unpack(x, b);
+    } else {
+      tm_wait_ld<TM_W>(w);
+    }
+    tm_unpack(w, a);
   }
   __device__ __forceinline__ void store(const PipeSlot& s, const T (&v)[NEP]) const {
     tcs_u32 a[TM_W], r[TM_W];

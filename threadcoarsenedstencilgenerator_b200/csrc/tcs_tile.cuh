@@ -575,20 +575,28 @@ __device__ __forceinline__ void apply_own(SL& s, const T (&v)[NEP]) {
 //   * finishes the output centred on c-R (accumulators from the ring): its R upper arm terms
 //     from planes c-R+1 .. c-1 (ring) and c (the centre values just read);
 //   * stores the new accumulators and plane c's own values into the ring entries just read.
-// RING provides load_acc(slot&), load_raw<i>(v) (own values of plane c-R+i) and
-// store(slot, v); its entries are addressed relative to plane c.
+// RING provides load_first(slot&, v) (the accumulators of the output centred on c-R and the own
+// values of plane c-R), load_two<i>(a, b) (own values of planes c-R+i and c-R+i+1; b only when
+// i+1 < R) and store(slot, v); its entries are addressed relative to plane c.  Entries come in
+// pairs so that the kernel waits for tensor memory once per two entries.
 template <class LD, class RING>
 __device__ __forceinline__ void ring_step(const LD& ld, RING& ring, PipeSlot& done) {
   PipeSlot cur;
-  T v[NEP];
-  ring.load_acc(done);
-  ring.template load_raw<0>(v);
-  apply_own<-R>(cur, v);
-  static_for<1, R>([&](auto ii) {
-    constexpr int i = decltype(ii)::value;
-    ring.template load_raw<i>(v);
-    apply_own<i - R>(cur, v);
-    apply_own<i>(done, v);
+  {
+    T v[NEP];
+    ring.load_first(done, v);
+    apply_own<-R>(cur, v);
+  }
+  static_for<0, R / 2>([&](auto pp) {
+    constexpr int i = 1 + 2 * decltype(pp)::value;  // entries i and i+1 (i+1 < R unless R is even)
+    T a[NEP], b[NEP];
+    ring.template load_two<i>(a, b);
+    apply_own<i - R>(cur, a);
+    apply_own<i>(done, a);
+    if constexpr (i + 1 < R) {
+      apply_own<i + 1 - R>(cur, b);
+      apply_own<i + 1>(done, b);
+    }
   });
   T cv[NEP];
   pipe_cross(ld, cur, cv);
