@@ -26,8 +26,10 @@ from concurrent.futures import ThreadPoolExecutor
 from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
-REF_ROOT = Path(os.environ.get("TCS_REFERENCE_ROOT", "/root/reference"))
-REF_CUDA = REF_ROOT / "cuda"
+# The reference tree is named by TCS_REFERENCE_ROOT (or --reference-root): no default, so nothing
+# here reads a fixed path; without it the recipe builds nothing.
+REF_ROOT = Path(os.environ["TCS_REFERENCE_ROOT"]) if os.environ.get("TCS_REFERENCE_ROOT") else None
+REF_CUDA = REF_ROOT / "cuda" if REF_ROOT else None
 OUT = HERE / "_ref"
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
@@ -35,8 +37,15 @@ sys.path.insert(0, str(HERE.parent))
 from oracle.ref_configs import ALL, key  # noqa: E402
 
 
+def set_reference_root(path) -> None:
+    """Point the recipe at a reference tree (what TCS_REFERENCE_ROOT does)."""
+    global REF_ROOT, REF_CUDA
+    REF_ROOT = Path(path)
+    REF_CUDA = REF_ROOT / "cuda"
+
+
 def reference_available() -> bool:
-    return (REF_CUDA / "generate2DStencil_cuda.py").exists()
+    return REF_CUDA is not None and (REF_CUDA / "generate2DStencil_cuda.py").exists()
 
 
 def _generator_text(dim: int) -> str:
@@ -141,7 +150,10 @@ if __name__ == "__main__":
     ap = argparse.ArgumentParser()
     ap.add_argument("--shipped", action="store_true", help="also build with the reference Makefile flags")
     ap.add_argument("-j", type=int, default=8)
+    ap.add_argument("--reference-root", help="the reference tree (default: $TCS_REFERENCE_ROOT)")
     a = ap.parse_args()
+    if a.reference_root:
+        set_reference_root(a.reference_root)
     if not reference_available():
         print("reference tree not found at %s; nothing built" % REF_ROOT)
         sys.exit(0)

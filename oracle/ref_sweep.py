@@ -17,7 +17,7 @@ over coarsening factors 1..4 per axis and all block shapes.  This recipe
 This measures the reference, to choose the reference shape that bench.py times beside the
 engine.  It loads only oracle/_ref libraries and the block enumeration's plain-Python file.
 
-    python oracle/ref_sweep.py build
+    TCS_REFERENCE_ROOT=<reference tree> python oracle/ref_sweep.py build
     python oracle/ref_sweep.py run --out gpurun_out/ref_sweep.jsonl
 """
 
