@@ -1032,17 +1032,18 @@ def run_case(args) -> dict:
 
 
 def case_launch(spec, text: str):
-    """(spec, Launch) of a pipelined launch written cx,cy,bx,by,chunk[,shuffle[,tmem]]: the profiling
-    case of one point of the launch space instead of the tuned launch."""
+    """(spec, Launch) of a pipelined launch written cx,cy,bx,by,chunk[,shuffle[,tmem[,ctas]]]: the
+    profiling case of one point of the launch space instead of the tuned launch (ctas: the number
+    of persistent CTAs, 0 = one wave)."""
     from threadcoarsenedstencilgenerator_b200.stencil import Launch
 
     v = [int(t) for t in text.split(",")]
-    if len(v) not in (5, 6, 7):
-        raise SystemExit("--case-launch wants cx,cy,bx,by,chunk[,shuffle[,tmem]]")
+    if len(v) not in (5, 6, 7, 8):
+        raise SystemExit("--case-launch wants cx,cy,bx,by,chunk[,shuffle[,tmem[,ctas]]]")
     cx, cy, bx, by, ch = v[:5]
     spec = spec.replace(cx=cx, cy=cy, cz=1) if spec.dimension == 3 else spec.replace(cx=cx, cy=1)
     return spec, Launch(block=(bx, by, 1), variant="pipe", chunk=ch, shuffle=bool(v[5]) if len(v) > 5 else False,
-                        tmem=bool(v[6]) if len(v) > 6 else False)
+                        tmem=bool(v[6]) if len(v) > 6 else False, segments=v[7] if len(v) > 7 else 0)
 
 
 def check_world(gpus: int, world: int) -> str | None:
@@ -1079,7 +1080,7 @@ def main(argv=None) -> int:
                     help="profiling case: which kernel")
     ap.add_argument("--case-precision", default="f64", choices=["f64", "f32"], help="profiling case: precision")
     ap.add_argument("--case-launch", default="", help="profiling case: pipelined launch "
-                    "cx,cy,bx,by,chunk[,shuffle[,tmem]] instead of the tuned one")
+                    "cx,cy,bx,by,chunk[,shuffle[,tmem[,ctas]]] instead of the tuned one")
     args = ap.parse_args(argv)
     args.warmup = max(3, args.warmup)
     err = check_world(args.gpus, _dist()[0])
