@@ -104,6 +104,10 @@ typedef struct tcs_launch {
  * centre values and finished crosses in two R-entry rings in tensor memory, two output planes in
  * registers (plain single-grid sweeps; cx*cy*sizeof(element)/4 of 4, 8, 16 or 32). */
 #define TCS_LAUNCH_TMEM 4u
+/* tcs_launch.flags: the pipelined sweep's persistent CTAs each take one tile column (or an equal
+ * part of one): the tiles sweep the march axis in step, so neighbouring tiles' shared halo rows
+ * are read from L2 (CTA count = tiles x the largest k the resident CTAs allow). */
+#define TCS_LAUNCH_LOCKSTEP 8u
 
 /* Resolved launch of one sweep (what tcs_update_grid will run). */
 typedef struct tcs_plan {

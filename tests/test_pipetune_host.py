@@ -70,18 +70,25 @@ def test_tuner_times_top_k_or_falls_back(monkeypatch, scenario):
         timings[cands[3]] = 300.0  # a much faster candidate the model ranks 4th: large prediction error
     timed = []
 
-    def fake_time(b, grid, cand, mask, bufs, sweeps=3):
-        timed.append(cand)
-        return timings[cand]
+    def fake_time(b, grid, cand, mask, bufs, sweeps=3, form=(0, 0)):
+        timed.append((cand, form))
+        # the lockstep ring form is faster, the other non-default forms slower
+        return timings[cand] + {(0, 0): 0.0, (1, 1): 5.0}.get(tuple(form), -1.0)
 
     monkeypatch.setattr(P, "time_candidate", fake_time)
     model = _FakeModel(in_domain=scenario != "outside")
     r = P.PipeTuner(model, top_k=5).tune(base, (100, 100, 100))
+    forms_of = lambda cs: sum(len(P.forms(base, c)) for c in cs)  # noqa: E731
     if scenario == "agrees":
-        assert not r.fell_back and r.timed == 5 and r.candidate == cands[0] and len(timed) == 5
+        # the model's top 5 shapes in the default form, then their other forms
+        assert not r.fell_back and r.candidate == cands[0]
+        assert len(timed) == r.timed == forms_of(cands[:5])
+        assert r.form == ((1, 1) if P.tmem_applies(base, cands[0]) else (0, 0))
     else:
-        assert r.fell_back and len(timed) == 5 * (scenario == "disagrees") + len(cands)
-        assert r.candidate == max(timings, key=timings.get)
+        assert r.fell_back and len(timed) == 5 * (scenario == "disagrees") + forms_of(cands)
+        best = max(timings, key=lambda c: timings[c] + (5.0 if P.tmem_applies(base, c) else 0.0))
+        assert r.candidate == best
+    assert r.candidates == forms_of(cands)
 
 
 def test_write_tuned_records_a_launch_the_workload_reads(tmp_path, monkeypatch):
@@ -107,3 +114,30 @@ def test_write_tuned_records_a_launch_the_workload_reads(tmp_path, monkeypatch):
     import json
 
     assert json.loads(path.read_text())["other"] == {"block": [8, 8, 1]}
+
+
+def test_forms_follow_the_ring_form_rules():
+    """The ring form is offered exactly where the library builds it: 3D Star Row, FP64/FP32,
+    4..32 TMEM columns per ring entry within 512, blocks of whole warps."""
+    star = StencilSpec(dimension=3, neighbourhood="Star", coefficients="Variable", range=4)
+    assert P.tmem_applies(star, (2, 4, 64, 7, 2)) and P.tmem_applies(star, (2, 2, 64, 8, 3))
+    assert not P.tmem_applies(star, (4, 4, 64, 8, 2))      # 4 column groups x 8 entries x 32 > 512
+    assert not P.tmem_applies(star, (1, 1, 32, 1, 2))      # 2 columns per entry
+    assert not P.tmem_applies(star.replace(neighbourhood="Box"), (2, 4, 64, 4, 2))
+    assert not P.tmem_applies(star.replace(precision="f32c"), (2, 4, 64, 4, 2))
+    assert P.forms(star.replace(neighbourhood="Box"), (2, 4, 64, 4, 2)) == [(0, 0), (0, 1)]
+    L = P.launch_of((2, 4, 64, 7, 2), (1, 1))
+    assert L.tmem and L.lockstep and L.to_c().flags == P._lib.LAUNCH_TMEM | P._lib.LAUNCH_LOCKSTEP
+
+
+def test_tuned_entry_records_the_form(tmp_path, monkeypatch):
+    from threadcoarsenedstencilgenerator_b200 import workloads as W
+
+    path = tmp_path / "tuned.json"
+    r = P.PipeTuneResult((2, 4, 64, 7, 2), 324.0, 600, 640, True, 1.0, "no model",
+                         {(2, 4, 64, 7, 2, 1, 1): 324.0, (2, 4, 64, 7, 2, 1, 0): 289.0}, (1, 1))
+    e = P.write_tuned(path, "3d_star_var_r4_512", "f64", r)
+    assert e["tmem"] and e["lockstep"] and "289.0" in e["source"]
+    monkeypatch.setattr(W, "TUNED_PATH", path)
+    L = W.WORKLOADS["3d_star_var_r4_512"].tuned_launch()
+    assert (tuple(L.block), L.chunk, L.tmem, L.lockstep) == ((64, 7, 1), 2, True, True)

@@ -27,6 +27,7 @@ VARIANT_PIPE = 3
 LAUNCH_SHUFFLE = 1
 LAUNCH_NO_SHUFFLE = 2
 LAUNCH_TMEM = 4
+LAUNCH_LOCKSTEP = 8
 
 
 class TcsError(RuntimeError):

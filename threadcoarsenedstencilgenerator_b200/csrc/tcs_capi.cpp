@@ -854,6 +854,14 @@ int resolve_pipe(tcs_stencil* h, const TcsGeo& g, const tcs_launch* L, Resolved&
   }
   const unsigned long long total = (unsigned long long)ntx * nty * M;
   unsigned long long nctas = (unsigned long long)h->num_sms * (unsigned)occ;
+  if (L->flags & TCS_LAUNCH_LOCKSTEP) {
+    // Whole tile columns (or 1/k of one) per CTA, k as large as the resident CTAs allow: every
+    // CTA starts at a column's (or a column part's) first plane, so neighbouring tiles sweep the
+    // same planes at the same time and their shared halo rows come from L2, not DRAM.
+    const unsigned long long tiles = (unsigned long long)ntx * nty;
+    const unsigned long long k = std::max<unsigned long long>(1, nctas / tiles);
+    nctas = tiles * std::min<unsigned long long>(k, M);
+  }
   if (L->segments) nctas = L->segments;  // explicit CTA count
   const unsigned long long per = std::max<unsigned long long>(1, (total + nctas - 1) / nctas);
   const unsigned long long grid = std::max<unsigned long long>(1, (total + per - 1) / per);

@@ -58,7 +58,8 @@ def _l2(v) -> float:
 
 def candidates(base: StencilSpec) -> list:
     """(cx, cy, bx, by, chunk) of the pipelined kernel for a problem: coarsening 1/2/4 per tiled axis
-    (1..8 in x for 2D), blocks of 32..128 x 1..16 threads with 64..1024 in all (2D: 16..128 x 1),
+    (1..8 in x for 2D), blocks of 32..128 x 1..16 threads (heights 1, 2, 4, 6, 7, 8, 16) with
+    64..1024 in all (2D: 16..128 x 1),
     tile rows that fit a 256-element TMA box and a 16-byte granule, 2 or 3 planes per chunk (1 or 2
     in 2D), and at most ~200 registers of accumulators per thread."""
     R, es = base.range, base.itemsize
@@ -86,7 +87,7 @@ def candidates(base: StencilSpec) -> list:
                 tx = bx * cx
                 if tx % vec or tx + 2 * R + vec > 256:
                     continue
-                for by in (1, 2, 4, 8, 16):
+                for by in (1, 2, 4, 6, 7, 8, 16):
                     if not 64 <= bx * by <= 1024 or by * cy + 2 * R > 256:
                         continue
                     for ch in (2, 3):
@@ -167,13 +168,38 @@ def subset(cands: list, k: int, rng) -> list:
     return [cands[i] for i in sorted(idx)]
 
 
+# ---- launch forms ---------------------------------------------------------------------------------
+# Each shape runs in up to four forms (tmem, lockstep): the register pipeline or the ring form in
+# tensor memory (3D Star stencils in Row order), and the persistent CTAs splitting the work list
+# evenly or taking whole tile columns in step (TCS_LAUNCH_LOCKSTEP).  The form changes no feature
+# of the model, which ranks shapes; the tuner times every form of the shapes it times.
+FORMS = ((0, 0), (0, 1), (1, 0), (1, 1))
+
+
+def tmem_applies(base: StencilSpec, cand) -> bool:
+    """The ring form's conditions (tcs_capi.cpp tmem_cols): 3D Star Row, FP64 or FP32, 4..32
+    columns per ring entry, whole warps, the ring within 512 columns."""
+    cx, cy, bx, by, ch = cand[:5]
+    if base.dimension != 3 or base.neighbourhood != "Star" or base.orientation != "Row":
+        return False
+    if base.precision not in ("f64", "f32") or (bx * by) % 32:
+        return False
+    w = cx * cy * (2 if base.precision == "f64" else 1)
+    need = ((bx * by + 127) // 128) * 2 * base.range * w
+    return w in (4, 8, 16, 32) and need <= 512
+
+
+def forms(base: StencilSpec, cand) -> list:
+    return [f for f in FORMS if not f[0] or tmem_applies(base, cand)]
+
+
 # ---- timing -----------------------------------------------------------------------------------
-def launch_of(cand) -> Launch:
-    cx, cy, bx, by, ch = cand
-    return Launch(block=(bx, by, 1), variant="pipe", chunk=ch)
+def launch_of(cand, form=(0, 0)) -> Launch:
+    cx, cy, bx, by, ch = cand[:5]
+    return Launch(block=(bx, by, 1), variant="pipe", chunk=ch, tmem=bool(form[0]), lockstep=bool(form[1]))
 
 
-def time_candidate(base: StencilSpec, grid, cand, mask, bufs: dict, sweeps: int = 3) -> float | None:
+def time_candidate(base: StencilSpec, grid, cand, mask, bufs: dict, sweeps: int = 3, form=(0, 0)) -> float | None:
     """GLup/s of the pipelined kernel at this candidate on the problem's grid (geometry of the
     candidate's coarsening), or None when it cannot run."""
     import torch
@@ -197,7 +223,7 @@ def time_candidate(base: StencilSpec, grid, cand, mask, bufs: dict, sweeps: int 
             bufs["x"] = torch.rand(shape, dtype=dt, device="cuda", generator=g)
             bufs["y"] = bufs["x"].clone()
             bufs["shape"] = shape
-        launch = launch_of(cand)
+        launch = launch_of(cand, form)
         st.update_grid(geom, bufs["x"], bufs["y"], launch)
         ms = st.time_sweeps(geom, bufs["x"], bufs["y"], sweeps, launch)
         if st.device_status() != 0:
@@ -209,11 +235,11 @@ def time_candidate(base: StencilSpec, grid, cand, mask, bufs: dict, sweeps: int 
     return geom.interior_points * sweeps / (ms / 1e3) / 1e9 if ms > 0 else None
 
 
-def precompile(base: StencilSpec, cand) -> bool:
+def precompile(base: StencilSpec, cand, tmem: bool = False) -> bool:
     from .stencil import precompile_pipe
 
     try:
-        precompile_pipe(problem_spec(base, cand), (cand[2], cand[3], 1), cand[4])
+        precompile_pipe(problem_spec(base, cand), (cand[2], cand[3], 1), cand[4], tmem=tmem)
         return True
     except _lib.TcsError:
         return False
@@ -224,12 +250,13 @@ def precompile(base: StencilSpec, cand) -> bool:
 class PipeTuneResult:
     candidate: tuple                 # (cx, cy, bx, by, chunk)
     glups: float
-    timed: int                       # candidates compiled and timed
-    candidates: int                  # candidates in the space
+    timed: int                       # launches (shape x form) compiled and timed
+    candidates: int                  # launches in the space
     fell_back: bool
     seconds: float
     reason: str = ""
-    measured: dict = field(default_factory=dict)
+    measured: dict = field(default_factory=dict)  # (cx, cy, bx, by, chunk, tmem, lockstep) -> GLup/s
+    form: tuple = (0, 0)             # (tmem, lockstep) of the chosen launch
 
 
 class PipeTuner:
@@ -240,7 +267,17 @@ class PipeTuner:
         X = np.stack([features(base, grid, c) for c in cands])
         return X, self.model.predict(X)
 
+    def _space(self, base, cands) -> int:
+        return sum(len(forms(base, c)) for c in cands)
+
+    def _result(self, res, n_space, fell_back, t0, reason) -> PipeTuneResult:
+        best = max(res, key=res.get)
+        return PipeTuneResult(tuple(best[:5]), res[best], len(res), n_space, fell_back, time.perf_counter() - t0,
+                              reason, res, tuple(best[5:]))
+
     def tune(self, base: StencilSpec, grid, mask=None) -> PipeTuneResult:
+        """The model ranks the shapes (register form, even split); the top k are timed in that form
+        (the model is checked against those timings) and then in their other forms."""
         t0 = time.perf_counter()
         cands = candidates(base)
         bufs = {}
@@ -264,19 +301,25 @@ class PipeTuner:
         if err > self.tolerance:
             return self._exhaustive(base, grid, cands, mask, bufs, t0,
                                     "prediction error %.2f (log) above %.2f" % (err, self.tolerance))
-        return PipeTuneResult(best, measured[best], len(measured), len(cands), False, time.perf_counter() - t0,
-                              "model top-%d" % self.top_k, measured)
+        res = {tuple(c) + (0, 0): g for c, g in measured.items()}
+        for c in measured:
+            for f in forms(base, c):
+                if f != (0, 0):
+                    g = time_candidate(base, grid, c, mask, bufs, self.sweeps, f)
+                    if g is not None:
+                        res[tuple(c) + f] = g
+        return self._result(res, self._space(base, cands), False, t0, "model top-%d" % self.top_k)
 
     def _exhaustive(self, base, grid, cands, mask, bufs, t0, reason) -> PipeTuneResult:
         res = {}
         for c in cands:
-            g = time_candidate(base, grid, c, mask, bufs, self.sweeps)
-            if g is not None:
-                res[c] = g
+            for f in forms(base, c):
+                g = time_candidate(base, grid, c, mask, bufs, self.sweeps, f)
+                if g is not None:
+                    res[tuple(c) + f] = g
         if not res:
             raise _lib.UnsupportedLaunch(_lib.TCS_ERR_UNSUPPORTED, "no pipelined launch runs this problem")
-        best = max(res, key=res.get)
-        return PipeTuneResult(best, res[best], len(res), len(cands), True, time.perf_counter() - t0, reason, res)
+        return self._result(res, self._space(base, cands), True, t0, reason)
 
 
 # ---- corpus, training, evaluation ---------------------------------------------------------------
@@ -299,8 +342,8 @@ def corpus_plan(n_problems: int, per_problem: int, seed: int = 13) -> list:
 
 
 def _precompile_job(job):
-    pid, base, grid, c = job
-    return precompile(base, c)
+    pid, base, grid, c = job[:4]
+    return precompile(base, c, bool(job[4]) if len(job) > 4 else False)
 
 
 def build_corpus(n_problems: int, per_problem: int, out: Path, seed: int = 13, log=print) -> dict:
@@ -339,12 +382,20 @@ def workload_base(w, precision: str = "f64") -> StencilSpec:
 def tuned_entry(r: PipeTuneResult) -> dict:
     """A tuned-launch record (the format workloads.py reads) of a tuning result."""
     cx, cy, bx, by, ch = r.candidate
-    runner_up = sorted(((v, k) for k, v in r.measured.items() if k != r.candidate), reverse=True)[:1]
+    chosen = tuple(r.candidate) + tuple(r.form)
+    full = lambda k: tuple(k) if len(k) == 7 else tuple(k) + (0, 0)  # noqa: E731  (shape keys: default form)
+    runner_up = sorted(((v, k) for k, v in r.measured.items() if full(k) != chosen), reverse=True)[:1]
     how = "exhaustive" if r.fell_back else "learned (%s)" % r.reason
     src = "pipetune %s over %d of %d pipelined launches: %.1f GLup/s" % (how, r.timed, r.candidates, r.glups)
     if runner_up:
         src += "; next %s: %.1f" % ("x".join(map(str, runner_up[0][1])), runner_up[0][0])
-    return {"coarsening": [cx, cy, 1], "block": [bx, by, 1], "variant": "pipe", "chunk": ch, "source": src}
+    e = {"coarsening": [cx, cy, 1], "block": [bx, by, 1], "variant": "pipe", "chunk": ch}
+    if r.form[0]:
+        e["tmem"] = True
+    if r.form[1]:
+        e["lockstep"] = True
+    e["source"] = src
+    return e
 
 
 def write_tuned(path: Path, name: str, precision: str, r: PipeTuneResult) -> dict:
@@ -420,10 +471,11 @@ def live(model: CostModel, ids, n_problems: int, seed: int = 13, log=print) -> d
         learned = PipeTuner(model).tune(base, grid, mask)
         full = PipeTuner(None).tune(base, grid, mask)
         bufs = {}
-        g_l = time_candidate(base, grid, learned.candidate, mask, bufs, 10)
-        g_f = time_candidate(base, grid, full.candidate, mask, bufs, 10)
-        rows.append({"problem": int(pid), "spec": _name(base), "learned": list(learned.candidate),
-                     "exhaustive": list(full.candidate), "ratio": g_l / g_f, "learned_s": learned.seconds,
+        g_l = time_candidate(base, grid, learned.candidate, mask, bufs, 10, learned.form)
+        g_f = time_candidate(base, grid, full.candidate, mask, bufs, 10, full.form)
+        rows.append({"problem": int(pid), "spec": _name(base), "learned": list(learned.candidate) + list(learned.form),
+                     "exhaustive": list(full.candidate) + list(full.form), "ratio": g_l / g_f,
+                     "learned_s": learned.seconds,
                      "exhaustive_s": full.seconds, "timed": learned.timed, "candidates": full.candidates,
                      "fell_back": learned.fell_back, "reason": learned.reason})
         log(json.dumps(rows[-1]))
@@ -465,14 +517,16 @@ def main(argv=None) -> int:
         problems = sample_problems(a.problems)
         for pid in holdout_ids(a.problems)[:a.holdout_full]:
             base = problems[pid]
-            jobs += [(pid, base, corpus_grid(base), c) for c in candidates(base)]
+            jobs += [(pid, base, corpus_grid(base), c, tm) for c in candidates(base)
+                     for tm in sorted({f[0] for f in forms(base, c)})]
         if a.workload:
             from .workloads import WORKLOADS
 
             for item in a.workload:
                 name, _, prec = item.partition(":")
                 base = workload_base(WORKLOADS[name], prec or "f64")
-                jobs += [(-1, base, WORKLOADS[name].grid, c) for c in candidates(base)]
+                jobs += [(-1, base, WORKLOADS[name].grid, c, tm) for c in candidates(base)
+                         for tm in sorted({f[0] for f in forms(base, c)})]
         with mp.get_context("spawn").Pool(os.cpu_count() or 4) as pool:
             ok = pool.map(_precompile_job, jobs, chunksize=1)
         print(json.dumps({"instantiations": len(jobs), "compiled": int(sum(ok))}))
@@ -487,7 +541,8 @@ def main(argv=None) -> int:
         base = workload_base(w, a.precision)
         model = None if a.exhaustive else CostModel.load(PIPE_MODEL_PATH, PIPE_FEATURES)
         r = PipeTuner(model).tune(base, w.grid, w.make_mask())
-        print(json.dumps({"workload": w.name, "candidate": list(r.candidate), "glups": r.glups, "timed": r.timed,
+        print(json.dumps({"workload": w.name, "candidate": list(r.candidate), "form": list(r.form), "glups": r.glups,
+                          "timed": r.timed,
                           "candidates": r.candidates, "fell_back": r.fell_back, "seconds": r.seconds,
                           "reason": r.reason, "top": sorted(([list(k), v] for k, v in r.measured.items()),
                                                             key=lambda q: -q[1])[:10]}))

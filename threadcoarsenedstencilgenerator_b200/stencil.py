@@ -44,6 +44,7 @@ class Launch:
     chunk: int = 0                  # pipe: planes per ring chunk (0 = auto)
     shuffle: bool | None = None     # pipe, Star: middle rows through warp shuffles (None: planner's choice)
     tmem: bool = False              # pipe, 3D Star Row: the ring form in tensor memory
+    lockstep: bool = False          # pipe: one tile column (or an equal part) per persistent CTA
 
     _VARIANTS = {"auto": _lib.VARIANT_AUTO, "direct": _lib.VARIANT_DIRECT, "march": _lib.VARIANT_MARCH,
                  "pipe": _lib.VARIANT_PIPE}
@@ -54,6 +55,8 @@ class Launch:
         flags = 0 if self.shuffle is None else (_lib.LAUNCH_SHUFFLE if self.shuffle else _lib.LAUNCH_NO_SHUFFLE)
         if self.tmem:
             flags |= _lib.LAUNCH_TMEM
+        if self.lockstep:
+            flags |= _lib.LAUNCH_LOCKSTEP
         return _lib.CLaunch(_lib.U3(*b), _lib.U3(*g), self._VARIANTS[self.variant], int(self.segments),
                             int(self.depth), int(self.chunk), flags)
 

@@ -58,7 +58,8 @@ class Workload:
             if t:
                 return Launch(block=tuple(t["block"]), variant=t.get("variant", "auto"),
                               segments=int(t.get("segments", 0)), depth=int(t.get("depth", 0)),
-                              chunk=int(t.get("chunk", 0)))
+                              chunk=int(t.get("chunk", 0)), tmem=bool(t.get("tmem", False)),
+                              lockstep=bool(t.get("lockstep", False)))
         return self.launch
 
     def tuned_spec(self, precision: str = "f64") -> StencilSpec:
