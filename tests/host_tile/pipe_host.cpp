@@ -100,15 +100,14 @@ struct HostRing {
   tcs::PipeSlot* acc;
   long long c;  // current input plane (piece-relative)
   int entry(long long p) const { return (int)(((p % tcs::R) + tcs::R) % tcs::R); }
+  void load_first(tcs::PipeSlot& s, T (&v)[tcs::NEP]) const {
+    s = acc[entry(c - tcs::R)];
+    std::memcpy(v, raw[entry(c - tcs::R)], sizeof(v));
+  }
   template <int I>
   void load_two(T (&a)[tcs::NEP], T (&b)[tcs::NEP]) const {
     std::memcpy(a, raw[entry(c - tcs::R + I)], sizeof(a));
     if (I + 1 < tcs::R) std::memcpy(b, raw[entry(c - tcs::R + I + 1)], sizeof(b));
-  }
-  template <int I>
-  void load_two_acc(T (&a)[tcs::NEP], T (&b)[tcs::NEP], tcs::PipeSlot& s) const {
-    load_two<I>(a, b);
-    s = acc[entry(c + 1 - tcs::R)];
   }
   void store(const tcs::PipeSlot& s, const T (&v)[tcs::NEP]) {
     acc[entry(c)] = s;
@@ -128,8 +127,6 @@ extern "C" int pipe_sweep_ring(const unsigned grid[3], unsigned left_offset, uns
   // stale ring contents from the previous piece (or column) must not matter: start from garbage
   T raw[R][NEP];
   PipeSlot acc[R];
-  RingCarry carry;
-  std::memset(static_cast<void*>(&carry), 0, sizeof(carry));
   for (int i = 0; i < R; ++i)
     for (int e = 0; e < NEP; ++e) raw[i][e] = (T)NAN;
   std::memset(static_cast<void*>(acc), 0xff, sizeof(acc));
@@ -143,7 +140,7 @@ extern "C" int pipe_sweep_ring(const unsigned grid[3], unsigned left_offset, uns
           const HostPlane ld{in + x + y * xdim + p * plane, xdim};
           HostRing ring{raw, acc, pi};
           PipeSlot done;
-          ring_step(ld, ring, done, carry);
+          ring_step(ld, ring, done);
           const long long op = pi - 2 * R;
           if (op >= 0 && op < me - ms) {
             constexpr T c = T(1) / T(S);

@@ -691,6 +691,15 @@ struct TmemRing {
     const tcs_u32 e = e0 + i;
     return base + (e >= (tcs_u32)R ? e - R : e) * TM_W;
   }
+  __device__ __forceinline__ void load_first(PipeSlot& s, T (&v)[NEP]) const {
+    tm_wait_st();  // the previous plane's stores are in tensor memory
+    tcs_u32 w[TM_W], x[TM_W];
+    tm_ld<TM_W>(base + (R + e0) * TM_W, w);
+    tm_ld<TM_W>(raw_col(0), x);
+    tm_wait_ld2<TM_W>(w, x);
+    tm_unpack(w, s.v);
+    tm_unpack(x, v);
+  }
   template <int I>
   __device__ __forceinline__ void load_two(T (&a)[NEP], T (&b)[NEP]) const {
     tcs_u32 w[TM_W], x[TM_W];
@@ -703,29 +712,6 @@ struct TmemRing {
       tm_wait_ld<TM_W>(w);
     }
     tm_unpack(w, a);
-  }
-  // entries 1 and 2 of the raw ring and the accumulators centred on c+1-R (entry e0 + 1), after
-  // the previous plane's stores have landed
-  template <int I>
-  __device__ __forceinline__ void load_two_acc(T (&a)[NEP], T (&b)[NEP], PipeSlot& s) const {
-    static_assert(I == 1, "the accumulators come with the first pair");
-    tm_wait_st();
-    tcs_u32 w[TM_W], x[TM_W], y[TM_W];
-    const tcs_u32 e1 = (e0 + 1u == (tcs_u32)R) ? 0u : e0 + 1u;
-    tm_ld<TM_W>(raw_col(1), w);
-    tm_ld<TM_W>(base + (R + e1) * TM_W, y);
-    if constexpr (R > 2) {
-      tm_ld<TM_W>(raw_col(2), x);
-      tm_wait_ld<TM_W>(w);
-      tm_wait_ld<TM_W>(y);
-      tm_wait_ld<TM_W>(x);
-      tm_unpack(x, b);
-    } else {
-      tm_wait_ld<TM_W>(w);
-      tm_wait_ld<TM_W>(y);
-    }
-    tm_unpack(w, a);
-    tm_unpack(y, s.v);
   }
   __device__ __forceinline__ void store(const PipeSlot& s, const T (&v)[NEP]) const {
     tcs_u32 a[TM_W], r[TM_W];
@@ -905,15 +891,6 @@ __device__ __forceinline__ bool pipe_piece(const PipeGridView& G, tcs_u32 tile, 
   constexpr int U = (!TMEM && NP2 % CHP == 0 && TCS_CYCLE != 0 && NP2 * S * NEP <= 2400 && NP2 / CHP <= 3)
                         ? NP2 / CHP : 1;
   tcs_u32 tslot = 0;  // TCS_TMEM: ring entry of the current input plane (plane mod R)
-#if TCS_TMEM
-  // The first 2R planes of a piece only fill the rings: the outputs they would complete lie
-  // before the piece and are not stored, so the carry may start from any values.
-  RingCarry carry;
-  static_for<0, NEP>([&](auto e) {
-    carry.acc.v[decltype(e)::value] = T(0);
-    carry.raw[decltype(e)::value] = T(0);
-  });
-#endif
   tcs_u32 cur_slot = gc % nslot;
   tcs_u32 cur_par = (gc / nslot) & 1u;
   T* optr = obase + ((tcs_i64)ms - 2 * R) * plane_g;
@@ -982,7 +959,7 @@ __device__ __forceinline__ bool pipe_piece(const PipeGridView& G, tcs_u32 tile, 
           PipeSlot ring_done;  // the output centred R planes back, complete after this plane
           {
             const TmemRing ring{st.tm, tslot};
-            ring_step(ld, ring, ring_done, carry);
+            ring_step(ld, ring, ring_done);
             tslot = (tslot + 1u == (tcs_u32)R) ? 0u : tslot + 1u;
           }
 #else

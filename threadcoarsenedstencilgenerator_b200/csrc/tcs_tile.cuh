@@ -574,52 +574,34 @@ __device__ __forceinline__ void apply_own(SL& s, const T (&v)[NEP]) {
 //     c-R .. c-1 (ring), then the cross of plane c -- the reference's per-output order;
 //   * finishes the output centred on c-R (accumulators from the ring): its R upper arm terms
 //     from planes c-R+1 .. c-1 (ring) and c (the centre values just read);
-//   * stores the new accumulators and plane c's own values into the ring entries just read
-//     (entry c mod R, which held plane c-R's).
-// What one plane hands to the next: the accumulators of the output the next plane completes
-// (centred on c+1-R) and the own values of plane c+1-R, the first terms the next plane needs.
-struct RingCarry {
-  PipeSlot acc;
-  T raw[NEP];
-};
-
-// RING provides load_two<i>(a, b) (own values of planes c-R+i and c-R+i+1; b only when i+1 < R),
-// load_two_acc<1>(a, b, s) (the same for i = 1 plus the accumulators centred on c+1-R, one wait
-// for all three) and store(slot, v); its entries are addressed relative to plane c.  `carry`
-// comes in with the accumulators centred on c-R and the own values of plane c-R and leaves with
-// those of c+1-R, so a plane waits for tensor memory once per two entries and never for its
-// first ones.  (R = 1 keeps everything in the carry: the ring is not read.)
+//   * stores the new accumulators and plane c's own values into the ring entries just read.
+// RING provides load_first(slot&, v) (the accumulators of the output centred on c-R and the own
+// values of plane c-R), load_two<i>(a, b) (own values of planes c-R+i and c-R+i+1; b only when
+// i+1 < R) and store(slot, v); its entries are addressed relative to plane c.  Entries come in
+// pairs so that the kernel waits for tensor memory once per two entries.
 template <class LD, class RING>
-__device__ __forceinline__ void ring_step(const LD& ld, RING& ring, PipeSlot& done, RingCarry& carry) {
+__device__ __forceinline__ void ring_step(const LD& ld, RING& ring, PipeSlot& done) {
   PipeSlot cur;
-  done = carry.acc;
-  apply_own<-R>(cur, carry.raw);
+  {
+    T v[NEP];
+    ring.load_first(done, v);
+    apply_own<-R>(cur, v);
+  }
   static_for<0, R / 2>([&](auto pp) {
     constexpr int i = 1 + 2 * decltype(pp)::value;  // entries i and i+1 (i+1 < R unless R is even)
     T a[NEP], b[NEP];
-    if constexpr (i == 1)
-      ring.template load_two_acc<1>(a, b, carry.acc);
-    else
-      ring.template load_two<i>(a, b);
+    ring.template load_two<i>(a, b);
     apply_own<i - R>(cur, a);
     apply_own<i>(done, a);
     if constexpr (i + 1 < R) {
       apply_own<i + 1 - R>(cur, b);
       apply_own<i + 1>(done, b);
     }
-    if constexpr (i == 1) {
-      static_for<0, NEP>([&](auto e) { carry.raw[decltype(e)::value] = a[decltype(e)::value]; });
-    }
   });
   T cv[NEP];
   pipe_cross(ld, cur, cv);
   apply_own<R>(done, cv);
-  if constexpr (R == 1) {
-    carry.acc = cur;
-    static_for<0, NEP>([&](auto e) { carry.raw[decltype(e)::value] = cv[decltype(e)::value]; });
-  } else {
-    ring.store(cur, cv);
-  }
+  ring.store(cur, cv);
 }
 
 // Apply input plane (offset DZ relative to pending outputs) held in shared memory to the 2R+1
