@@ -58,16 +58,16 @@ def test_shuffled_rows_match_oracle(tcs, case, precision):
 
 
 def test_shuffled_rows_full_workload(tcs):
-    """The 512^3 Star Variable r4 workload with the tuned launch and shuffled rows, two sweeps."""
-    import dataclasses
-
+    """The 512^3 Star Variable r4 workload with shuffled rows, two sweeps: the register pipeline's
+    best shape (2x4 tiles, 64x4 blocks, 3 planes per chunk; shuffles are a register-pipeline
+    option, the tuned launch runs the ring form)."""
     import torch
 
     from threadcoarsenedstencilgenerator_b200.workloads import WORKLOADS
 
     w = WORKLOADS["3d_star_var_r4_512"]
-    spec = w.tuned_spec()
-    launch = dataclasses.replace(w.tuned_launch(), shuffle=True)
+    spec = w.spec.replace(cx=2, cy=4, cz=1)
+    launch = tcs.Launch(block=(64, 4, 1), variant="pipe", chunk=3, shuffle=True)
     geom = spec.geometry(*w.grid)
     st = tcs.Stencil(spec)
     mask = w.make_mask()
