@@ -141,3 +141,23 @@ def test_tuned_entry_records_the_form(tmp_path, monkeypatch):
     monkeypatch.setattr(W, "TUNED_PATH", path)
     L = W.WORKLOADS["3d_star_var_r4_512"].tuned_launch()
     assert (tuple(L.block), L.chunk, L.tmem, L.lockstep) == ((64, 7, 1), 2, True, True)
+
+
+def test_batch_candidates_and_record(tmp_path, monkeypatch):
+    """The batched search covers blocks within the TMA box and the thread limits; its record is
+    what the batch workload reads back (block and chunk on the batch's own coarsening)."""
+    from threadcoarsenedstencilgenerator_b200 import workloads as W
+
+    w = W.BATCH_WORKLOADS["batch_3d_star_jacobi_r2_64"]
+    cands = P.batch_candidates(w.spec)
+    assert cands and all(64 <= bx * by <= 1024 and bx * w.spec.cx + 2 * w.spec.range + 2 <= 256
+                         for bx, by, ch in cands)
+    assert {ch for _, _, ch in cands} == {1, 2, 3}
+    path = tmp_path / "tuned.json"
+    r = P.PipeTuneResult((64, 4, 3), 230.0, 39, 39, True, 1.0, "batched sweep: exhaustive",
+                         {(64, 4, 3): 230.0, (32, 8, 2): 228.0})
+    e = P.write_tuned(path, w.name, "f32", r, batch=True)
+    assert e["block"] == [64, 4, 1] and e["chunk"] == 3 and "228.0" in e["source"]
+    monkeypatch.setattr(W, "TUNED_PATH", path)
+    L = w.tuned_launch("f32")
+    assert (tuple(L.block), L.chunk, L.variant) == ((64, 4, 1), 3, "pipe")

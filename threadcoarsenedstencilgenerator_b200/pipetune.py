@@ -17,7 +17,9 @@ ranges, or the timed candidates disagree with the predicted ordering by more tha
     python -m threadcoarsenedstencilgenerator_b200.pipetune precompile|corpus|train|evaluate|tune
 
 ``tune --workload NAME [--precision f32] --exhaustive --write`` records the chosen launch in the
-package's tuned.json, the file the benchmark workloads read their launches from.
+package's tuned.json, the file the benchmark workloads read their launches from.  For the batched
+workload (many grids, one launch per sweep) ``tune`` searches the batched kernel's block and planes
+per chunk exhaustively.
 """
 
 from __future__ import annotations
@@ -374,6 +376,104 @@ def build_corpus(n_problems: int, per_problem: int, out: Path, seed: int = 13, l
     return {"samples": len(rows), "seconds": time.perf_counter() - t0}
 
 
+# ---- batched sweeps -------------------------------------------------------------------------------
+def batch_candidates(spec: StencilSpec) -> list:
+    """(bx, by, chunk) of the batched pipelined sweep for a batch's parameter set (its coarsening
+    is the batch's own): blocks of 32..128 x 1..16 threads with 64..1024 in all, tiles within the
+    256-element TMA box, 1 to 3 planes per chunk."""
+    R, es = spec.range, spec.itemsize
+    vec = 16 // es
+    out = []
+    for bx in (32, 64, 128):
+        tx = bx * spec.cx
+        if tx % vec or tx + 2 * R + vec > 256:
+            continue
+        for by in (1, 2, 4, 6, 7, 8, 16):
+            if not 64 <= bx * by <= 1024 or by * spec.cy + 2 * R > 256:
+                continue
+            for ch in (1, 2, 3):
+                out.append((bx, by, ch))
+    return out
+
+
+def time_batch(w, precision: str, cand, state: dict, sweeps: int = 10) -> float | None:
+    """GLup/s of one batched launch (one launch per sweep over every grid of the batch), CUDA
+    events around `sweeps` sweeps after two warm-up sweeps; None when the shape does not run."""
+    import torch
+
+    from .batch import BatchedSweeps
+
+    if "st" not in state:
+        spec = w.spec.replace(precision=precision)
+        state["st"] = Stencil(spec)
+        geoms = w.geometries(spec)
+        dt = np.float64 if precision == "f64" else np.float32
+        state["geoms"] = geoms
+        state["xs"] = [torch.from_numpy(np.ascontiguousarray(v)).cuda() for v in w.make_inputs(geoms, dt)]
+        state["ys"] = [x.clone() for x in state["xs"]]
+        state["points"] = sum(g.interior_points for g in geoms)
+    bx, by, ch = cand
+    try:
+        bt = BatchedSweeps(state["st"], state["geoms"], state["xs"], state["ys"],
+                           Launch(block=(bx, by, 1), variant="pipe", chunk=ch))
+    except _lib.TcsError:
+        return None
+    try:
+        stream = torch.cuda.current_stream()
+        bt.sweeps(2, stream)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        bt.sweeps(sweeps, stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        if state["st"].device_status() != 0:
+            raise RuntimeError("device status word set while timing %s" % (cand,))
+        ms = e0.elapsed_time(e1)
+    finally:
+        bt.close()
+    return state["points"] * sweeps / (ms / 1e3) / 1e9 if ms > 0 else None
+
+
+def tune_batch(w, precision: str = "f64") -> PipeTuneResult:
+    """Exhaustive search of the batched sweep's launch (the cost model covers single grids)."""
+    t0 = time.perf_counter()
+    cands = batch_candidates(w.spec)
+    state, res = {}, {}
+    for c in cands:
+        g = time_batch(w, precision, c, state)
+        if g is not None:
+            res[tuple(c)] = g
+    if "st" in state:
+        state["st"].close()
+    if not res:
+        raise _lib.UnsupportedLaunch(_lib.TCS_ERR_UNSUPPORTED, "no batched launch runs this batch")
+    best = max(res, key=res.get)
+    return PipeTuneResult(best, res[best], len(res), len(cands), True, time.perf_counter() - t0,
+                          "batched sweep: exhaustive", res)
+
+
+def batch_entry(r: PipeTuneResult) -> dict:
+    """A tuned-launch record of a batched tuning result (block and chunk; the batch's coarsening)."""
+    bx, by, ch = r.candidate
+    runner_up = sorted(((v, k) for k, v in r.measured.items() if tuple(k) != tuple(r.candidate)), reverse=True)[:1]
+    src = "pipetune exhaustive over %d of %d batched launches: %.1f GLup/s" % (r.timed, r.candidates, r.glups)
+    if runner_up:
+        src += "; next %s: %.1f" % ("x".join(map(str, runner_up[0][1])), runner_up[0][0])
+    return {"block": [bx, by, 1], "variant": "pipe", "chunk": ch, "source": src}
+
+
+def _precompile_batch_job(job):
+    from .batch import precompile_batch
+
+    spec, cand = job
+    try:
+        precompile_batch(spec, (cand[0], cand[1], 1), cand[2])
+        return True
+    except _lib.TcsError:
+        return False
+
+
 def workload_base(w, precision: str = "f64") -> StencilSpec:
     """The problem of a benchmark workload: its stencil at coarsening 1 (the tuner chooses it)."""
     return w.spec.replace(precision=precision, cx=1, cy=1, cz=1)
@@ -398,12 +498,12 @@ def tuned_entry(r: PipeTuneResult) -> dict:
     return e
 
 
-def write_tuned(path: Path, name: str, precision: str, r: PipeTuneResult) -> dict:
+def write_tuned(path: Path, name: str, precision: str, r: PipeTuneResult, batch: bool = False) -> dict:
     """Record a workload's tuned pipelined launch under ``name`` (FP64) or ``name_precision``,
     keeping the file's other entries."""
     d = json.loads(path.read_text()) if path.exists() else {}
     k = name if precision == "f64" else name + "_" + precision
-    d[k] = tuned_entry(r)
+    d[k] = batch_entry(r) if batch else tuned_entry(r)
     path.parent.mkdir(parents=True, exist_ok=True)
     path.write_text(json.dumps(d, indent=1) + "\n")
     return d[k]
@@ -519,24 +619,39 @@ def main(argv=None) -> int:
             base = problems[pid]
             jobs += [(pid, base, corpus_grid(base), c, tm) for c in candidates(base)
                      for tm in sorted({f[0] for f in forms(base, c)})]
+        batch_jobs = []
         if a.workload:
-            from .workloads import WORKLOADS
+            from .workloads import BATCH_WORKLOADS, WORKLOADS
 
             for item in a.workload:
                 name, _, prec = item.partition(":")
+                if name in BATCH_WORKLOADS:
+                    spec = BATCH_WORKLOADS[name].spec.replace(precision=prec or "f64")
+                    batch_jobs += [(spec, c) for c in batch_candidates(spec)]
+                    continue
                 base = workload_base(WORKLOADS[name], prec or "f64")
                 jobs += [(-1, base, WORKLOADS[name].grid, c, tm) for c in candidates(base)
                          for tm in sorted({f[0] for f in forms(base, c)})]
         with mp.get_context("spawn").Pool(os.cpu_count() or 4) as pool:
             ok = pool.map(_precompile_job, jobs, chunksize=1)
-        print(json.dumps({"instantiations": len(jobs), "compiled": int(sum(ok))}))
+            ok += pool.map(_precompile_batch_job, batch_jobs, chunksize=1)
+        print(json.dumps({"instantiations": len(jobs) + len(batch_jobs), "compiled": int(sum(ok))}))
         return 0
     if a.cmd == "corpus":
         print(json.dumps(build_corpus(a.problems, a.per_problem, PIPE_CORPUS_PATH)))
         return 0
     if a.cmd == "tune":
-        from .workloads import WORKLOADS
+        from .workloads import BATCH_WORKLOADS, WORKLOADS
 
+        if a.workload in BATCH_WORKLOADS:
+            w = BATCH_WORKLOADS[a.workload]
+            r = tune_batch(w, a.precision)
+            print(json.dumps({"workload": w.name, "precision": a.precision, "candidate": list(r.candidate),
+                              "glups": r.glups, "timed": r.timed, "candidates": r.candidates, "seconds": r.seconds,
+                              "top": sorted(([list(k), v] for k, v in r.measured.items()), key=lambda q: -q[1])[:10]}))
+            if a.write is not None:
+                write_tuned(a.write, w.name, a.precision, r, batch=True)
+            return 0
         w = WORKLOADS[a.workload]
         base = workload_base(w, a.precision)
         model = None if a.exhaustive else CostModel.load(PIPE_MODEL_PATH, PIPE_FEATURES)
