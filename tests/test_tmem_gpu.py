@@ -100,3 +100,34 @@ def test_ring_form_rejected_where_it_does_not_apply(tcs):
     with pytest.raises(tcs.UnsupportedLaunch):
         st.plan(spec.geometry(96, 64, 40), tcs.Launch(block=(32, 4, 1), variant="pipe", chunk=1, tmem=True))
     st.close()
+
+
+LOCKSTEP_CASES = [
+    # cfg, block, chunk, ring form
+    ((3, "Star", "Row", "Variable", 4, 2, 4, 1, "Read", 16), (64, 7), 2, True),
+    ((3, "Star", "Row", "Variable", 4, 2, 4, 1, "Read", 16), (32, 7), 3, False),
+    ((3, "Box", "Row", "Variable", 2, 2, 2, 1, "Write", 8), (32, 4), 2, False),
+    ((3, "Star", "Row", "Jacobi", 3, 2, 2, 1, "None", 0), (64, 6), 3, True),
+]
+
+
+@pytest.mark.parametrize("case", LOCKSTEP_CASES,
+                         ids=lambda c: "%s_r%d_b%dx%d_ch%d_%s" % (c[0][1], c[0][4], *c[1], c[2], "ring" if c[3] else "reg"))
+def test_lockstep_matches_oracle(tcs, case):
+    """Lockstep CTAs (whole tile columns or equal parts of one) give the same bits: grids whose tile
+    count does not divide the resident CTAs, whose march length does not divide into the parts
+    (pieces straddle tile columns), with ragged last tiles."""
+    cfg, (bx, by), ch, ring = case
+    d, sh, o, c, r, cx, cy, cz, al, cl = cfg
+    spec = _spec(tcs, cfg, "f64")
+    tx, ty = bx * cx, by * cy
+    geom = spec.geometry(2 * r + 2 * tx + 3 * cx + 1, 2 * r + 3 * ty + cy + 1, 2 * r + 53)
+    rng = np.random.default_rng(23)
+    a = rng.random(geom.shape)
+    mask = rng.standard_normal(spec.stencil_size) if c == "Variable" else None
+    launch = tcs.Launch(block=(bx, by, 1), variant="pipe", chunk=ch, tmem=ring, lockstep=True)
+    got, plan = _run(tcs, spec, geom, a, mask, 3, launch)
+    tiles = -(-geom.elements[0] // tx) * -(-geom.elements[1] // ty)
+    assert plan.grid_blocks[0] <= tiles * max(1, plan.num_sms * plan.ctas_per_sm // tiles)
+    want = O.sweeps(O.make_spec(*cfg), a, 3, geom.right_offset, mask)
+    assert np.array_equal(got, want), "max |diff| %g" % float(np.abs(got - want).max())
