@@ -474,10 +474,14 @@ def run_autotune_live(n_sets: int) -> dict:
     cfg, X, y = A.load_corpus()
     hold, _ = A.split(cfg)
     m = A.CostModel.load()
-    rows = []
+    rows, rows_ref = [], []
     r = A.live(m, hold[:n_sets], log=lambda line: rows.append(line))
+    # the same sets over the reference's whole block enumeration (cuda/primes.cpp: 464 shapes in 2D,
+    # 2,723 in 3D): the model ranks shapes it never saw in training, the exhaustive sweep times all
+    r_ref = A.live(m, hold[:n_sets], log=lambda line: rows_ref.append(line), space="reference")
     m.close()
-    return {**r, "sets": [json.loads(q) for q in rows]}
+    return {**r, "sets": [json.loads(q) for q in rows],
+            "reference_space": {**r_ref, "sets": [json.loads(q) for q in rows_ref]}}
 
 
 def run_precision(args) -> dict | None:

@@ -77,6 +77,22 @@ def candidate_blocks(dimension: int, max_threads: int = 1024) -> list:
     return out
 
 
+def reference_blocks(dimension: int, max_threads: int = 1024) -> list:
+    """Every block shape of the reference's sweep (cuda/primes.cpp as restated by primes.py):
+    464 in 2D, 2,723 in 3D at 1024 threads -- the space the reference times shape by shape."""
+    from .primes import block_shapes
+
+    return [tuple(b) + (1,) * (3 - len(b)) for b in block_shapes(dimension, max_threads)]
+
+
+def blocks_of(space: str, dimension: int) -> list:
+    """Candidate blocks of a search space: "pow2" (power-of-two shapes, the corpus's) or
+    "reference" (the reference's whole enumeration)."""
+    if space == "reference":
+        return reference_blocks(dimension)
+    return candidate_blocks(dimension)
+
+
 def features(spec: StencilSpec, geom: Geometry, block, potential_block: int, plan) -> np.ndarray:
     """Feature vector of one candidate (order: FEATURES); ``plan`` is the direct launch resolved for
     it (CTA grid and resident CTAs per SM, from the driver's occupancy calculator)."""
@@ -354,8 +370,9 @@ class Autotuner:
     """Picks the direct kernel's block for (stencil, grid): model-ranked top-k, exhaustive fallback."""
 
     def __init__(self, model: CostModel | None = None, top_k: int = 5, tolerance: float = 0.25,
-                 sweeps: int = 2):
+                 sweeps: int = 2, space: str = "pow2"):
         self.model = model
+        self.space = space  # candidate blocks: "pow2" or the reference's whole enumeration
         self.top_k = top_k
         # allowed gap between measured and predicted log-throughput differences of the timed blocks
         self.tolerance = tolerance
@@ -368,7 +385,7 @@ class Autotuner:
 
     def tune(self, st: Stencil, geom: Geometry, x, y) -> TuneResult:
         t0 = time.perf_counter()
-        blocks = candidate_blocks(st.spec.dimension)
+        blocks = blocks_of(self.space, st.spec.dimension)
         if self.model is None:
             return self._exhaustive(st, geom, x, y, blocks, t0, "no model")
         keep, X, pred = self.rank(st, geom, blocks)
@@ -529,14 +546,14 @@ def evaluate(model: CostModel, cfg, X, y, ids, top_k: int = 3, seed: int = 3) ->
             "timed_fraction": top_k / float(np.mean([np.sum(cfg == c) for c in ids]))}
 
 
-def live(model: CostModel, ids, n_configs: int = 400, seed: int = 7, log=print) -> dict:
+def live(model: CostModel, ids, n_configs: int = 400, seed: int = 7, log=print, space: str = "pow2") -> dict:
     """Tune held-out parameter sets on the GPU twice -- the learned tuner (model top-5, fallback)
-    and the exhaustive sweep -- and compare the chosen blocks re-timed with 10 sweeps each, and the
-    wall time each method spent."""
+    and the exhaustive sweep, both over the candidate space `space` -- and compare the chosen
+    blocks re-timed with 10 sweeps each, and the wall time each method spent."""
     import torch
 
     specs = sample_configs(n_configs, seed)
-    tuner = Autotuner(model)
+    tuner = Autotuner(model, space=space)
     rows = []
     for cid in ids:
         spec = specs[int(cid)]
@@ -546,7 +563,7 @@ def live(model: CostModel, ids, n_configs: int = 400, seed: int = 7, log=print) 
             st.copy_mask(np.random.default_rng(int(cid)).standard_normal(spec.stencil_size) / spec.stencil_size)
         x, y = _alloc(spec, geom, int(cid))
         learned = tuner.tune(st, geom, x, y)
-        full = Autotuner(None).tune(st, geom, x, y)
+        full = Autotuner(None, space=space).tune(st, geom, x, y)
         g_l = time_block(st, geom, x, y, learned.block, 10)
         g_f = time_block(st, geom, x, y, full.block, 10)
         rows.append({"config": int(cid), "spec": _spec_str(spec), "learned_block": list(learned.block),
@@ -582,6 +599,8 @@ def main(argv=None) -> int:
     e.add_argument("--corpus", type=Path, default=CORPUS_PATH)
     e.add_argument("--model", type=Path, default=MODEL_PATH)
     e.add_argument("--live", type=int, default=0, help="also tune this many held-out sets live on the GPU")
+    e.add_argument("--space", default="pow2", choices=["pow2", "reference"],
+                   help="live candidate blocks: power-of-two shapes or the reference's whole enumeration")
     a = ap.parse_args(argv)
     if a.cmd == "corpus":
         if a.precompile:
@@ -611,7 +630,7 @@ def main(argv=None) -> int:
     m = CostModel.load(a.model)
     out = {"corpus": evaluate(m, cfg, X, y, hold)}
     if a.live:
-        out["live"] = live(m, hold[:a.live])
+        out["live"] = live(m, hold[:a.live], space=a.space)
     print(json.dumps(out))
     return 0
 
