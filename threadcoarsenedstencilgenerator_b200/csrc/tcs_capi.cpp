@@ -257,6 +257,9 @@ std::string instance_macros(const tcs_spec& s, const PipeKey* pk) {
   if (pk) {
     const char* cyc = std::getenv("TCS_PIPE_CYCLE");
     if (cyc && std::string(cyc) == "0") m << "#define TCS_CYCLE 0\n";
+    // TCS_PIPE_STREAM_STORES=1: output pairs with streaming (evict-first) stores
+    const char* sts = std::getenv("TCS_PIPE_STREAM_STORES");
+    if (sts && std::string(sts) == "1") m << "#define TCS_STCS 1\n";
   }
   // the two-sweep kernel has thread tiles of its own (tb3 x tb3 x 1); the term order of every
   // output does not depend on them

@@ -494,6 +494,11 @@ extern "C" __global__ void tcs_init(T* __restrict__ a, const tcs_u64 xdim, const
 #ifndef TCS_CYCLE
 #define TCS_CYCLE 1
 #endif
+// TCS_STCS: output pairs written with the streaming (evict-first) store, so that the outputs do
+// not push the input planes' halo rows out of L2.
+#ifndef TCS_STCS
+#define TCS_STCS 0
+#endif
 #ifndef TCS_EPI
 #define TCS_EPI 0
 #endif
@@ -1046,7 +1051,10 @@ __device__ __forceinline__ bool pipe_piece(const PipeGridView& G, tcs_u32 tile, 
                     typename PairOf<T>::type v2;
                     v2.x = v0;
                     v2.y = v1;
-                    *reinterpret_cast<typename PairOf<T>::type*>(o) = v2;
+                    if constexpr (TCS_STCS)
+                      __stcs(reinterpret_cast<typename PairOf<T>::type*>(o), v2);
+                    else
+                      *reinterpret_cast<typename PairOf<T>::type*>(o) = v2;
                   } else {
                     o[0] = v0;
                     o[1] = v1;
