@@ -409,7 +409,8 @@ def run_config1(steps: int = 20, warmup: int = 3) -> dict:
            "variant": st.plan(geom, launch).variant}
     nt = steps + (steps % 2)
     for name, run in (("single_sweep", lambda u, v, k: st.sweeps(geom, u, v, k, launch, stream)),
-                      ("temporal_blocking", lambda u, v, k: st.sweeps_tb2(geom, u, v, k, stream))):
+                      ("temporal_blocking", lambda u, v, k: st.sweeps_tb2(geom, u, v, k, stream)),
+                      ("temporal_blocking_strips", lambda u, v, k: st.sweeps_tb3(geom, u, v, k, None, stream))):
         x = torch.from_numpy(a).cuda()
         y = x.clone()
         run(x, y, 2 * warmup)
@@ -435,6 +436,11 @@ def run_config1(steps: int = 20, warmup: int = 3) -> dict:
                      "parity": bool(np.array_equal(res.cpu().numpy(), want))}
         del x, y
     out["temporal_vs_single"] = out["temporal_blocking"]["glups"] / out["single_sweep"]["glups"]
+    out["temporal_strips_vs_single"] = out["temporal_blocking_strips"]["glups"] / out["single_sweep"]["glups"]
+    out["temporal_methods"] = {
+        "temporal_blocking": "tcs_sweeps_tb2: tiles of 128 x 32 outputs loaded with their halo, two sweeps per pass",
+        "temporal_blocking_strips": "tcs_sweeps_tb3 in 2D: strips marching along y through a TMA ring, stage 2 on "
+                                    "stage 1's completed rows, two sweeps per pass"}
     out["roofline_note"] = ("single sweep: 16 B per lattice update (read + write); temporal blocking: 16 B per "
                             "two updates, so its HBM fraction counts 8 B per update")
     st.close()
@@ -993,8 +999,13 @@ def run_case(args) -> dict:
     w = WORKLOADS[args.workload]
     spec = w.tuned_spec(args.case_precision).replace(precision=args.case_precision)
     launch = w.tuned_launch(args.case_precision)
+    tb3_launch = None  # temporal-strips: the two-sweep kernel's block, chunk and CTA count
     if args.case_launch:
-        spec, launch = case_launch(spec, args.case_launch)
+        case_spec, launch = case_launch(spec, args.case_launch)
+        if args.case == "temporal-strips":
+            tb3_launch = launch  # its thread tiles are its own: the parameter set keeps its coarsening
+        else:
+            spec = case_spec
     grid = tuple(args.grid) + (1,) * (3 - len(args.grid))
     geom = spec.geometry(*grid)
     st = tcs.Stencil(spec)
@@ -1012,6 +1023,9 @@ def run_case(args) -> dict:
         if args.case == "temporal":
             st.sweeps_tb2(geom, x, y, n)
             return
+        if args.case == "temporal-strips":
+            st.sweeps_tb3(geom, x, y, n, tb3_launch)
+            return
         for _ in range(n):
             if args.case == "tensor-cores":
                 st.tc_update_grid(geom, x, y)
@@ -1019,7 +1033,7 @@ def run_case(args) -> dict:
                 st.update_grid(geom, x, y, launch)
             x, y = y, x
 
-    run(2 if args.case == "temporal" else 1)  # warm-up (module load, first touch)
+    run(2 if args.case.startswith("temporal") else 1)  # warm-up (module load, first touch)
     torch.cuda.synchronize()
     e0.record(stream)
     run(args.steps)
@@ -1080,7 +1094,7 @@ def main(argv=None) -> int:
     ap.add_argument("--period", type=int, default=20, help="precision mode: FP32 sweeps per FP64 defect")
     ap.add_argument("--grid", type=int, nargs="+", help="profiling case: --steps sweeps on this reduced grid")
     ap.add_argument("--grids", type=int, default=0, help="profiling case (batch): the first K grids")
-    ap.add_argument("--case", default="sweep", choices=["sweep", "tensor-cores", "temporal"],
+    ap.add_argument("--case", default="sweep", choices=["sweep", "tensor-cores", "temporal", "temporal-strips"],
                     help="profiling case: which kernel")
     ap.add_argument("--case-precision", default="f64", choices=["f64", "f32"], help="profiling case: precision")
     ap.add_argument("--case-launch", default="", help="profiling case: pipelined launch "

@@ -258,13 +258,15 @@ int tcs_precompile_pipe_flags(const tcs_spec* spec, unsigned bx, unsigned by, un
 int tcs_precompile_pipe_epilogue(const tcs_spec* spec, unsigned bx, unsigned by, unsigned chunk, unsigned epi,
                                  char* cubin_path, unsigned path_cap);
 
-/* Two sweeps per pass over HBM for 3D grids (temporal blocking; no counterpart in the reference,
- * which sweeps once per launch: cuda/generateLaunchUpdateGrid.py:128-139).  n ping-pong sweeps
- * starting from a, in passes of two (tcs_tb3 kernel), an odd last sweep as an ordinary sweep;
- * *result_in_b says which buffer holds the result.  Bit-identical to n tcs_update_grid sweeps.
- * `launch` (may be NULL) gives the block (bx, by) of the kernel's thread tiles -- 2 x 2 points for
- * even ranges, 1 x 1 for odd ones -- the planes per ring chunk and the chunks in flight.  FP64 and
- * FP32 (FP32: even ranges), grids of whole coarsening tiles; TCS_ERR_UNSUPPORTED otherwise. */
+/* Two sweeps per pass over HBM (temporal blocking; no counterpart in the reference, which sweeps
+ * once per launch: cuda/generateLaunchUpdateGrid.py:128-139).  n ping-pong sweeps starting from a,
+ * in passes of two (tcs_tb3 kernel), an odd last sweep as an ordinary sweep; *result_in_b says
+ * which buffer holds the result.  Bit-identical to n tcs_update_grid sweeps.  `launch` (may be
+ * NULL) gives the block (bx, by) of the kernel's thread tiles -- 2 x 2 points for even ranges,
+ * 1 x 1 for odd ones; in 2D, strips of bx thread tiles of 2 x 1 or 1 x 1 marching along y, block
+ * (bx, 1, 1) -- the planes (2D: rows) per ring chunk, the chunks in flight and the CTA count
+ * (segments).  3D, and 2D in Row order; FP64 and FP32 (FP32: even ranges), grids of whole
+ * coarsening tiles; TCS_ERR_UNSUPPORTED otherwise. */
 int tcs_sweeps_tb3(tcs_stencil* h, const unsigned grid[3], unsigned right_offset, const tcs_launch* launch,
                    void* a, void* b, unsigned n, void* stream, int* result_in_b);
 
@@ -273,7 +275,7 @@ int tcs_plan_tb3(tcs_stencil* h, const unsigned grid[3], unsigned right_offset, 
                  tcs_plan* plan);
 
 /* Instantiate the two-sweep kernel of a parameter set (block bx x by, 0 = the default; chunk 0 =
- * 2 planes) into the cubin cache without a GPU. */
+ * 2 planes in 3D, 8 rows in 2D) into the cubin cache without a GPU. */
 int tcs_precompile_tb3(const tcs_spec* spec, unsigned bx, unsigned by, unsigned chunk, char* cubin_path,
                        unsigned path_cap);
 

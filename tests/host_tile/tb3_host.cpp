@@ -1,4 +1,4 @@
-// Host build of the 3D two-sweep kernel's control flow (test harness for tcs_tb3).
+// Host build of the two-sweep kernel's control flow (test harness for tcs_tb3, 3D and 2D).
 //
 // Runs tcs_tb3's per-piece logic for every CTA tile and piece, one thread tile after another:
 // stage 1 applies each input plane to pipeline 1 with tcs::pipe_plane (reading the input with zero
@@ -6,7 +6,9 @@
 // buffer -- points outside the interior take the input's value -- and, once every thread of the
 // tile has written, stage 2 applies the buffer plane to pipeline 2 and stores the inner thread
 // tiles' completed outputs.  Same tile geometry (extended tile, output tile, thread tiles of
-// TCS_CX x TCS_CY dividing R), same plane offsets and slot rotation as the kernel.
+// TCS_CX x TCS_CY dividing R), same plane offsets and slot rotation as the kernel.  In 2D the
+// march axis is y: a "plane" is one row, the extended tile a strip of bx * CX columns, the plane
+// buffer one row with an R-wide margin.
 #include <cstring>
 #include <vector>
 
@@ -23,6 +25,10 @@ struct GlobalPlane {  // input plane at a thread origin; zero outside the grid
   template <int GX, int GY>
   T one() const {
     const long long xx = x + GX, yy = y + GY;
+    if constexpr (DIM == 2) {  // z is the row
+      if (xx < 0 || z < 0 || xx >= xdim || z >= ydim) return T(0);
+      return in[xx + z * xdim];
+    }
     if (xx < 0 || yy < 0 || z < 0 || xx >= xdim || yy >= ydim || z >= zdim) return T(0);
     return in[xx + yy * xdim + z * xdim * ydim];
   }
@@ -59,21 +65,24 @@ extern "C" int tb3_pass(const unsigned grid[3], unsigned left_offset, unsigned r
     for (int k = 0; k < S; ++k) tcs_mask[k] = (T)mask[k];
   if (COEFF == 1 && tcs::PAIRS)
     for (int k = 0; k < S; ++k) tcs_mask_pairs[k] = make_float2((float)mask[k], (float)mask[k]);
-  const long long xdim = grid[0], ydim = grid[1], zdim = grid[2];
-  const long long plane = xdim * ydim;
+  constexpr bool D3 = DIM == 3;
+  const long long xdim = grid[0], ydim = grid[1], zdim = D3 ? grid[2] : 1;
+  const long long plane = D3 ? xdim * ydim : xdim;  // stride of the march axis
   const long long x0 = R + left_offset;
   const long long x_lim = xdim - R - (aligned ? right_offset : 0), y_lim = ydim - R, z_lim = zdim - R;
-  const int EX = (int)bx * CX, EY = (int)by * CY, OX = EX - 2 * R, OY = EY - 2 * R;
-  const int BW = EX + 2 * R, BH = EY + 2 * R;
-  if (OX <= 0 || OY <= 0 || R % CX || R % CY) return 1;
-  const long long ntx = (x_lim - x0 + OX - 1) / OX, nty = (y_lim - R + OY - 1) / OY;
+  const long long m_lim = D3 ? z_lim : y_lim, m_dim = D3 ? zdim : ydim;  // march axis
+  if (!D3) by = 1;
+  const int EX = (int)bx * CX, EY = D3 ? (int)by * CY : 1, OX = EX - 2 * R, OY = D3 ? EY - 2 * R : 1;
+  const int BW = EX + 2 * R, BH = D3 ? EY + 2 * R : 1;
+  if (OX <= 0 || OY <= 0 || R % CX || (D3 && R % CY) || (!D3 && CY != 1)) return 1;
+  const long long ntx = (x_lim - x0 + OX - 1) / OX, nty = D3 ? (y_lim - R + OY - 1) / OY : 1;
   const int nthr = (int)(bx * by);
   std::vector<T> buf(2 * (size_t)BW * BH, T(0));
   std::vector<PipeSlot> acc1((size_t)nthr * NP2), acc2((size_t)nthr * NP2);
   constexpr T c = T(1) / T(S);
   for (long long tile = 0; tile < ntx * nty; ++tile)
-    for (long long zs = 0; zs < z_lim - R; zs += piece) {
-      const long long ze = (zs + piece < z_lim - R) ? zs + piece : z_lim - R;
+    for (long long zs = 0; zs < m_lim - R; zs += piece) {
+      const long long ze = (zs + piece < m_lim - R) ? zs + piece : m_lim - R;
       const long long ms = R + zs, nout = ze - zs, np = nout + 4 * R, m_first = ms - 2 * R;
       const long long X0 = x0 - R + (tile % ntx) * OX, Y0 = (tile / ntx) * OY;
       for (long long pi = 0; pi < np; ++pi) {
@@ -94,22 +103,23 @@ extern "C" int tb3_pass(const unsigned grid[3], unsigned left_offset, unsigned r
             static_for<0, CX>([&](auto ex) {
               constexpr int e = decltype(ex)::value + decltype(ey)::value * CX;
               const long long gx = X0 + ex0 + decltype(ex)::value, gy = Y0 + ey0 + decltype(ey)::value;
-              const bool interior = gx >= x0 && gx < x_lim && gy >= R && gy < y_lim && q >= R && q < z_lim;
+              const bool interior =
+                  gx >= x0 && gx < x_lim && (!D3 || (gy >= R && gy < y_lim)) && q >= R && q < m_lim;
               T v = (COEFF == 0) ? slot_value<e>(d1) * c : slot_value<e>(d1);
               if (!interior) {
-                const bool ing = gx >= 0 && gx < xdim && gy >= 0 && gy < ydim && q >= 0 && q < zdim;
-                v = ing ? in[gx + gy * xdim + q * plane] : T(0);
+                const bool ing = gx >= 0 && gx < xdim && (!D3 || (gy >= 0 && gy < ydim)) && q >= 0 && q < m_dim;
+                v = ing ? in[gx + (D3 ? gy * xdim : 0) + q * plane] : T(0);
               }
-              bq[(R + ey0 + decltype(ey)::value) * BW + R + ex0 + decltype(ex)::value] = v;
+              bq[(D3 ? (R + ey0 + decltype(ey)::value) * BW : 0) + R + ex0 + decltype(ex)::value] = v;
             });
           });
         }
         for (int th = 0; th < nthr; ++th) {  // stage 2
           const int ex0 = (th % (int)bx) * CX, ey0 = (th / (int)bx) * CY;
           PipeSlot* a2 = &acc2[(size_t)th * NP2];
-          const bool inner = ex0 >= R && ex0 < EX - R && ey0 >= R && ey0 < EY - R;
+          const bool inner = ex0 >= R && ex0 < EX - R && (!D3 || (ey0 >= R && ey0 < EY - R));
           // edge thread tiles read the buffer's margin (never written); their outputs are discarded
-          const BufPlane ldb{bq + (R + ey0) * BW + R + ex0, BW};
+          const BufPlane ldb{bq + (D3 ? (R + ey0) * BW : 0) + R + ex0, BW};
           auto slot2 = [&](auto kk) -> PipeSlot& {
             constexpr int k = decltype(kk)::value;
             return a2[((t - k) % NP2 + NP2) % NP2];
@@ -122,8 +132,9 @@ extern "C" int tb3_pass(const unsigned grid[3], unsigned left_offset, unsigned r
               static_for<0, CX>([&](auto ex) {
                 constexpr int e = decltype(ex)::value + decltype(ey)::value * CX;
                 const long long ox = X0 + ex0 + decltype(ex)::value, oy = Y0 + ey0 + decltype(ey)::value;
-                if (ox < x_lim && oy < y_lim)
-                  out[ox + oy * xdim + (ms + op) * plane] = (COEFF == 0) ? slot_value<e>(d2) * c : slot_value<e>(d2);
+                if (ox < x_lim && (!D3 || oy < y_lim))
+                  out[ox + (D3 ? oy * xdim : 0) + (ms + op) * plane] =
+                      (COEFF == 0) ? slot_value<e>(d2) * c : slot_value<e>(d2);
               });
             });
           }

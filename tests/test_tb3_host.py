@@ -1,4 +1,4 @@
-"""The 3D two-sweep kernel's control flow on the CPU (tests/host_tile/tb3_host.cpp): one pass
+"""The two-sweep kernel's control flow (3D, and 2D strips) on the CPU (tests/host_tile/tb3_host.cpp): one pass
 equals two oracle sweeps bit for bit -- extended and output tiles, ragged last tiles, the border
 copy into the plane buffer, pieces that restart both pipelines, the slot rotation at chunk ends."""
 
@@ -17,6 +17,12 @@ CASES = [
     ((3, "Star", "Column", "Variable", 3, 1, 1, 1, "Write", 8), (41, 30, 22), (12, 10), 6, 2),
     ((3, "Star", "Row", "Variable", 4, 2, 2, 1, "Read", 16), (52, 40, 26), (10, 8), 9, 3),
     ((3, "Box", "Row", "Variable", 2, 2, 2, 1, "None", 0), (31, 27, 16), (6, 6), 1 << 30, 2),
+    # 2D: strips marching along y (block[1] ignored)
+    ((2, "Box", "Row", "Jacobi", 1, 1, 1, 1, "None", 0), (45, 37, 1), (10, 1), 9, 8),
+    ((2, "Box", "Row", "Jacobi", 1, 1, 1, 1, "None", 0), (33, 30, 1), (8, 1), 1 << 30, 3),
+    ((2, "Star", "Row", "Variable", 2, 2, 1, 1, "Read", 8), (52, 41, 1), (8, 1), 11, 5),
+    ((2, "Box", "Row", "Variable", 3, 1, 1, 1, "Write", 8), (47, 35, 1), (12, 1), 7, 7),
+    ((2, "Star", "Row", "Jacobi", 4, 2, 1, 1, "None", 0), (61, 44, 1), (10, 1), 1 << 30, 8),
 ]
 
 
@@ -29,7 +35,8 @@ def test_two_sweep_pass_equals_two_sweeps(case, precision):
     g = O.geometry(spec, *n)
     rng = np.random.default_rng(61)
     dt = np.float64 if precision == "f64" else np.float32
-    a = rng.uniform(-1, 1, (g.grid[2], g.grid[1], g.grid[0])).astype(dt)
+    shape = (g.grid[2], g.grid[1], g.grid[0]) if cfg[0] == 3 else (g.grid[1], g.grid[0])
+    a = rng.uniform(-1, 1, shape).astype(dt)
     mask = rng.standard_normal(O.stencil_size(spec)) if cfg[3] == "Variable" else None
     want = O.sweeps(spec, a, 4, g.right_offset, mask)
     got = host_tile.tb3_passes(cfg, a, g.grid, g.left_offset, g.right_offset, 2, mask, precision, block, piece,

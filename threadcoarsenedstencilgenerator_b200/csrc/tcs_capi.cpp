@@ -217,7 +217,7 @@ struct PipeKey {
   unsigned bx, by, ch, lshift;
   unsigned batch = 0;
   unsigned epi = 0;  // epilogue mode (tcs_kernels.cuh, TCS_EPI): 0 plain, 1 FP64 defect, 2 FP32 accumulate
-  unsigned tb3 = 0;  // tcs_tb3 (two sweeps per pass, 3D) with thread tiles tb3 x tb3; 0: tcs_pipe
+  unsigned tb3 = 0;  // tcs_tb3 (two sweeps per pass) with thread tiles tb3 x tb3 (2D: tb3 x 1); 0: tcs_pipe
   unsigned shfl = 0;  // Star middle rows through warp shuffles (TCS_SHFL)
   unsigned tmem = 0;  // ring form in tensor memory (TCS_TMEM)
   bool operator==(const PipeKey& o) const {
@@ -263,7 +263,8 @@ std::string instance_macros(const tcs_spec& s, const PipeKey* pk) {
   }
   // the two-sweep kernel has thread tiles of its own (tb3 x tb3 x 1); the term order of every
   // output does not depend on them
-  const int cx = (pk && pk->tb3) ? (int)pk->tb3 : s.cx, cy = (pk && pk->tb3) ? (int)pk->tb3 : s.cy;
+  const int cx = (pk && pk->tb3) ? (int)pk->tb3 : s.cx;
+  const int cy = (pk && pk->tb3) ? (s.dimension == 3 ? (int)pk->tb3 : 1) : s.cy;
   const int cz = (pk && pk->tb3) ? 1 : (s.dimension == 3 ? s.cz : 1);
   m << "#define TCS_T " << (s.precision == TCS_F64 ? "double" : "float") << "\n"
     << "#define TCS_COMP " << (s.precision == TCS_F32C ? 1 : 0) << "\n"
@@ -914,34 +915,44 @@ int resolve_pipe(tcs_stencil* h, const TcsGeo& g, const tcs_launch* L, Resolved&
   return TCS_OK;
 }
 
-// The two-sweep kernel tcs_tb3 (3D): thread tiles C x C with C = 2 for even ranges and 1 for odd
+// The two-sweep kernel tcs_tb3.  3D: thread tiles C x C with C = 2 for even ranges and 1 for odd
 // ones (C divides R, so a thread tile lies wholly inside or outside the output tile); by default
 // an extended tile of 64 x 32 columns (C = 2: 32 x 16 threads) or 32 x 32 (C = 1: 32 x 32
-// threads), whose inner (EX - 2R) x (EY - 2R) columns are the output tile.  `L` (may be NULL)
-// gives the block (bx, by) and the planes per ring chunk.
+// threads), whose inner (EX - 2R) x (EY - 2R) columns are the output tile.  2D (Row order): a
+// strip of EX = bx * C columns marching along y, thread tiles C x 1, by default 128 threads, whose
+// inner EX - 2R columns are the output strip.  `L` (may be NULL) gives the block (bx, by), the
+// planes (2D: rows) per ring chunk, the chunks in flight and the CTA count.
 int resolve_tb3(tcs_stencil* h, const TcsGeo& g, const tcs_launch* L, Resolved& out) {
   const tcs_spec& s = h->spec;
-  if (s.dimension != 3) return fail(TCS_ERR_UNSUPPORTED, "tb3: 3D stencils only");
   if (s.precision == TCS_F32C) return fail(TCS_ERR_UNSUPPORTED, "tb3: plain FP64 or FP32 sweeps only");
+  if (s.dimension == 2 && s.orientation == TCS_COLUMN)
+    return fail(TCS_ERR_UNSUPPORTED, "tb3: 2D stencils in Row order only");
+  const bool d3 = s.dimension == 3;
   const unsigned R = (unsigned)s.range;
   const unsigned es = (unsigned)elem_size(s), vec = 16u / es;
   const unsigned C = (R % 2 == 0) ? 2u : 1u;
-  unsigned bx = (C == 2) ? 32u : 32u, by = (C == 2) ? 16u : 32u;
+  unsigned bx = d3 ? 32u : 128u, by = d3 ? ((C == 2) ? 16u : 32u) : 1u;
+  while (!d3 && bx > 8 && bx * C + 2 * R + vec > 256) bx -= 8;  // 2D: the strip fits a TMA box
   if (L && L->block[0]) {
     bx = L->block[0];
     by = L->block[1] ? L->block[1] : 1u;
   }
-  const unsigned EX = bx * C, EY = by * C;
-  if (EX <= 2 * R || EY <= 2 * R) return fail(TCS_ERR_UNSUPPORTED, "tb3: tile too small for the range");
-  const unsigned OX = EX - 2 * R, OY = EY - 2 * R;
-  if (OX % vec != 0) return fail(TCS_ERR_UNSUPPORTED, "tb3: output tile width not a multiple of 16 bytes");
+  if (!d3 && by != 1) return fail(TCS_ERR_UNSUPPORTED, "tb3: 2D blocks are (bx, 1, 1)");
+  const unsigned EX = bx * C, EY = d3 ? by * C : 1u;
+  if (EX <= 2 * R || (d3 && EY <= 2 * R)) return fail(TCS_ERR_UNSUPPORTED, "tb3: tile too small for the range");
+  const unsigned OX = EX - 2 * R, OY = d3 ? EY - 2 * R : 1u;
+  if (OX % vec != 0 || EX % vec != 0)
+    return fail(TCS_ERR_UNSUPPORTED, "tb3: extended or output tile width not a multiple of 16 bytes");
   const unsigned lshift = (unsigned)((((int)h->left_off - (int)R) % (int)vec + (int)vec) % (int)vec);
-  const unsigned ch = (L && L->chunk) ? L->chunk : 2u;
-  const unsigned rows = EY + 2 * R;
+  // 2D rows are short: 8 per chunk by default (a chunk of 8 rows is a multiple of 128 bytes for
+  // any row width, so the ring rows need no padding and the TMA box reads no extra columns)
+  const unsigned ch = (L && L->chunk) ? L->chunk : (d3 ? 2u : 8u);
+  const unsigned rows = d3 ? EY + 2 * R : 1u;
   const unsigned W = pipe_width(EX, R, lshift, vec, ch, rows, es);
-  if (W > 256 || rows > 256) return fail(TCS_ERR_UNSUPPORTED, "tb3: tile exceeds the 256-element TMA box limit");
+  if (W > 256 || rows > 256 || ch > 256)
+    return fail(TCS_ERR_UNSUPPORTED, "tb3: tile exceeds the 256-element TMA box limit");
   const unsigned chunk_bytes = ch * rows * W * es;
-  const unsigned buf_bytes = 2u * (EX + 2 * R) * (EY + 2 * R) * es;
+  const unsigned buf_bytes = 2u * (EX + 2 * R) * (d3 ? EY + 2 * R : 1u) * es;
   PipeKey key{bx, by, ch, lshift, 0u, 0u, C};
   PipeMod* pm = nullptr;
   int rc = pipe_module(h, key, &pm);
@@ -967,10 +978,16 @@ int resolve_tb3(tcs_stencil* h, const TcsGeo& g, const tcs_launch* L, Resolved& 
   TCS_CU(g_drv.OccMaxActive(&occ, pm->f, nthr, smem));
   if (occ < 1) return fail(TCS_ERR_UNSUPPORTED, "tb3 kernel cannot be resident at this shape");
   const unsigned long long ex = g.x_lim > g.x0 ? g.x_lim - g.x0 : 0;
-  const unsigned ntx = std::max(1u, cdiv(ex, OX)), nty = std::max(1u, cdiv(g.y_lim - R, OY));
-  const unsigned long long M = g.z_lim - R;
+  const unsigned ntx = std::max(1u, cdiv(ex, OX)), nty = d3 ? std::max(1u, cdiv(g.y_lim - R, OY)) : 1u;
+  const unsigned long long M = d3 ? g.z_lim - R : g.y_lim - R;
   const unsigned long long total = (unsigned long long)ntx * nty * M;
   unsigned long long nctas = (unsigned long long)h->num_sms * (unsigned)occ;
+  if (!d3) {
+    // Every piece re-reads 4R rows and recomputes 2R rows of stage 1: keep pieces at least
+    // 64 rows long unless that leaves SMs idle.
+    const unsigned long long cap = std::max<unsigned long long>((unsigned long long)h->num_sms, total / 64);
+    nctas = std::min(nctas, cap);
+  }
   if (L && L->segments) nctas = L->segments;
   const unsigned long long per = std::max<unsigned long long>(1, (total + nctas - 1) / nctas);
   const unsigned long long grid = std::max<unsigned long long>(1, (total + per - 1) / per);
@@ -1002,8 +1019,8 @@ int resolve_tb3(tcs_stencil* h, const TcsGeo& g, const tcs_launch* L, Resolved& 
   out.block[1] = by;
   out.block[2] = 1;
   out.box[0] = W;
-  out.box[1] = rows;
-  out.box[2] = ch;
+  out.box[1] = d3 ? rows : ch;
+  out.box[2] = d3 ? ch : 1u;
   out.smem = smem;
   out.depth = nslot - 1;
   out.occ = occ;
@@ -2573,17 +2590,20 @@ int tcs_precompile_tb3(const tcs_spec* spec, unsigned bx, unsigned by, unsigned 
                        unsigned path_cap) {
   int rc = validate(spec);
   if (rc) return rc;
-  if (spec->dimension != 3) return fail(TCS_ERR_UNSUPPORTED, "tb3: 3D stencils only");
+  const bool d3 = spec->dimension == 3;
+  if (!d3 && spec->orientation == TCS_COLUMN) return fail(TCS_ERR_UNSUPPORTED, "tb3: 2D stencils in Row order only");
   const unsigned R = (unsigned)spec->range, vec = 16u / (unsigned)elem_size(*spec);
   const unsigned C = (R % 2 == 0) ? 2u : 1u;
   if (bx == 0) {
-    bx = 32;
-    by = (C == 2) ? 16u : 32u;
+    bx = d3 ? 32u : 128u;
+    by = d3 ? ((C == 2) ? 16u : 32u) : 1u;
+    while (!d3 && bx > 8 && bx * C + 2 * R + vec > 256) bx -= 8;
   }
-  if (bx * C <= 2 * R || by * C <= 2 * R || (bx * C - 2 * R) % vec != 0)
+  if (!d3) by = 1;
+  if (bx * C <= 2 * R || (d3 && by * C <= 2 * R) || (bx * C - 2 * R) % vec != 0 || (bx * C) % vec != 0)
     return fail(TCS_ERR_UNSUPPORTED, "tb3: no output tile of 16-byte multiples for this range and block");
   const unsigned lshift = (unsigned)((((int)left_offset_of(*spec) - (int)R) % (int)vec + (int)vec) % (int)vec);
-  PipeKey key{bx, by, chunk ? chunk : 2u, lshift, 0u, 0u, C};
+  PipeKey key{bx, by, chunk ? chunk : (d3 ? 2u : 8u), lshift, 0u, 0u, C};
   std::vector<char> cubin;
   std::string path;
   if ((rc = instantiate(*spec, &key, cubin, &path))) return rc;

@@ -1275,7 +1275,7 @@ extern "C" __global__ void __launch_bounds__(TCS_BX * ((TCS_DIM == 3) ? TCS_BY :
 #endif  // TCS_BATCH
 
 #ifdef TCS_TB3
-// ---- tcs_tb3: two sweeps in one pass over HBM (temporal blocking, 3D) -------------------------
+// ---- tcs_tb3: two sweeps in one pass over HBM (temporal blocking, 3D and 2D) -------------------
 // The pipelined sweep run twice in the same CTA, stage 2 on the output of stage 1.  A CTA owns an
 // extended tile of TB_EX x TB_EY columns (its threads' coverage, CX x CY per thread, with CX = CY
 // dividing R) and streams its input planes through the TMA ring as tcs_pipe does.  Stage 1 keeps
@@ -1285,13 +1285,16 @@ extern "C" __global__ void __launch_bounds__(TCS_BX * ((TCS_DIM == 3) ? TCS_BY :
 // plane to its own register pipeline (pipeline 2) and stores the completed planes of S(S(in)) for
 // the inner (TB_EX - 2R) x (TB_EY - 2R) columns; the outer ring of threads only serves stage 1.
 // Both stages use the per-output term order of one sweep, so out = S(S(in)) bit for bit.
+// In 2D the march axis is y and a "plane" is one row: the extended tile is a strip of TB_EX
+// columns (CX per thread dividing R), the plane buffer one row with an R-wide margin, and the
+// output tile the inner TB_EX - 2R columns of every row.
 namespace tcs {
-constexpr int TB_EX = TXP, TB_EY = TYP;                      // extended tile (stage 1)
-constexpr int TB_OX = TB_EX - 2 * R, TB_OY = TB_EY - 2 * R;  // output tile (stage 2)
-constexpr int TB_BW = TB_EX + 2 * R, TB_BH = TB_EY + 2 * R;  // plane buffer, range-wide margin
-static_assert(DIM == 3, "tcs_tb3 is the 3D two-sweep kernel");
+constexpr int TB_EX = TXP, TB_EY = TYP;                                       // extended tile (stage 1)
+constexpr int TB_OX = TB_EX - 2 * R, TB_OY = (DIM == 3) ? TB_EY - 2 * R : 1;  // output tile (stage 2)
+constexpr int TB_BW = TB_EX + 2 * R, TB_BH = (DIM == 3) ? TB_EY + 2 * R : 1;  // plane buffer, range-wide margin
 static_assert(TB_OX > 0 && TB_OY > 0 && TB_OX % VEC == 0, "output tile: positive, 16-byte multiple");
-static_assert(R % CX == 0 && R % CY == 0, "thread tiles must not straddle the output tile's edge");
+static_assert(R % CX == 0 && (DIM == 2 || R % CY == 0), "thread tiles must not straddle the output tile's edge");
+static_assert(DIM == 3 || CY == 1, "2D strips: one row per thread");
 static_assert(!COMP && EPI == 0, "plain sweeps only");
 
 // Reader of a stage-1 plane in the plane buffer at a thread origin (row pitch TB_BW).  Pairs are
@@ -1326,7 +1329,7 @@ __device__ __forceinline__ bool tb3_piece(const PipeGridView& G, tcs_u32 tile, t
   const tcs_u32 nch = (tcs_u32)((np + CHP - 1) / CHP);
   const int m_first = ms - 2 * R;                   // input plane of pi = 0
   const int X0 = (int)G.x0 - R + (int)(tile % G.ntx) * TB_OX;  // extended tile origin
-  const int Y0 = (int)(tile / G.ntx) * TB_OY;                  // = R + ty*TB_OY - R
+  const int Y0 = (DIM == 3) ? (int)(tile / G.ntx) * TB_OY : 0;  // 3D: = R + ty*TB_OY - R
   const int xl = X0 - R - LSHIFT;                   // TMA x start: a multiple of VEC (may be < 0)
   auto issue = [&](tcs_u32 j) {
     const tcs_u32 slot = (gc + j) % nslot;
@@ -1334,7 +1337,11 @@ __device__ __forceinline__ bool tb3_piece(const PipeGridView& G, tcs_u32 tile, t
     const int m0 = m_first + (int)(j * CHP);
     if (use_tma) {
       mbar_expect_tx(bar, CHUNK_BYTES);
+#if TCS_DIM == 2
+      tma_load_2d(st.ring_s + slot * CHUNK_BYTES, G.map, bar, xl, m0);
+#else
       tma_load_3d(st.ring_s + slot * CHUNK_BYTES, G.map, bar, xl, Y0 - R, m0);
+#endif
     } else {
       // negative coordinates wrap to large unsigned values and read as zeros
       pipe_copy_chunk<1>(G, st.ring_s + slot * CHUNK_BYTES, (tcs_u32)xl, (tcs_u32)(Y0 - R), (tcs_u32)m0, tid);
@@ -1350,10 +1357,14 @@ __device__ __forceinline__ bool tb3_piece(const PipeGridView& G, tcs_u32 tile, t
       for (tcs_u32 j = 0; j < pro; ++j) issue(j);
     }
   }
-  const int ex0 = (int)threadIdx.x * CX, ey0 = (int)threadIdx.y * CY;  // thread tile in the extended tile
-  const tcs_u32 lane_off = (R + threadIdx.y * CY) * PW + LSHIFT + R + threadIdx.x * CX;
-  const bool inner = ex0 >= R && ex0 < TB_EX - R && ey0 >= R && ey0 < TB_EY - R;
-  const tcs_i64 xdim = (tcs_i64)G.xdim, plane_g = (tcs_i64)(G.xdim * G.ydim);
+  const int ex0 = (int)threadIdx.x * CX;  // thread tile in the extended tile
+  const int ey0 = (DIM == 3) ? (int)threadIdx.y * CY : 0;
+  const tcs_u32 lane_off = ((DIM == 3) ? (R + threadIdx.y * CY) * PW : 0u) + LSHIFT + R + threadIdx.x * CX;
+  const bool inner = ex0 >= R && ex0 < TB_EX - R && (DIM == 2 || (ey0 >= R && ey0 < TB_EY - R));
+  const tcs_i64 xdim = (tcs_i64)G.xdim;
+  const tcs_i64 plane_g = (DIM == 3) ? (tcs_i64)(G.xdim * G.ydim) : xdim;  // stride of the march axis
+  const int plane_lim = (DIM == 3) ? (int)G.z_lim : (int)G.y_lim;         // interior bound along it
+  const int plane_dim = (DIM == 3) ? (int)G.zdim : (int)G.ydim;
   constexpr T c = T(1) / T(S);
   tcs_u32 cur_slot = gc % nslot;
   tcs_u32 cur_par = (gc / nslot) & 1u;
@@ -1400,20 +1411,20 @@ __device__ __forceinline__ bool tb3_piece(const PipeGridView& G, tcs_u32 tile, t
           static_for<0, CX>([&](auto ex) {
             constexpr int e = decltype(ex)::value + decltype(ey)::value * CX;
             const int gx = X0 + ex0 + decltype(ex)::value, gy = Y0 + ey0 + decltype(ey)::value;
-            const bool interior = gx >= (int)G.x0 && gx < (int)G.x_lim && gy >= R && gy < (int)G.y_lim &&
-                                  q >= R && q < (int)G.z_lim;
+            const bool interior = gx >= (int)G.x0 && gx < (int)G.x_lim &&
+                                  (DIM == 2 || (gy >= R && gy < (int)G.y_lim)) && q >= R && q < plane_lim;
             T v = (COEFF == 0) ? slot_value<e>(d1) * c : slot_value<e>(d1);
             if (!interior) {
-              const bool in_grid = gx >= 0 && gx < (int)G.xdim && gy >= 0 && gy < (int)G.ydim && q >= 0 &&
-                                   q < (int)G.zdim;
-              v = in_grid ? G.in[gx + gy * xdim + q * plane_g] : T(0);
+              const bool in_grid = gx >= 0 && gx < (int)G.xdim && (DIM == 2 || (gy >= 0 && gy < (int)G.ydim)) &&
+                                   q >= 0 && q < plane_dim;
+              v = in_grid ? G.in[gx + gy * xdim + q * plane_g] : T(0);  // gy = 0 in 2D
             }
-            bq[(R + ey0 + decltype(ey)::value) * TB_BW + R + ex0 + decltype(ex)::value] = v;
+            bq[((DIM == 3) ? (R + ey0 + decltype(ey)::value) * TB_BW : 0) + R + ex0 + decltype(ex)::value] = v;
           });
         });
         __syncthreads();
         // stage 2: plane q of S(in); completes plane p = q - R of S(S(in)), output pi - 4R
-        const TbPlane ldb{bq + (R + ey0) * TB_BW + R + ex0};
+        const TbPlane ldb{bq + ((DIM == 3) ? (R + ey0) * TB_BW : 0) + R + ex0};
         auto slot2 = [&](auto kk) -> PipeSlot& {
           constexpr int k = decltype(kk)::value;
           return acc2[((t - k) % NP2 + NP2) % NP2];
