@@ -263,7 +263,7 @@ int tcs_precompile_pipe_epilogue(const tcs_spec* spec, unsigned bx, unsigned by,
  * in passes of two (tcs_tb3 kernel), an odd last sweep as an ordinary sweep; *result_in_b says
  * which buffer holds the result.  Bit-identical to n tcs_update_grid sweeps.  `launch` (may be
  * NULL) gives the block (bx, by) of the kernel's thread tiles -- 2 x 2 points for even ranges,
- * 1 x 1 for odd ones; in 2D, strips of bx thread tiles of 2 x 1 or 1 x 1 marching along y, block
+ * 1 x 1 for odd ones; in 2D, strips of bx thread tiles of 2 x 1 points marching along y, block
  * (bx, 1, 1) -- the planes (2D: rows) per ring chunk, the chunks in flight and the CTA count
  * (segments).  3D, and 2D in Row order; FP64 and FP32 (FP32: even ranges), grids of whole
  * coarsening tiles; TCS_ERR_UNSUPPORTED otherwise. */

@@ -99,10 +99,10 @@ def pipe_ring_sweeps(cfg, a: np.ndarray, grid, left_offset, right_offset, n: int
 def tb3_passes(cfg, a: np.ndarray, grid, left_offset, right_offset, n: int, mask=None, precision="f64",
                block=(8, 8), piece: int = 1 << 30, unroll: int = 2):
     """n passes (2n sweeps) through the host build of the two-sweep kernel's control flow,
-    compiled with the kernel's own thread tile (2 x 2 for even ranges, 1 x 1 for odd ones; in 2D
-    2 x 1 or 1 x 1, and block[1] is ignored)."""
+    compiled with the kernel's own thread tile (3D: 2 x 2 for even ranges, 1 x 1 for odd ones;
+    2D: 2 x 1, and block[1] is ignored)."""
     d, sh, o, c, r, cx, cy, cz, al, cl = cfg
-    C = 2 if r % 2 == 0 else 1
+    C = 2 if (r % 2 == 0 or d == 2) else 1
     lib = build((d, sh, o, c, r, C, C if d == 3 else 1, 1, al, cl), precision, "tb3_host.cpp")
     x = np.ascontiguousarray(a).copy()
     y = x.copy()

@@ -6,7 +6,7 @@
 // buffer -- points outside the interior take the input's value -- and, once every thread of the
 // tile has written, stage 2 applies the buffer plane to pipeline 2 and stores the inner thread
 // tiles' completed outputs.  Same tile geometry (extended tile, output tile, thread tiles of
-// TCS_CX x TCS_CY dividing R), same plane offsets and slot rotation as the kernel.  In 2D the
+// TCS_CX x TCS_CY dividing R in 3D), same plane offsets and slot rotation as the kernel.  In 2D the
 // march axis is y: a "plane" is one row, the extended tile a strip of bx * CX columns, the plane
 // buffer one row with an R-wide margin.
 #include <cstring>
@@ -74,7 +74,7 @@ extern "C" int tb3_pass(const unsigned grid[3], unsigned left_offset, unsigned r
   if (!D3) by = 1;
   const int EX = (int)bx * CX, EY = D3 ? (int)by * CY : 1, OX = EX - 2 * R, OY = D3 ? EY - 2 * R : 1;
   const int BW = EX + 2 * R, BH = D3 ? EY + 2 * R : 1;
-  if (OX <= 0 || OY <= 0 || R % CX || (D3 && R % CY) || (!D3 && CY != 1)) return 1;
+  if (OX <= 0 || OY <= 0 || (D3 && (R % CX || R % CY)) || (!D3 && CY != 1)) return 1;
   const long long ntx = (x_lim - x0 + OX - 1) / OX, nty = D3 ? (y_lim - R + OY - 1) / OY : 1;
   const int nthr = (int)(bx * by);
   std::vector<T> buf(2 * (size_t)BW * BH, T(0));
@@ -117,7 +117,7 @@ extern "C" int tb3_pass(const unsigned grid[3], unsigned left_offset, unsigned r
         for (int th = 0; th < nthr; ++th) {  // stage 2
           const int ex0 = (th % (int)bx) * CX, ey0 = (th / (int)bx) * CY;
           PipeSlot* a2 = &acc2[(size_t)th * NP2];
-          const bool inner = ex0 >= R && ex0 < EX - R && (!D3 || (ey0 >= R && ey0 < EY - R));
+          const bool inner = ex0 + CX > R && ex0 < EX - R && (!D3 || (ey0 >= R && ey0 < EY - R));
           // edge thread tiles read the buffer's margin (never written); their outputs are discarded
           const BufPlane ldb{bq + (D3 ? (R + ey0) * BW : 0) + R + ex0, BW};
           auto slot2 = [&](auto kk) -> PipeSlot& {
@@ -132,7 +132,8 @@ extern "C" int tb3_pass(const unsigned grid[3], unsigned left_offset, unsigned r
               static_for<0, CX>([&](auto ex) {
                 constexpr int e = decltype(ex)::value + decltype(ey)::value * CX;
                 const long long ox = X0 + ex0 + decltype(ex)::value, oy = Y0 + ey0 + decltype(ey)::value;
-                if (ox < x_lim && (!D3 || oy < y_lim))
+                const int exx = ex0 + decltype(ex)::value;  // 2D thread tiles may straddle the edge
+                if (ox < x_lim && (!D3 || oy < y_lim) && exx >= R && exx < EX - R)
                   out[ox + (D3 ? oy * xdim : 0) + (ms + op) * plane] =
                       (COEFF == 0) ? slot_value<e>(d2) * c : slot_value<e>(d2);
               });

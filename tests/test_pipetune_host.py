@@ -154,10 +154,34 @@ def test_batch_candidates_and_record(tmp_path, monkeypatch):
                          for bx, by, ch in cands)
     assert {ch for _, _, ch in cands} == {1, 2, 3}
     path = tmp_path / "tuned.json"
-    r = P.PipeTuneResult((64, 4, 3), 230.0, 39, 39, True, 1.0, "batched sweep: exhaustive",
-                         {(64, 4, 3): 230.0, (32, 8, 2): 228.0})
+    r = P.PipeTuneResult((64, 4, 3, 1776), 230.0, 39, 39, True, 1.0, "batched sweep: exhaustive",
+                         {(64, 4, 3, 1776): 230.0, (32, 8, 2, 0): 228.0})
     e = P.write_tuned(path, w.name, "f32", r, batch=True)
-    assert e["block"] == [64, 4, 1] and e["chunk"] == 3 and "228.0" in e["source"]
+    assert e["block"] == [64, 4, 1] and e["chunk"] == 3 and e["segments"] == 1776 and "228.0" in e["source"]
     monkeypatch.setattr(W, "TUNED_PATH", path)
     L = w.tuned_launch("f32")
-    assert (tuple(L.block), L.chunk, L.variant) == ((64, 4, 1), 3, "pipe")
+    assert (tuple(L.block), L.chunk, L.variant, L.segments) == ((64, 4, 1), 3, "pipe", 1776)
+
+
+def test_batch_tuner_searches_cta_counts_of_its_fastest_shapes(monkeypatch):
+    """Stage 1 times every shape at one wave; stage 2 times the three fastest at BATCH_WAVES waves
+    of CTAs, and the record keeps the fastest (shape, CTA count) (scripted timings, no GPU)."""
+    from threadcoarsenedstencilgenerator_b200 import workloads as W
+
+    w = W.BATCH_WORKLOADS["batch_3d_star_jacobi_r2_64"]
+    timed = []
+
+    def fake_time(w_, prec, cand, state, sweeps=10):
+        timed.append(tuple(cand))
+        bx, by, ch, ctas = cand
+        return 100.0 + bx * by / 64.0 + ch + (ctas == 12 * 148 and (bx, by, ch) == (64, 8, 3)) * 50.0
+
+    monkeypatch.setattr(P, "time_batch", fake_time)
+    r = P.tune_batch(w, "f32", num_sms=148)
+    shapes = P.batch_candidates(w.spec)
+    assert len(timed) == len(shapes) + 3 * (len(P.BATCH_WAVES) - 1)
+    assert all(t[3] == 0 for t in timed[:len(shapes)])
+    assert {t[3] for t in timed[len(shapes):]} == {k * 148 for k in P.BATCH_WAVES[1:]}
+    e = P.batch_entry(r)
+    if (64, 8, 3) in {tuple(t[:3]) for t in timed[len(shapes):]}:
+        assert r.candidate == (64, 8, 3, 12 * 148) and e["segments"] == 12 * 148

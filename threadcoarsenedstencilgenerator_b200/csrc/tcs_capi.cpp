@@ -919,8 +919,9 @@ int resolve_pipe(tcs_stencil* h, const TcsGeo& g, const tcs_launch* L, Resolved&
 // ones (C divides R, so a thread tile lies wholly inside or outside the output tile); by default
 // an extended tile of 64 x 32 columns (C = 2: 32 x 16 threads) or 32 x 32 (C = 1: 32 x 32
 // threads), whose inner (EX - 2R) x (EY - 2R) columns are the output tile.  2D (Row order): a
-// strip of EX = bx * C columns marching along y, thread tiles C x 1, by default 128 threads, whose
-// inner EX - 2R columns are the output strip.  `L` (may be NULL) gives the block (bx, by), the
+// strip of EX = bx * 2 columns marching along y, thread tiles 2 x 1 (which may straddle the
+// output strip's edge), by default 64 threads (narrower where a TMA box needs it), whose inner
+// EX - 2R columns are the output strip.  `L` (may be NULL) gives the block (bx, by), the
 // planes (2D: rows) per ring chunk, the chunks in flight and the CTA count.
 int resolve_tb3(tcs_stencil* h, const TcsGeo& g, const tcs_launch* L, Resolved& out) {
   const tcs_spec& s = h->spec;
@@ -930,8 +931,10 @@ int resolve_tb3(tcs_stencil* h, const TcsGeo& g, const tcs_launch* L, Resolved& 
   const bool d3 = s.dimension == 3;
   const unsigned R = (unsigned)s.range;
   const unsigned es = (unsigned)elem_size(s), vec = 16u / es;
-  const unsigned C = (R % 2 == 0) ? 2u : 1u;
-  unsigned bx = d3 ? 32u : 128u, by = d3 ? ((C == 2) ? 16u : 32u) : 1u;
+  const unsigned C = (R % 2 == 0 || !d3) ? 2u : 1u;
+  // 2D: 64 threads (128-column strips) by default; on the 4096^2 Box r1 grid 64, 96, 120 and 126
+  // threads measured 514, 500-520, 504 and 503-520 GLup/s
+  unsigned bx = d3 ? 32u : 64u, by = d3 ? ((C == 2) ? 16u : 32u) : 1u;
   while (!d3 && bx > 8 && bx * C + 2 * R + vec > 256) bx -= 8;  // 2D: the strip fits a TMA box
   if (L && L->block[0]) {
     bx = L->block[0];
@@ -961,7 +964,9 @@ int resolve_tb3(tcs_stencil* h, const TcsGeo& g, const tcs_launch* L, Resolved& 
   int maxthr = 0;
   TCS_CU(g_drv.FuncGetAttribute(&maxthr, CU_FUNC_ATTRIBUTE_MAX_THREADS_PER_BLOCK, pm->f));
   if (nthr > maxthr) return fail(TCS_ERR_UNSUPPORTED, "tb3: block exceeds the kernel's thread limit");
-  unsigned nslot = (L && L->depth) ? 1 + L->depth : 3u, smem = 0;
+  // 2D: one chunk in flight by default (the smaller ring admits more CTAs per SM; measured on the
+  // 4096^2 Box r1 grid: 520.9 GLup/s against 503.8 with two)
+  unsigned nslot = (L && L->depth) ? 1 + L->depth : (d3 ? 3u : 2u), smem = 0;
   for (;; --nslot) {
     smem = ((nslot * 8 + 127) / 128) * 128 + 128 + nslot * chunk_bytes + buf_bytes;
     if (smem <= (unsigned)h->smem_optin || nslot == 2) break;
@@ -983,10 +988,12 @@ int resolve_tb3(tcs_stencil* h, const TcsGeo& g, const tcs_launch* L, Resolved& 
   const unsigned long long total = (unsigned long long)ntx * nty * M;
   unsigned long long nctas = (unsigned long long)h->num_sms * (unsigned)occ;
   if (!d3) {
-    // Every piece re-reads 4R rows and recomputes 2R rows of stage 1: keep pieces at least
-    // 64 rows long unless that leaves SMs idle.
-    const unsigned long long cap = std::max<unsigned long long>((unsigned long long)h->num_sms, total / 64);
-    nctas = std::min(nctas, cap);
+    // 2D: three waves of resident CTAs (on the 4096^2 Box r1 grid 1, 1.6, 2.4, 3.2 and 4.8 waves
+    // of 128-thread CTAs measured 369, 467, 520, 521 and 521 GLup/s: later waves fill the SMs
+    // whose CTAs finish first), but pieces of at least 16 rows (each re-reads 4R rows and
+    // recomputes 2R rows of stage 1).
+    const unsigned long long cap = std::max<unsigned long long>((unsigned long long)h->num_sms, total / 16);
+    nctas = std::min(3 * nctas, cap);
   }
   if (L && L->segments) nctas = L->segments;
   const unsigned long long per = std::max<unsigned long long>(1, (total + nctas - 1) / nctas);
@@ -2593,9 +2600,9 @@ int tcs_precompile_tb3(const tcs_spec* spec, unsigned bx, unsigned by, unsigned 
   const bool d3 = spec->dimension == 3;
   if (!d3 && spec->orientation == TCS_COLUMN) return fail(TCS_ERR_UNSUPPORTED, "tb3: 2D stencils in Row order only");
   const unsigned R = (unsigned)spec->range, vec = 16u / (unsigned)elem_size(*spec);
-  const unsigned C = (R % 2 == 0) ? 2u : 1u;
+  const unsigned C = (R % 2 == 0 || !d3) ? 2u : 1u;
   if (bx == 0) {
-    bx = d3 ? 32u : 128u;
+    bx = d3 ? 32u : 64u;
     by = d3 ? ((C == 2) ? 16u : 32u) : 1u;
     while (!d3 && bx > 8 && bx * C + 2 * R + vec > 256) bx -= 8;
   }

@@ -1286,14 +1286,15 @@ extern "C" __global__ void __launch_bounds__(TCS_BX * ((TCS_DIM == 3) ? TCS_BY :
 // the inner (TB_EX - 2R) x (TB_EY - 2R) columns; the outer ring of threads only serves stage 1.
 // Both stages use the per-output term order of one sweep, so out = S(S(in)) bit for bit.
 // In 2D the march axis is y and a "plane" is one row: the extended tile is a strip of TB_EX
-// columns (CX per thread dividing R), the plane buffer one row with an R-wide margin, and the
-// output tile the inner TB_EX - 2R columns of every row.
+// columns, the plane buffer one row with an R-wide margin, and the output tile the inner
+// TB_EX - 2R columns of every row; a thread tile (CX columns) may straddle the output tile's
+// edge, so the store tests each column.
 namespace tcs {
 constexpr int TB_EX = TXP, TB_EY = TYP;                                       // extended tile (stage 1)
 constexpr int TB_OX = TB_EX - 2 * R, TB_OY = (DIM == 3) ? TB_EY - 2 * R : 1;  // output tile (stage 2)
 constexpr int TB_BW = TB_EX + 2 * R, TB_BH = (DIM == 3) ? TB_EY + 2 * R : 1;  // plane buffer, range-wide margin
 static_assert(TB_OX > 0 && TB_OY > 0 && TB_OX % VEC == 0, "output tile: positive, 16-byte multiple");
-static_assert(R % CX == 0 && (DIM == 2 || R % CY == 0), "thread tiles must not straddle the output tile's edge");
+static_assert(DIM == 2 || (R % CX == 0 && R % CY == 0), "3D thread tiles must not straddle the output tile's edge");
 static_assert(DIM == 3 || CY == 1, "2D strips: one row per thread");
 static_assert(!COMP && EPI == 0, "plain sweeps only");
 
@@ -1360,7 +1361,8 @@ __device__ __forceinline__ bool tb3_piece(const PipeGridView& G, tcs_u32 tile, t
   const int ex0 = (int)threadIdx.x * CX;  // thread tile in the extended tile
   const int ey0 = (DIM == 3) ? (int)threadIdx.y * CY : 0;
   const tcs_u32 lane_off = ((DIM == 3) ? (R + threadIdx.y * CY) * PW : 0u) + LSHIFT + R + threadIdx.x * CX;
-  const bool inner = ex0 >= R && ex0 < TB_EX - R && (DIM == 2 || (ey0 >= R && ey0 < TB_EY - R));
+  // some column of the thread tile lies in the output tile (3D: all of them)
+  const bool inner = ex0 + CX > R && ex0 < TB_EX - R && (DIM == 2 || (ey0 >= R && ey0 < TB_EY - R));
   const tcs_i64 xdim = (tcs_i64)G.xdim;
   const tcs_i64 plane_g = (DIM == 3) ? (tcs_i64)(G.xdim * G.ydim) : xdim;  // stride of the march axis
   const int plane_lim = (DIM == 3) ? (int)G.z_lim : (int)G.y_lim;         // interior bound along it
@@ -1438,7 +1440,9 @@ __device__ __forceinline__ bool tb3_piece(const PipeGridView& G, tcs_u32 tile, t
             static_for<0, CX>([&](auto ex) {
               constexpr int e = decltype(ex)::value + decltype(ey)::value * CX;
               const int ox = X0 + ex0 + decltype(ex)::value, oy = Y0 + ey0 + decltype(ey)::value;
-              if (ox < (int)G.x_lim && oy < (int)G.y_lim)
+              constexpr bool EDGE = DIM == 2 && R % CX != 0;  // thread tiles straddling the edge
+              const int exx = ex0 + decltype(ex)::value;
+              if (ox < (int)G.x_lim && oy < (int)G.y_lim && (!EDGE || (exx >= R && exx < TB_EX - R)))
                 G.out[ox + oy * xdim + pz] = (COEFF == 0) ? slot_value<e>(d2) * c : slot_value<e>(d2);
             });
           });

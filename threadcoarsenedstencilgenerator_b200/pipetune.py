@@ -412,10 +412,11 @@ def time_batch(w, precision: str, cand, state: dict, sweeps: int = 10) -> float 
         state["xs"] = [torch.from_numpy(np.ascontiguousarray(v)).cuda() for v in w.make_inputs(geoms, dt)]
         state["ys"] = [x.clone() for x in state["xs"]]
         state["points"] = sum(g.interior_points for g in geoms)
-    bx, by, ch = cand
+    bx, by, ch = cand[:3]
+    ctas = cand[3] if len(cand) > 3 else 0
     try:
         bt = BatchedSweeps(state["st"], state["geoms"], state["xs"], state["ys"],
-                           Launch(block=(bx, by, 1), variant="pipe", chunk=ch))
+                           Launch(block=(bx, by, 1), variant="pipe", chunk=ch, segments=ctas))
     except _lib.TcsError:
         return None
     try:
@@ -435,32 +436,57 @@ def time_batch(w, precision: str, cand, state: dict, sweeps: int = 10) -> float 
     return state["points"] * sweeps / (ms / 1e3) / 1e9 if ms > 0 else None
 
 
-def tune_batch(w, precision: str = "f64") -> PipeTuneResult:
-    """Exhaustive search of the batched sweep's launch (the cost model covers single grids)."""
+# CTA counts of the batched launch's second stage, in waves of one CTA per SM (0: one wave of
+# every resident CTA).  Several waves of short contiguous work runs let the CTAs that finish early
+# (runs of TMA-loaded grids) take more of the work list than those on cp.async-loaded grids.
+BATCH_WAVES = (0, 2, 4, 6, 8, 12, 16)
+
+
+def tune_batch(w, precision: str = "f64", num_sms: int | None = None) -> PipeTuneResult:
+    """Exhaustive search of the batched sweep's launch (the cost model covers single grids):
+    every (bx, by, chunk) at one wave of CTAs, then the CTA count (BATCH_WAVES) for the three
+    fastest shapes.  Candidates are (bx, by, chunk, ctas)."""
+    from .stencil import device_sm_count
+
     t0 = time.perf_counter()
     cands = batch_candidates(w.spec)
     state, res = {}, {}
     for c in cands:
-        g = time_batch(w, precision, c, state)
+        g = time_batch(w, precision, tuple(c) + (0,), state)
         if g is not None:
-            res[tuple(c)] = g
+            res[tuple(c) + (0,)] = g
+    n_sms = num_sms or device_sm_count()
+    top = sorted(res, key=res.get, reverse=True)[:3]
+    n_cands = len(cands)
+    for c in top:
+        for waves in BATCH_WAVES[1:]:
+            cc = tuple(c[:3]) + (waves * n_sms,)
+            n_cands += 1
+            g = time_batch(w, precision, cc, state)
+            if g is not None:
+                res[cc] = g
     if "st" in state:
         state["st"].close()
     if not res:
         raise _lib.UnsupportedLaunch(_lib.TCS_ERR_UNSUPPORTED, "no batched launch runs this batch")
     best = max(res, key=res.get)
-    return PipeTuneResult(best, res[best], len(res), len(cands), True, time.perf_counter() - t0,
+    return PipeTuneResult(best, res[best], len(res), n_cands, True, time.perf_counter() - t0,
                           "batched sweep: exhaustive", res)
 
 
 def batch_entry(r: PipeTuneResult) -> dict:
-    """A tuned-launch record of a batched tuning result (block and chunk; the batch's coarsening)."""
-    bx, by, ch = r.candidate
+    """A tuned-launch record of a batched tuning result (block, chunk and CTA count; the batch's
+    coarsening)."""
+    bx, by, ch = r.candidate[:3]
+    ctas = r.candidate[3] if len(r.candidate) > 3 else 0
     runner_up = sorted(((v, k) for k, v in r.measured.items() if tuple(k) != tuple(r.candidate)), reverse=True)[:1]
     src = "pipetune exhaustive over %d of %d batched launches: %.1f GLup/s" % (r.timed, r.candidates, r.glups)
     if runner_up:
         src += "; next %s: %.1f" % ("x".join(map(str, runner_up[0][1])), runner_up[0][0])
-    return {"block": [bx, by, 1], "variant": "pipe", "chunk": ch, "source": src}
+    e = {"block": [bx, by, 1], "variant": "pipe", "chunk": ch, "source": src}
+    if ctas:
+        e["segments"] = ctas
+    return e
 
 
 def _precompile_batch_job(job):
