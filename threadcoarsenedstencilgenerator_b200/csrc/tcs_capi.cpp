@@ -955,7 +955,9 @@ int resolve_tb3(tcs_stencil* h, const TcsGeo& g, const tcs_launch* L, Resolved& 
   if (W > 256 || rows > 256 || ch > 256)
     return fail(TCS_ERR_UNSUPPORTED, "tb3: tile exceeds the 256-element TMA box limit");
   const unsigned chunk_bytes = ch * rows * W * es;
-  const unsigned buf_bytes = 2u * (EX + 2 * R) * (d3 ? EY + 2 * R : 1u) * es;
+  // two plane buffers; a 2D row has its left margin rounded up to even and an even width (at
+  // most EX + 2R + 2 elements)
+  const unsigned buf_bytes = 2u * (d3 ? (EX + 2 * R) * (EY + 2 * R) : EX + 2 * R + 2) * es;
   PipeKey key{bx, by, ch, lshift, 0u, 0u, C};
   PipeMod* pm = nullptr;
   int rc = pipe_module(h, key, &pm);

@@ -1292,18 +1292,22 @@ extern "C" __global__ void __launch_bounds__(TCS_BX * ((TCS_DIM == 3) ? TCS_BY :
 namespace tcs {
 constexpr int TB_EX = TXP, TB_EY = TYP;                                       // extended tile (stage 1)
 constexpr int TB_OX = TB_EX - 2 * R, TB_OY = (DIM == 3) ? TB_EY - 2 * R : 1;  // output tile (stage 2)
-constexpr int TB_BW = TB_EX + 2 * R, TB_BH = (DIM == 3) ? TB_EY + 2 * R : 1;  // plane buffer, range-wide margin
+// Plane buffer with a range-wide margin; in 2D the left margin TB_ML is rounded up to even and the
+// row to an even width, so a thread's column pairs sit on 2-element boundaries (one access each).
+constexpr int TB_ML = (DIM == 3) ? R : R + (R & 1);
+constexpr int TB_BW = (DIM == 3) ? TB_EX + 2 * R : ((TB_ML + TB_EX + R + 1) / 2) * 2;
+constexpr int TB_BH = (DIM == 3) ? TB_EY + 2 * R : 1;
 static_assert(TB_OX > 0 && TB_OY > 0 && TB_OX % VEC == 0, "output tile: positive, 16-byte multiple");
 static_assert(DIM == 2 || (R % CX == 0 && R % CY == 0), "3D thread tiles must not straddle the output tile's edge");
 static_assert(DIM == 3 || CY == 1, "2D strips: one row per thread");
 static_assert(!COMP && EPI == 0, "plain sweeps only");
 
 // Reader of a stage-1 plane in the plane buffer at a thread origin (row pitch TB_BW).  Pairs are
-// aligned where the buffer column R + gx is even (the buffer starts on 128 bytes, TB_BW is even).
+// aligned where the buffer column TB_ML + gx is even (the buffer starts on 128 bytes, TB_BW is even).
 struct TbPlane {
   const T* p;
   __host__ __device__ static constexpr bool pair_aligned(int gx) {
-    return (CX % 2 == 0) && (TB_BW % 2 == 0) && (((R + gx) % 2 + 2) % 2 == 0);
+    return (CX % 2 == 0) && (TB_BW % 2 == 0) && (((TB_ML + gx) % 2 + 2) % 2 == 0);
   }
   template <int GX, int GY>
   __device__ __forceinline__ T one() const {
@@ -1410,6 +1414,7 @@ __device__ __forceinline__ bool tb3_piece(const PipeGridView& G, tcs_u32 tile, t
         T* bq = bbuf + (pi & 1) * (TB_BW * TB_BH);
         PipeSlot& d1 = acc1[((t - 2 * R) % NP2 + NP2) % NP2];
         static_for<0, CY>([&](auto ey) {
+          T vrow[CX];
           static_for<0, CX>([&](auto ex) {
             constexpr int e = decltype(ex)::value + decltype(ey)::value * CX;
             const int gx = X0 + ex0 + decltype(ex)::value, gy = Y0 + ey0 + decltype(ey)::value;
@@ -1421,12 +1426,25 @@ __device__ __forceinline__ bool tb3_piece(const PipeGridView& G, tcs_u32 tile, t
                                    q >= 0 && q < plane_dim;
               v = in_grid ? G.in[gx + gy * xdim + q * plane_g] : T(0);  // gy = 0 in 2D
             }
-            bq[((DIM == 3) ? (R + ey0 + decltype(ey)::value) * TB_BW : 0) + R + ex0 + decltype(ex)::value] = v;
+            vrow[decltype(ex)::value] = v;
           });
+          T* brow = bq + ((DIM == 3) ? (R + ey0 + decltype(ey)::value) * TB_BW : 0) + TB_ML + ex0;
+          if constexpr (DIM == 2 && CX % 2 == 0) {
+            // TB_ML and ex0 are even: each pair of the thread's row is one aligned access
+            static_for<0, CX / 2>([&](auto pp) {
+              constexpr int k = 2 * decltype(pp)::value;
+              typename PairOf<T>::type v2;
+              v2.x = vrow[k];
+              v2.y = vrow[k + 1];
+              *reinterpret_cast<typename PairOf<T>::type*>(brow + k) = v2;
+            });
+          } else {
+            static_for<0, CX>([&](auto ex) { brow[decltype(ex)::value] = vrow[decltype(ex)::value]; });
+          }
         });
         __syncthreads();
         // stage 2: plane q of S(in); completes plane p = q - R of S(S(in)), output pi - 4R
-        const TbPlane ldb{bq + ((DIM == 3) ? (R + ey0) * TB_BW : 0) + R + ex0};
+        const TbPlane ldb{bq + ((DIM == 3) ? (R + ey0) * TB_BW : 0) + TB_ML + ex0};
         auto slot2 = [&](auto kk) -> PipeSlot& {
           constexpr int k = decltype(kk)::value;
           return acc2[((t - k) % NP2 + NP2) % NP2];
@@ -1436,16 +1454,38 @@ __device__ __forceinline__ bool tb3_piece(const PipeGridView& G, tcs_u32 tile, t
         if (inner && op >= 0 && op < nout) {
           PipeSlot& d2 = acc2[((t - 2 * R) % NP2 + NP2) % NP2];
           const tcs_i64 pz = (tcs_i64)(ms + op) * plane_g;
-          static_for<0, CY>([&](auto ey) {
-            static_for<0, CX>([&](auto ex) {
-              constexpr int e = decltype(ex)::value + decltype(ey)::value * CX;
-              const int ox = X0 + ex0 + decltype(ex)::value, oy = Y0 + ey0 + decltype(ey)::value;
-              constexpr bool EDGE = DIM == 2 && R % CX != 0;  // thread tiles straddling the edge
-              const int exx = ex0 + decltype(ex)::value;
-              if (ox < (int)G.x_lim && oy < (int)G.y_lim && (!EDGE || (exx >= R && exx < TB_EX - R)))
-                G.out[ox + oy * xdim + pz] = (COEFF == 0) ? slot_value<e>(d2) * c : slot_value<e>(d2);
+          if constexpr (DIM == 2 && CX % 2 == 0) {
+            // column pairs: one access where both are outputs and the address allows it
+            static_for<0, CX / 2>([&](auto pp) {
+              constexpr int k = 2 * decltype(pp)::value;
+              const int exa = ex0 + k, ox = X0 + exa;
+              const T a = (COEFF == 0) ? slot_value<k>(d2) * c : slot_value<k>(d2);
+              const T b = (COEFF == 0) ? slot_value<k + 1>(d2) * c : slot_value<k + 1>(d2);
+              const bool sa = ox < (int)G.x_lim && exa >= R && exa < TB_EX - R;
+              const bool sb = ox + 1 < (int)G.x_lim && exa + 1 >= R && exa + 1 < TB_EX - R;
+              T* o = G.out + ox + pz;
+              if (sa && sb && G.st_pair && (ox & 1) == 0) {
+                typename PairOf<T>::type v2;
+                v2.x = a;
+                v2.y = b;
+                *reinterpret_cast<typename PairOf<T>::type*>(o) = v2;
+              } else {
+                if (sa) o[0] = a;
+                if (sb) o[1] = b;
+              }
             });
-          });
+          } else {
+            static_for<0, CY>([&](auto ey) {
+              static_for<0, CX>([&](auto ex) {
+                constexpr int e = decltype(ex)::value + decltype(ey)::value * CX;
+                const int ox = X0 + ex0 + decltype(ex)::value, oy = Y0 + ey0 + decltype(ey)::value;
+                constexpr bool EDGE = DIM == 2 && R % CX != 0;  // thread tiles straddling the edge
+                const int exx = ex0 + decltype(ex)::value;
+                if (ox < (int)G.x_lim && oy < (int)G.y_lim && (!EDGE || (exx >= R && exx < TB_EX - R)))
+                  G.out[ox + oy * xdim + pz] = (COEFF == 0) ? slot_value<e>(d2) * c : slot_value<e>(d2);
+              });
+            });
+          }
         }
       }
     });
@@ -1487,7 +1527,8 @@ extern "C" __global__ void __launch_bounds__(TCS_BX * TCS_BY)
   G.ntx = g.ntx;
   G.use_tma = (g.loader == 0);
   G.cp_pair = false;
-  G.st_pair = false;
+  // output pairs with one access: even pitch and a pair-aligned base (2D strips)
+  G.st_pair = (g.xdim % 2 == 0) && (reinterpret_cast<tcs_u64>(out) % (2 * sizeof(T)) == 0);
   G.src_pair = false;
   G.aux = nullptr;
   if (G.use_tma && threadIdx.x == 0 && threadIdx.y == 0) tma_prefetch_map(&tmap);
