@@ -42,3 +42,20 @@ def test_two_sweep_pass_equals_two_sweeps(case, precision):
     got = host_tile.tb3_passes(cfg, a, g.grid, g.left_offset, g.right_offset, 2, mask, precision, block, piece,
                                unroll)
     assert np.array_equal(got, want)
+
+
+def test_2d_strip_instances_compile_and_reject_what_they_cannot_run():
+    """The 2D two-sweep kernel instantiates without a GPU for Row stencils of several ranges (its
+    default strip of 64 threads, narrowed where a TMA box needs it) and rejects Column order and
+    FP32 with an odd range (no output strip of 16-byte multiples)."""
+    import threadcoarsenedstencilgenerator_b200 as tcs
+    from threadcoarsenedstencilgenerator_b200.stencil import precompile_tb3
+
+    for sh, co, r, prec in [("Box", "Jacobi", 1, "f64"), ("Star", "Variable", 3, "f64"),
+                            ("Box", "Variable", 6, "f64"), ("Star", "Jacobi", 2, "f32")]:
+        spec = tcs.StencilSpec(dimension=2, neighbourhood=sh, coefficients=co, range=r, precision=prec)
+        assert precompile_tb3(spec).endswith(".cubin")
+    with pytest.raises(tcs.UnsupportedLaunch):
+        precompile_tb3(tcs.StencilSpec(dimension=2, neighbourhood="Star", orientation="Column", range=1))
+    with pytest.raises(tcs.UnsupportedLaunch):
+        precompile_tb3(tcs.StencilSpec(dimension=2, neighbourhood="Box", range=1, precision="f32"))
