@@ -1041,7 +1041,7 @@ def run_case(args) -> dict:
     torch.cuda.synchronize()
     if st.device_status() != 0:
         raise RuntimeError("device status word set")
-    plan = st.plan(geom, launch)
+    plan = st.plan_tb3(geom, tb3_launch) if args.case == "temporal-strips" else st.plan(geom, launch)
     ms = e0.elapsed_time(e1)  # CUDA events around the --steps sweeps after the warm-up
     return {"case": args.workload, "grid": list(grid), "points": geom.interior_points, "sweeps": args.steps,
             "kernel": args.case, "variant": plan.variant, "block": list(plan.block), "chunk": plan.chunk,
