@@ -59,3 +59,17 @@ def test_2d_strip_instances_compile_and_reject_what_they_cannot_run():
         precompile_tb3(tcs.StencilSpec(dimension=2, neighbourhood="Star", orientation="Column", range=1))
     with pytest.raises(tcs.UnsupportedLaunch):
         precompile_tb3(tcs.StencilSpec(dimension=2, neighbourhood="Box", range=1, precision="f32"))
+
+
+@pytest.mark.parametrize("R", range(1, 9))
+def test_2d_strip_row_buffer_fits_the_host_allocation(R):
+    """The 2D strip kernel's row buffer (left margin TB_ML = R rounded up to even, width rounded up
+    to even: tcs_kernels.cuh) never exceeds the EX + 2R + 2 elements per buffer that the host
+    reserves (tcs_capi.cpp, resolve_tb3), and every thread's column pair starts on an even column."""
+    for EX in range(2 * R + 2, 258, 2):
+        ml = R + (R & 1)
+        bw = ((ml + EX + R + 1) // 2) * 2
+        assert bw <= EX + 2 * R + 2 and bw % 2 == 0 and ml % 2 == 0
+        assert all((ml + ex0) % 2 == 0 for ex0 in range(0, EX, 2))
+        # stage 2 reads columns ml + ex0 - R .. ml + ex0 + 1 + R of the buffer: inside it
+        assert ml - R >= 0 and ml + (EX - 2) + 1 + R < bw
